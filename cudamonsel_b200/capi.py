@@ -1,0 +1,290 @@
+"""ctypes binding of the C ABI in include/cudamonsel_b200.h.
+
+The shared library is built in-tree (``python -m cudamonsel_b200.build``).
+There is no fallback: if the library is missing or no sm_100 device is
+present, creating an Engine raises.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIBPATH = os.path.join(HERE, "libcudamonsel_b200.so")
+
+PREC_FP64 = 0
+PREC_FP32 = 1
+OPT_JMONSEL_FIXES = 1
+
+# every symbol include/cudamonsel_b200.h declares
+EXPORTS = (
+    "cm_context_create", "cm_context_destroy", "cm_last_error", "cm_set_options", "cm_version",
+    "cm_add_mott_element", "cm_add_table", "cm_add_material", "cm_add_msm", "cm_msm_add_nistmott",
+    "cm_msm_add_tabulated", "cm_msm_add_fitted", "cm_msm_add_phonon", "cm_msm_add_polaron", "cm_msm_set_csd_jln",
+    "cm_msm_set_min_e", "cm_msm_set_barrier", "cm_shape_sphere", "cm_shape_planes", "cm_shape_intersection",
+    "cm_shape_translate", "cm_shape_line", "cm_region_add", "cm_run", "cm_run_device", "cm_eval_nistmott",
+    "cm_eval_table", "cm_eval_tabulated", "cm_eval_elastic", "cm_eval_csd", "cm_eval_phonon", "cm_eval_shape",
+    "cm_eval_barrier", "cm_eval_freepath",
+)
+
+
+class RunDesc(C.Structure):
+    _fields_ = [("chamber", C.c_int), ("precision", C.c_int), ("npix", C.c_int), ("beam_width", C.c_double),
+                ("pixel_center", C.POINTER(C.c_double)), ("pixel_energy", C.POINTER(C.c_double)),
+                ("pixel_nprim", C.POINTER(C.c_int)), ("pixel_nbins", C.POINTER(C.c_int)), ("seed", C.c_uint64),
+                ("hist_stride", C.c_int), ("wave", C.c_int), ("max_iterations", C.c_int)]
+
+
+class RunStats(C.Structure):
+    _fields_ = [("primaries", C.c_int64), ("steps", C.c_int64), ("scatter_events", C.c_int64),
+                ("barrier_events", C.c_int64), ("escapes", C.c_int64), ("secondaries", C.c_int64),
+                ("iterations", C.c_int64), ("device_ms", C.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class CMError(RuntimeError):
+    pass
+
+
+_lib = None
+
+
+def load():
+    """Load the in-tree library (raises if it was not built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIBPATH):
+        raise CMError("libcudamonsel_b200.so not built; run `python -m cudamonsel_b200.build`")
+    L = C.CDLL(LIBPATH)
+    d = C.POINTER(C.c_double)
+    i = C.POINTER(C.c_int)
+    ctx = C.c_void_p
+    sig = {
+        "cm_context_create": [C.c_int, C.POINTER(C.c_void_p)],
+        "cm_context_destroy": [ctx],
+        "cm_set_options": [ctx, C.c_int],
+        "cm_add_mott_element": [ctx, C.c_int, d, d],
+        "cm_add_table": [ctx, C.c_int, i, d, d, i],
+        "cm_add_material": [ctx, C.c_int, i, d, d, C.c_double, C.c_double, C.c_double, C.c_double, C.c_int, d, i],
+        "cm_add_msm": [ctx, C.c_int, i],
+        "cm_msm_add_nistmott": [ctx, C.c_int, C.c_int, i],
+        "cm_msm_add_tabulated": [ctx, C.c_int, C.c_int, C.c_double, i, i],
+        "cm_msm_add_fitted": [ctx, C.c_int, C.c_double, C.c_double, i],
+        "cm_msm_add_phonon": [ctx, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double, i],
+        "cm_msm_add_polaron": [ctx, C.c_int, C.c_double, C.c_double, i],
+        "cm_msm_set_csd_jln": [ctx, C.c_int, C.c_double],
+        "cm_msm_set_min_e": [ctx, C.c_int, C.c_double],
+        "cm_msm_set_barrier": [ctx, C.c_int, C.c_int, C.c_double],
+        "cm_shape_sphere": [ctx, d, C.c_double, i],
+        "cm_shape_planes": [ctx, C.c_int, d, d, i],
+        "cm_shape_intersection": [ctx, C.c_int, C.c_int, i],
+        "cm_shape_translate": [ctx, C.c_int, d],
+        "cm_shape_line": [ctx, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double, i],
+        "cm_region_add": [ctx, C.c_int, C.c_int, C.c_int, i],
+        "cm_run": [ctx, C.POINTER(RunDesc), C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.POINTER(RunStats)],
+        "cm_run_device": [ctx, C.POINTER(RunDesc), C.c_void_p, C.c_void_p, C.POINTER(RunStats), C.c_void_p],
+        "cm_eval_nistmott": [ctx, C.c_int, C.c_int, d, d, d, d, C.c_int],
+        "cm_eval_table": [ctx, C.c_int, C.c_int, d, C.c_int, d, C.c_int],
+        "cm_eval_tabulated": [ctx, C.c_int, C.c_int, C.c_int, d, d, C.c_int],
+        "cm_eval_elastic": [ctx, C.c_int, C.c_int, C.c_int, d, d, C.c_int],
+        "cm_eval_csd": [ctx, C.c_int, C.c_int, d, d, C.c_int],
+        "cm_eval_phonon": [ctx, C.c_int, C.c_int, C.c_int, d, d, C.c_int],
+        "cm_eval_shape": [ctx, C.c_int, C.c_int, d, d],
+        "cm_eval_barrier": [ctx, C.c_int, C.c_int, C.c_int, d, d, C.c_int],
+        "cm_eval_freepath": [ctx, C.c_int, C.c_int, d, d, C.c_int],
+    }
+    for name, args in sig.items():
+        f = getattr(L, name)
+        f.argtypes = args
+        f.restype = C.c_int
+    L.cm_last_error.restype = C.c_char_p
+    L.cm_last_error.argtypes = []
+    L.cm_version.restype = C.c_int
+    _lib = L
+    return L
+
+
+def _d(a):
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    return a, a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def _i(a):
+    a = np.ascontiguousarray(a, dtype=np.int32)
+    return a, a.ctypes.data_as(C.POINTER(C.c_int))
+
+
+class Engine:
+    """One cm_context on one CUDA device.  Methods mirror the C ABI (SI units)."""
+
+    def __init__(self, device=0):
+        self.L = load()
+        h = C.c_void_p()
+        self._check(self.L.cm_context_create(device, C.byref(h)))
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.cm_context_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc):
+        if rc != 0:
+            raise CMError("cudamonsel_b200 error %d: %s" % (rc, self.L.cm_last_error().decode()))
+
+    def _out(self, fn, *args):
+        o = C.c_int(-1)
+        self._check(fn(self.h, *args, C.byref(o)))
+        return o.value
+
+    # ---- scene (same method names as oracle/pyoracle.Scene via scene.SceneSpec)
+    def set_options(self, opt):
+        self._check(self.L.cm_set_options(self.h, opt))
+
+    def mott(self, Z, spwem, x1):
+        a, pa = _d(spwem)
+        b, pb = _d(x1)
+        self._check(self.L.cm_add_mott_element(self.h, Z, pa, pb))
+
+    def table(self, dim, n, axes, values):
+        ni, pn = _i(n)
+        ax, pax = _d(np.concatenate([np.asarray(a, dtype=np.float64) for a in axes]))
+        v, pv = _d(np.asarray(values, dtype=np.float64).ravel())
+        return self._out(self.L.cm_add_table, dim, pn, pax, pv)
+
+    def material(self, Z, A, wf, density, workfunction, ecb, bandgap, core=()):
+        z, pz = _i(Z if len(Z) else [0])
+        a, pa = _d(A if len(A) else [0])
+        w, pw = _d(wf if len(wf) else [0])
+        c, pc = _d(core if len(core) else [0])
+        return self._out(self.L.cm_add_material, len(Z), pz, pa, pw, density, workfunction, ecb, bandgap, len(core), pc)
+
+    def msm(self, material):
+        return self._out(self.L.cm_add_msm, material)
+
+    def nistmott(self, msm, method=1):
+        return self._out(self.L.cm_msm_add_nistmott, msm, method)
+
+    def tabulated(self, msm, method_se, offset, tables):
+        t, pt = _i(tables)
+        return self._out(self.L.cm_msm_add_tabulated, msm, method_se, offset, pt)
+
+    def fitted(self, msm, energy_se_gen, break_e):
+        return self._out(self.L.cm_msm_add_fitted, msm, energy_se_gen, break_e)
+
+    def phonon(self, msm, ratemult, phonon_e, temperature, eps0, eps_inf):
+        return self._out(self.L.cm_msm_add_phonon, msm, ratemult, phonon_e, temperature, eps0, eps_inf)
+
+    def polaron(self, msm, prefactor, extinction):
+        return self._out(self.L.cm_msm_add_polaron, msm, prefactor, extinction)
+
+    def csd_jln(self, msm, break_e):
+        self._check(self.L.cm_msm_set_csd_jln(self.h, msm, break_e))
+
+    def min_e(self, msm, e):
+        self._check(self.L.cm_msm_set_min_e(self.h, msm, e))
+
+    def barrier(self, msm, classical, lam):
+        self._check(self.L.cm_msm_set_barrier(self.h, msm, classical, lam))
+
+    def sphere(self, c, r):
+        a, pa = _d(c)
+        return self._out(self.L.cm_shape_sphere, pa, r)
+
+    def planes(self, normals, points):
+        n, pn = _d(normals)
+        p, pp = _d(points)
+        return self._out(self.L.cm_shape_planes, len(n) // 3, pn, pp)
+
+    def intersection(self, a, b):
+        return self._out(self.L.cm_shape_intersection, a, b)
+
+    def translate(self, shape, d):
+        a, pa = _d(d)
+        self._check(self.L.cm_shape_translate(self.h, shape, pa))
+
+    def line(self, topz, width, length, thetal, thetar):
+        return self._out(self.L.cm_shape_line, topz, width, length, thetal, thetar)
+
+    def region(self, parent, msm, shape):
+        return self._out(self.L.cm_region_add, parent, msm, shape)
+
+    # ---- runs
+    def run(self, chamber, centers, energies, nprim, nbins, beam_width, seed, precision=PREC_FP64, wave=0,
+            max_iterations=0):
+        centers = np.ascontiguousarray(centers, dtype=np.float64).reshape(-1, 3)
+        npix = len(centers)
+        e, pe = _d(np.broadcast_to(np.asarray(energies, dtype=np.float64), (npix,)).copy())
+        c, pc = _d(centers.ravel())
+        n, pn = _i(np.broadcast_to(np.asarray(nprim), (npix,)).copy())
+        b, pb = _i(np.broadcast_to(np.asarray(nbins), (npix,)).copy())
+        stride = int(b.max()) + 2
+        desc = RunDesc(chamber, precision, npix, beam_width, pc, pe, pn, pb, seed, stride, wave, max_iterations)
+        back = np.zeros((npix, stride), dtype=np.uint32)
+        fwd = np.zeros((npix, stride), dtype=np.uint32)
+        st = RunStats()
+        self._check(self.L.cm_run(self.h, C.byref(desc), back.ctypes.data_as(C.POINTER(C.c_uint32)),
+                                  fwd.ctypes.data_as(C.POINTER(C.c_uint32)), C.byref(st)))
+        return back, fwd, st
+
+    def run_device(self, desc, back_ptr, fwd_ptr, stream_ptr=None):
+        st = RunStats()
+        self._check(self.L.cm_run_device(self.h, C.byref(desc), C.c_void_p(back_ptr), C.c_void_p(fwd_ptr),
+                                         C.byref(st), C.c_void_p(stream_ptr) if stream_ptr else None))
+        return st
+
+    # ---- per-function entry points
+    def eval_nistmott(self, Z, E, u, precision=PREC_FP64):
+        E, pE = _d(E)
+        u, pu = _d(u)
+        s = np.zeros(len(E))
+        t = np.zeros(len(E))
+        self._check(self.L.cm_eval_nistmott(self.h, Z, len(E), pE, pu, s.ctypes.data_as(C.POINTER(C.c_double)),
+                                            t.ctypes.data_as(C.POINTER(C.c_double)), precision))
+        return s, t
+
+    def _eval(self, fn, args, inp, n_out, precision=None):
+        inp = np.ascontiguousarray(inp, dtype=np.float64)
+        n = inp.shape[0]
+        out = np.zeros((n, n_out), dtype=np.float64)
+        extra = () if precision is None else (precision,)
+        self._check(fn(self.h, *args, n, inp.ctypes.data_as(C.POINTER(C.c_double)),
+                       out.ctypes.data_as(C.POINTER(C.c_double)), *extra))
+        return out
+
+    def eval_table(self, table, x3, order, precision=PREC_FP64):
+        x3 = np.ascontiguousarray(x3, dtype=np.float64)
+        out = np.zeros(len(x3))
+        self._check(self.L.cm_eval_table(self.h, table, len(x3), x3.ctypes.data_as(C.POINTER(C.c_double)), order,
+                                         out.ctypes.data_as(C.POINTER(C.c_double)), precision))
+        return out
+
+    def eval_tabulated(self, msm, mech, inp, precision=PREC_FP64):
+        return self._eval(self.L.cm_eval_tabulated, (msm, mech), inp, 12, precision)
+
+    def eval_elastic(self, msm, mech, inp, precision=PREC_FP64):
+        return self._eval(self.L.cm_eval_elastic, (msm, mech), inp, 6, precision)
+
+    def eval_csd(self, msm, inp, precision=PREC_FP64):
+        return self._eval(self.L.cm_eval_csd, (msm,), inp, 3, precision)
+
+    def eval_phonon(self, msm, mech, inp, precision=PREC_FP64):
+        return self._eval(self.L.cm_eval_phonon, (msm, mech), inp, 6, precision)
+
+    def eval_shape(self, shape, p01):
+        return self._eval(self.L.cm_eval_shape, (shape,), p01, 5)
+
+    def eval_barrier(self, frm, to, inp, precision=PREC_FP64):
+        return self._eval(self.L.cm_eval_barrier, (frm, to), inp, 8, precision)
+
+    def eval_freepath(self, msm, inp, precision=PREC_FP64):
+        return self._eval(self.L.cm_eval_freepath, (msm,), inp, 1, precision)[:, 0]

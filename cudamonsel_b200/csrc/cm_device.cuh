@@ -1,0 +1,734 @@
+// cm_device.cuh -- per-event device arithmetic of the transport path.
+//
+// Templated on the compute precision R (double for the plain form, float for
+// the batched form); positions and the plane solves are double in both.
+// Units: eV, nm, 1/nm.  Each function cites the reference source it follows
+// (paths relative to CudaMONSEL/CudaMONSEL/gov/nist/).
+#pragma once
+#include <math.h>
+#include <stdint.h>
+
+#include "cm_scene.h"
+
+namespace cm {
+
+#define CM_HD __host__ __device__ __forceinline__
+#define CM_D __device__ __forceinline__
+
+// ------------------------------------------------------------ counter-based RNG
+// Philox-4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11), keyed per electron.
+struct U4 { uint32_t x, y, z, w; };
+
+CM_D U4 philox(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3, uint32_t k0, uint32_t k1) {
+  const uint32_t M0 = 0xD2511F53u, M1 = 0xCD9E8D57u, W0 = 0x9E3779B9u, W1 = 0xBB67AE85u;
+#pragma unroll
+  for (int r = 0; r < 10; ++r) {
+    uint32_t hi0 = __umulhi(M0, c0), lo0 = M0 * c0;
+    uint32_t hi1 = __umulhi(M1, c2), lo1 = M1 * c2;
+    uint32_t n0 = hi1 ^ c1 ^ k0, n2 = hi0 ^ c3 ^ k1;
+    c0 = n0; c1 = lo1; c2 = n2; c3 = lo0;
+    k0 += W0; k1 += W1;
+  }
+  return {c0, c1, c2, c3};
+}
+
+CM_HD uint64_t mix64(uint64_t z) {
+  z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ULL;
+  z = (z ^ (z >> 27)) * 0x94d049bb133111ebULL;
+  return z ^ (z >> 31);
+}
+
+// Deviate source for one event: counter (step, sub) of the electron's stream.
+// Uniforms lie in the open interval (0, 1).
+template <typename R> struct Rng;
+
+template <> struct Rng<double> {
+  uint32_t k0, k1, step, sub;
+  U4 buf;
+  int left;
+  CM_D Rng(uint64_t key, uint32_t st, uint32_t sb) : k0((uint32_t)key), k1((uint32_t)(key >> 32)), step(st), sub(sb), left(0) {}
+  CM_D double next() {
+    if (left == 0) { buf = philox(step, sub++, 0x5eedu, 0u, k0, k1); left = 2; }
+    uint32_t a, b;
+    if (left == 2) { a = buf.x; b = buf.y; } else { a = buf.z; b = buf.w; }
+    --left;
+    uint64_t x = (((uint64_t)a << 32) | b) >> 11;
+    return ((double)x + 0.5) * (1.0 / 9007199254740992.0);
+  }
+};
+
+template <> struct Rng<float> {
+  uint32_t k0, k1, step, sub;
+  U4 buf;
+  int left;
+  CM_D Rng(uint64_t key, uint32_t st, uint32_t sb) : k0((uint32_t)key), k1((uint32_t)(key >> 32)), step(st), sub(sb), left(0) {}
+  CM_D float next() {
+    if (left == 0) { buf = philox(step, sub++, 0x5eedu, 0u, k0, k1); left = 4; }
+    uint32_t a = left == 4 ? buf.x : left == 3 ? buf.y : left == 2 ? buf.z : buf.w;
+    --left;
+    return ((float)(a >> 8) + 0.5f) * (1.0f / 16777216.0f);
+  }
+};
+
+// A fixed list of deviates (the per-function parity entry points inject the oracle's)
+template <typename R> struct FixedRng {
+  const double* u;
+  int n, used;
+  CM_D R next() { R v = used < n ? (R)u[used] : R(0.5); ++used; return v; }
+};
+
+// ------------------------------------------------------------ precision helpers
+template <typename R> CM_D R msqrt(R x);
+template <> CM_D double msqrt(double x) { return sqrt(x); }
+template <> CM_D float msqrt(float x) { return sqrtf(x); }
+template <typename R> CM_D R mlog(R x);
+template <> CM_D double mlog(double x) { return log(x); }
+template <> CM_D float mlog(float x) { return logf(x); }
+template <typename R> CM_D R mexp(R x);
+template <> CM_D double mexp(double x) { return exp(x); }
+template <> CM_D float mexp(float x) { return expf(x); }
+template <typename R> CM_D R mpow(R x, R y);
+template <> CM_D double mpow(double x, double y) { return pow(x, y); }
+template <> CM_D float mpow(float x, float y) { return powf(x, y); }
+template <typename R> CM_D R macos(R x);
+template <> CM_D double macos(double x) { return acos(x); }
+template <> CM_D float macos(float x) { return acosf(x); }
+template <typename R> CM_D R matan2(R y, R x);
+template <> CM_D double matan2(double y, double x) { return atan2(y, x); }
+template <> CM_D float matan2(float y, float x) { return atan2f(y, x); }
+template <typename R> CM_D void msincos(R x, R* s, R* c);
+template <> CM_D void msincos(double x, double* s, double* c) { sincos(x, s, c); }
+template <> CM_D void msincos(float x, float* s, float* c) { sincosf(x, s, c); }
+template <typename R> CM_D R mcos(R x);
+template <> CM_D double mcos(double x) { return cos(x); }
+template <> CM_D float mcos(float x) { return cosf(x); }
+template <typename R> CM_D R mround(R x);
+template <> CM_D double mround(double x) { return round(x); }
+template <> CM_D float mround(float x) { return roundf(x); }
+template <typename R> CM_D R msinh(R x);
+template <> CM_D double msinh(double x) { return sinh(x); }
+template <> CM_D float msinh(float x) { return sinhf(x); }
+
+template <typename R> CM_D R pick4(const R* a, int k) { return k <= 0 ? a[0] : k == 1 ? a[1] : k == 2 ? a[2] : a[3]; }
+
+// ------------------------------------------------------------ uniform-grid Lagrange
+// JMONSELutils/ULagrangeInterpolation.cu:5-33, order 3; f points at 4 values.
+template <typename R> CM_D R uneville3(R f0, R f1, R f2, R f3, R x) {
+  int ns = (int)mround(x);
+  if (ns < 0) ns = 0;
+  else if (ns > 3) ns = 3;
+  R c[4] = {f0, f1, f2, f3}, d[4] = {f0, f1, f2, f3};
+  R y = pick4(c, ns--);
+  R dy = 0;
+#pragma unroll
+  for (int m = 1; m <= 3; m++) {
+#pragma unroll
+    for (int i = 0; i <= 3 - m; i++) {
+      R ho = (R)i - x;
+      R hp = (R)(i + m) - x;
+      R w = c[i + 1] - d[i];
+      d[i] = -hp * w / (R)m;
+      c[i] = -ho * w / (R)m;
+    }
+    if (2 * ns < (3 - 1 - m)) dy = pick4(c, ns + 1);
+    else dy = pick4(d, ns--);
+    y += dy;
+  }
+  return y;
+}
+
+// ULagrangeInterpolation.cu:35-48
+template <typename R> CM_D R ulagrange_d1(const R* f, int len, R x0, R xinc, R x) {
+  const R reducedx = (x - x0) / xinc;
+  int index0 = (int)reducedx - 1;
+  if (index0 < 0) index0 = 0;
+  else if (index0 > len - 4) index0 = len - 4;
+  return uneville3(f[index0], f[index0 + 1], f[index0 + 2], f[index0 + 3], reducedx - (R)index0);
+}
+
+// ULagrangeInterpolation.cu:80-103, f row-major [n0][n1]
+template <typename R> CM_D R ulagrange_d2(const R* f, int n0, int n1, R x00, R x01, R xinc0, R xinc1, R xa, R xb) {
+  const R reducedx1 = (xa - x00) / xinc0;
+  int index0 = (int)reducedx1 - 1;
+  if (index0 < 0) index0 = 0;
+  else if (index0 > n0 - 4) index0 = n0 - 4;
+  R y[4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) y[i] = ulagrange_d1(f + (size_t)(index0 + i) * n1, n1, x01, xinc1, xb);
+  // the final 1-D step runs on the 4 values with x0 moved to the window start
+  const R x0w = x00 + (R)index0 * xinc0;
+  const R reducedx = (xa - x0w) / xinc0;
+  return uneville3(y[0], y[1], y[2], y[3], reducedx);
+}
+
+// ------------------------------------------------------------ non-uniform Lagrange
+// JMONSELutils/NULagrangeInterpolation.cu:5-68
+template <typename R> CM_D void nu_locate(R x, const R* xs, int n, int order, int& first, int& nearest) {
+  int lowlim = -1, uplim = n, maxindex = n - 1;
+  bool ascending = xs[maxindex] > xs[0];
+  while ((uplim - lowlim) > 1) {
+    int mid = (uplim + lowlim) >> 1;
+    if ((x > xs[mid]) == ascending) lowlim = mid;
+    else uplim = mid;
+  }
+  if (lowlim < 0) { first = 0; nearest = 0; return; }
+  if (uplim > maxindex) { first = maxindex - order; nearest = maxindex; return; }
+  const R xl = xs[lowlim], xu = xs[uplim];
+  if (ascending) nearest = ((x - xl) <= (xu - x)) ? lowlim : uplim;
+  else nearest = ((xl - x) <= (x - xu)) ? lowlim : uplim;
+  int firstInd = lowlim, lastInd = uplim;
+  while (((lastInd - firstInd) < order) && (firstInd > 0) && (lastInd < maxindex)) {
+    if (((((xl - xs[firstInd - 1]) + xu) - xs[lastInd + 1]) >= 0) == ascending) lastInd += 1;
+    else firstInd -= 1;
+  }
+  if (lastInd >= maxindex) first = maxindex - order;
+  else if (firstInd <= 0) first = 0;
+  else first = firstInd;
+}
+
+// NULagrangeInterpolation.cu:85-112 with order 3 (4 values, their abscissae)
+template <typename R> CM_D R nu_neville3(const R* fv, const R* xv, int ns, R x) {
+  R c[4] = {fv[0], fv[1], fv[2], fv[3]}, d[4] = {fv[0], fv[1], fv[2], fv[3]};
+  R y = pick4(c, ns--);
+  R dy = 0;
+#pragma unroll
+  for (int m = 1; m <= 3; m++) {
+#pragma unroll
+    for (int i = 0; i <= 3 - m; i++) {
+      R ho = xv[i] - x;
+      R hp = xv[i + m] - x;
+      R w = c[i + 1] - d[i];
+      R den = w / (ho - hp);
+      d[i] = hp * den;
+      c[i] = ho * den;
+    }
+    if ((2 * ns) < (3 - 1 - m)) dy = pick4(c, ns + 1);
+    else dy = pick4(d, ns--);
+    y += dy;
+  }
+  return y;
+}
+
+// order-1 Neville (linear), NULagrangeInterpolation.cu:85-112 with order 1:
+// y starts at the nearest node and takes one correction (c[0] when the
+// nearest node is the first, d[0] otherwise).
+template <typename R> CM_D R nu_neville1(R f0, R f1, R x0, R x1, int ns, R x) {
+  const R ho = x0 - x, hp = x1 - x;
+  const R den = (f1 - f0) / (ho - hp);
+  return ns == 0 ? f0 + ho * den : f1 + hp * den;
+}
+
+// NULagrangeInterpolation.cu:131-147 for a 1-D table, order 1 (TabulatedInelasticSM::scatterRate)
+template <typename R> CM_D R nu_d1_order1(const R* f, const R* xs, int n, R x) {
+  int first, nearest;
+  nu_locate(x, xs, n, 1, first, nearest);
+  return nu_neville1(f[first], f[first + 1], xs[first], xs[first + 1], nearest - first, x);
+}
+
+// d1 of order 3 on a small 4-point array (the last step of d2/d3)
+template <typename R> CM_D R nu_d1_4(const R* fv, const R* xv, R x) {
+  int first, nearest;
+  nu_locate(x, xv, 4, 3, first, nearest);
+  // first is always 0 for a 4-point array
+  return nu_neville3(fv, xv, nearest - first, x);
+}
+
+// NULagrangeInterpolation.cu:169-192 on a 2-D table (order 3)
+template <typename R> CM_D R nu_d2(const R* f, const R* xs0, int n0, const R* xs1, int n1, R xa, R xb) {
+  int i0, near0;
+  nu_locate(xa, xs0, n0, 3, i0, near0);
+  int j0, near1;
+  nu_locate(xb, xs1, n1, 3, j0, near1);
+  R xv1[4] = {xs1[j0], xs1[j0 + 1], xs1[j0 + 2], xs1[j0 + 3]};
+  R y[4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const R* row = f + (size_t)(i0 + i) * n1 + j0;
+    R fv[4] = {row[0], row[1], row[2], row[3]};
+    y[i] = nu_neville3(fv, xv1, near1 - j0, xb);
+  }
+  R xv0[4] = {xs0[i0], xs0[i0 + 1], xs0[i0 + 2], xs0[i0 + 3]};
+  return nu_d1_4(y, xv0, xa);
+}
+
+// NULagrangeInterpolation.cu:215-240 on a 3-D table (order 3).  The reference's
+// final 1-D step uses xsamp[0][0..3] (line 236) whatever the window; `fixes`
+// uses the window's own abscissae.
+template <typename R> CM_D R nu_d3(const R* f, const R* xs0, int n0, const R* xs1, int n1, const R* xs2, int n2, R xa, R xb,
+                                   R xc, bool fixes) {
+  int i0, near0, j0, near1, k0, near2;
+  nu_locate(xa, xs0, n0, 3, i0, near0);
+  nu_locate(xb, xs1, n1, 3, j0, near1);
+  nu_locate(xc, xs2, n2, 3, k0, near2);
+  R xv1[4] = {xs1[j0], xs1[j0 + 1], xs1[j0 + 2], xs1[j0 + 3]};
+  R xv2[4] = {xs2[k0], xs2[k0 + 1], xs2[k0 + 2], xs2[k0 + 3]};
+  R y[4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    R z[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const R* row = f + ((size_t)(i0 + i) * n1 + (j0 + j)) * n2 + k0;
+      R fv[4] = {row[0], row[1], row[2], row[3]};
+      z[j] = nu_neville3(fv, xv2, near2 - k0, xc);
+    }
+    y[i] = nu_d1_4(z, xv1, xb);
+  }
+  const int base = fixes ? i0 : 0;
+  R xv0[4] = {xs0[base], xs0[base + 1], xs0[base + 2], xs0[base + 3]};
+  return nu_d1_4(y, xv0, xa);
+}
+
+// NUTableInterpolation::interpolate (JMONSEL/NUTableInterpolation.cu:98-115)
+template <typename R> CM_D R table_interp(const SceneView<R>& s, int t, R x0, R x1, R x2, int order) {
+  const Table& tb = s.tables[t];
+  const R* v = s.blob + tb.off_v;
+  if (tb.dim == 1) {
+    if (order == 1) return nu_d1_order1(v, s.blob + tb.off_x[0], tb.n[0], x0);
+    int first, nearest;
+    const R* xs = s.blob + tb.off_x[0];
+    nu_locate(x0, xs, tb.n[0], 3, first, nearest);
+    R fv[4] = {v[first], v[first + 1], v[first + 2], v[first + 3]};
+    R xv[4] = {xs[first], xs[first + 1], xs[first + 2], xs[first + 3]};
+    return nu_neville3(fv, xv, nearest - first, x0);
+  }
+  if (tb.dim == 2) return nu_d2(v, s.blob + tb.off_x[0], tb.n[0], s.blob + tb.off_x[1], tb.n[1], x0, x1);
+  return nu_d3(v, s.blob + tb.off_x[0], tb.n[0], s.blob + tb.off_x[1], tb.n[1], s.blob + tb.off_x[2], tb.n[2], x0, x1, x2,
+               (s.options & 1) != 0);
+}
+
+// ------------------------------------------------------------ elastic scattering
+// EPQLibrary/BrowningEmpiricalCrossSection.cu:24-29, sigma in m^2, E in eV
+template <typename R> CM_D R browning_sigma(const Mott& m, R E) {
+  const R e = E / R(1000);
+  const R re = msqrt(e);
+  const R z17 = (R)m.zp17;
+  return R(3.0e-22) * z17 / (e + R(0.005) * z17 * re + R(0.0007) * (R)m.zp2 / re);
+}
+
+// BrowningEmpiricalCrossSection.cu:31-45.  The reference reads z through a
+// reference bound to a temporary Element (BrowningEmpiricalCrossSection.cuh:20,
+// instances built from ints at BrowningEmpiricalCrossSection.cu:47-...); the
+// compiled reference reads 0, so r/(r+1) is NaN and every angle is isotropic.
+// `fixes` uses the element's atomic number.
+template <typename R, typename G> CM_D R browning_angle(const Mott& m, R E, G& g, bool fixes) {
+  const R r1 = g.next(), r2 = g.next();
+  if (!fixes) return macos(1 - R(2.0) * r2);
+  const R z = (R)m.Z;
+  const R e = E / R(1000);
+  const R r = (R(300.0) * e / z) + ((R)m.zp3 / (R(3.0e5) * e));
+  if (r1 <= r / (r + 1)) {
+    const R alpha = R(7.0e-3) / e;
+    return macos(R(1.0) - ((R(2.0) * alpha * r2) / (alpha - r2 + 1)));
+  }
+  return macos(1 - R(2.0) * r2);
+}
+
+// JMONSEL/NISTMottRS.cu:103-119 times the SelectableElasticSM rate factor (1/nm)
+template <typename R> CM_D R nistmott_rate(const SceneView<R>& s, const Mott& m, R kel, R kbrown, R E, R logE) {
+  if (E < (R)m.extrapolateBelowEnergy) return (R)m.sfBrowning * browning_sigma(m, E) * kbrown;
+  if (E < (R)s.maxMott) {
+    return kel * ulagrange_d1(s.blob + m.off_spwem, 61, (R)s.dl50, (R)s.param, logE);
+  }
+  // ScreenedRutherfordScatteringAngle.cu:24-30
+  return (R)m.rutherfordA / (E + (R)m.rutherfordB) * kbrown;
+}
+
+// NISTMottRS.cu:121-154
+template <typename R, typename G> CM_D R nistmott_angle(const SceneView<R>& s, const Mott& m, R E, G& g) {
+  if (E < (R)m.extrapolateBelowEnergy) return browning_angle(m, E, g, (s.options & 1) != 0);
+  if (E < (R)s.maxMott) {
+    const R lg = mlog(E);
+    const R u = g.next();
+    const R q = ulagrange_d2(s.blob + m.off_x1, 61, 201, (R)s.dl50, R(0), (R)s.param, R(0.005), lg, u);
+    const R com = R(1.0) - (R(2.0) * q * q);
+    return com > R(-1.0) ? (com < R(1.0) ? macos(com) : R(0)) : R(kPi);
+  }
+  // ScreenedRutherfordScatteringAngle.cu:32-39
+  const R alpha = (R)m.rutherfordAlpha / E;
+  const R r = g.next();
+  return macos(1 - R(2.0) * alpha * r / (1 + alpha - r));
+}
+
+// ------------------------------------------------------------ direction algebra
+// Electron::updateDirection (NISTMonte/Electron.cu:111-131) on a unit vector.
+// When the direction is exactly along z the reference's phi is 0 for every
+// electron that reaches here with sin(theta) == 0, so cp = 1, sp = 0.
+template <typename R> CM_D void update_dir(R d[3], R dTheta, R dPhi) {
+  const R ct = d[2];
+  const R st = msqrt(d[0] * d[0] + d[1] * d[1]);
+  R cp = 1, sp = 0;
+  if (st > 0) { cp = d[0] / st; sp = d[1] / st; }
+  R sa, ca, sb, cb;
+  msincos(dTheta, &sa, &ca);
+  msincos(dPhi, &sb, &cb);
+  const R xx = (cb * ct * sa) + (ca * st);
+  const R yy = sa * sb;
+  const R dx = (cp * xx) - (sp * yy);
+  const R dy = (cp * yy) + (sp * xx);
+  const R dz = (ca * ct) - (cb * sa * st);
+  const R inv = R(1) / msqrt(dx * dx + dy * dy + dz * dz);
+  d[0] = dx * inv; d[1] = dy * inv; d[2] = dz * inv;
+}
+
+template <typename R> CM_D void dir_from_angles(R d[3], R theta, R phi) {
+  R st, ct, sp, cp;
+  msincos(theta, &st, &ct);
+  msincos(phi, &sp, &cp);
+  d[0] = st * cp; d[1] = st * sp; d[2] = ct;
+}
+
+// ------------------------------------------------------------ slowing down
+// JMONSEL/JoyLuoNieminenCSD.cu:91-121; the recursive halving is run with an
+// explicit stack in the same order (first half, then second half at the
+// energy reached after the first).
+template <typename R> CM_D R jln_compute(const Jln& c, R len, R kE) {
+  if ((c.nce == 0) || (kE < (R)c.minE) || (kE <= R(0))) return 0;
+  if (kE <= (R)c.breakE) return (kE / mpow(R(1) + (R(1.5) * (R)c.gamma * len * kE * msqrt(kE)), R(2) / R(3))) - kE;
+  R stack[48];
+  int sp = 0;
+  stack[sp++] = len;
+  R total = 0;
+  while (sp > 0) {
+    const R l = stack[--sp];
+    const R e = kE + total;
+    if ((e < (R)c.minE) || (e <= R(0))) continue;
+    if (e <= (R)c.breakE) {
+      total += (e / mpow(R(1) + (R(1.5) * (R)c.gamma * l * e * msqrt(e)), R(2) / R(3))) - e;
+      continue;
+    }
+    R loss = 0;
+    for (int i = 0; i < c.nce; i++) loss += (R)c.coef[i] * mlog(((R)c.recipJ[i] * e) + (R)c.beta[i]);
+    loss *= l / e;
+    if (loss <= (R(0.1) * e) || sp >= 46) { total += -loss; continue; }
+    stack[sp++] = l / 2;   // second half, processed after the first
+    stack[sp++] = l / 2;   // first half
+  }
+  return total;
+}
+
+// ------------------------------------------------------------ mechanism rates
+// TabulatedInelasticSM.cu:436-459
+template <typename R> CM_D R tabulated_rate(const SceneView<R>& s, const Mech& k, R E) {
+  const R kEa = E + (R)k.energyOffset;
+  if (kEa < (R)k.iimfpDomain0) return 0;
+  return (R)k.rateMult * table_interp(s, k.tIIMFP, kEa, R(0), R(0), 1);
+}
+
+// GanachaudMokraniPhononInelasticSM.cu:46-72
+template <typename R> CM_D R phonon_rate(const Mech& k, R kE) {
+  const R pe = (R)k.phononE;
+  if (kE < pe) return 0;
+  const R x = pe / kE;
+  if (x < R(0.1)) return (R)k.prefactor * x * mlog(R(4) / x);
+  if (x >= R(1)) return 0;
+  const R t = msqrt(R(1) - x);
+  return (R)k.prefactor * x * mlog((R(1) + t) / (R(1) - t));
+}
+
+// ------------------------------------------------------------ geometry (double)
+struct NV { double n[3]; double u; };
+
+CM_D NV nv_none() { NV r; r.n[0] = r.n[1] = r.n[2] = 0.; r.u = INFINITY; return r; }
+
+// NormalMultiPlaneShape.cu:26-38
+CM_D bool tie_break(const double* n) {
+  if (n[0] < 0.) return false;
+  if (n[0] == 0.) {
+    if (n[1] < 0.) return false;
+    if (n[1] == 0.)
+      if (n[2] < 0.) return false;
+  }
+  return true;
+}
+
+// NormalMultiPlaneShape.cu:40-171
+CM_D NV planes_first_normal(const Plane* pl, int np, const double* p0, const double* p1) {
+  double umin = -INFINITY, umax = INFINITY;
+  int minindex = -1, maxindex = -1;
+  const double delta[3] = {p1[0] - p0[0], p1[1] - p0[1], p1[2] - p0[2]};
+  for (int i = 0; i < np; i++) {
+    const Plane& P = pl[i];
+    const double pmc[3] = {p0[0] - P.p[0], p0[1] - P.p[1], p0[2] - P.p[2]};
+    const double num = (pmc[0] * P.n[0]) + (pmc[1] * P.n[1]) + (pmc[2] * P.n[2]);
+    const double den = (delta[0] * P.n[0]) + (delta[1] * P.n[1]) + (delta[2] * P.n[2]);
+    if (den == 0) {
+      if ((num < 0) || ((num == 0) && tie_break(P.n))) continue;
+      return nv_none();
+    }
+    const double u = -num / den;
+    if (den > 0) {
+      if (u < umax) {
+        if ((u < 0) || (u <= umin)) return nv_none();
+        umax = u;
+        maxindex = i;
+      }
+    } else if (u > umin) {
+      if ((u > 1) || (u >= umax)) return nv_none();
+      umin = u;
+      minindex = i;
+    }
+  }
+  NV r;
+  if (umin > 0) {
+    r.u = umin;
+    r.n[0] = pl[minindex].n[0]; r.n[1] = pl[minindex].n[1]; r.n[2] = pl[minindex].n[2];
+    return r;
+  }
+  if ((umax <= 1) && (umax > 0.)) {
+    r.u = umax;
+    r.n[0] = pl[maxindex].n[0]; r.n[1] = pl[maxindex].n[1]; r.n[2] = pl[maxindex].n[2];
+    return r;
+  }
+  return nv_none();
+}
+
+// MultiPlaneShape.cu:23-27 (Plane::contains)
+CM_D bool plane_contains(const Plane& P, const double* p) {
+  return (((p[0] - P.p[0]) * P.n[0] + (p[1] - P.p[1]) * P.n[1] + (p[2] - P.p[2]) * P.n[2]) <= 0.0);
+}
+
+// NormalMultiPlaneShape.cu:178-204.  The reference writes delta[0] three times
+// and leaves delta[1], delta[2] unset; they are 0 here.
+CM_D bool planes_contains2(const Plane* pl, int np, const double* p0, const double* p1) {
+  bool didDelta = false;
+  double delta[3] = {0., 0., 0.};
+  for (int i = 0; i < np; i++) {
+    const Plane& P = pl[i];
+    const double p0c[3] = {p0[0] - P.p[0], p0[1] - P.p[1], p0[2] - P.p[2]};
+    const double dn = (p0c[0] * P.n[0]) + (p0c[1] * P.n[1]) + (p0c[2] * P.n[2]);
+    if (dn > 0.) return false;
+    if (dn == 0.) {
+      if (!didDelta) {
+        delta[0] = p1[2] - p0[2];
+        didDelta = true;
+      }
+      const double dd = (delta[0] * P.n[0]) + (delta[1] * P.n[1]) + (delta[2] * P.n[2]);
+      if (dd > 0.) return false;
+      if ((dd == 0.) && !tie_break(P.n)) return false;
+    }
+  }
+  return true;
+}
+
+// Sphere.cu:11-14
+CM_D bool sphere_contains(const Shape& sh, const double* p) {
+  const double a = p[0] - sh.c[0], b = p[1] - sh.c[1], c = p[2] - sh.c[2];
+  return a * a + b * b + c * c <= sh.r * sh.r;
+}
+
+// Sphere.cu:21-45
+CM_D double sphere_first_intersection(const Shape& sh, const double* p0, const double* p1) {
+  const double d[3] = {p1[0] - p0[0], p1[1] - p0[1], p1[2] - p0[2]};
+  const double m[3] = {p0[0] - sh.c[0], p0[1] - sh.c[1], p0[2] - sh.c[2]};
+  const double ma2 = -2.0 * (d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+  const double b = 2.0 * (m[0] * d[0] + m[1] * d[1] + m[2] * d[2]);
+  const double c2 = 2.0 * ((m[0] * m[0] + m[1] * m[1] + m[2] * m[2]) - sh.r * sh.r);
+  const double f = b * b + ma2 * c2;
+  if (f >= 0) {
+    const double sf = sqrt(f);
+    double up = (b + sf) / ma2, un = (b - sf) / ma2;
+    if (up < 0.0) up = INFINITY;
+    if (un < 0.0) un = INFINITY;
+    return fmin(up, un);
+  }
+  return INFINITY;
+}
+
+template <typename R> CM_D bool shape_contains(const SceneView<R>& s, int id, const double* p) {
+  // shapes form a binary tree of intersections over plane sets; walk it with a small stack
+  int stack[2 * kMaxShapeDepth + 2];
+  int sp = 0;
+  stack[sp++] = id;
+  while (sp > 0) {
+    const Shape& sh = s.shapes[stack[--sp]];
+    if (sh.kind == SHAPE_PLANES) {
+      for (int i = 0; i < sh.np; ++i)
+        if (!plane_contains(s.planes[sh.plane0 + i], p)) return false;
+    } else if (sh.kind == SHAPE_INTERSECTION) {
+      stack[sp++] = sh.b;
+      stack[sp++] = sh.a;
+    } else if (sh.kind == SHAPE_SPHERE) {
+      if (!sphere_contains(sh, p)) return false;
+    }
+  }
+  return true;
+}
+
+template <typename R> CM_D bool shape_contains2(const SceneView<R>& s, int id, const double* p0, const double* p1) {
+  int stack[2 * kMaxShapeDepth + 2];
+  int sp = 0;
+  stack[sp++] = id;
+  while (sp > 0) {
+    const Shape& sh = s.shapes[stack[--sp]];
+    if (sh.kind == SHAPE_PLANES) {
+      if (!planes_contains2(s.planes + sh.plane0, sh.np, p0, p1)) return false;
+    } else if (sh.kind == SHAPE_INTERSECTION) {
+      stack[sp++] = sh.b;
+      stack[sp++] = sh.a;
+    } else if (sh.kind == SHAPE_SPHERE) {
+      if (!sphere_contains(sh, p0)) return false;
+    }
+  }
+  return true;
+}
+
+template <typename R, int D> struct FirstNormal;
+
+// NormalIntersectionShape.cu:19-239
+template <typename R, int D> __device__ __noinline__ NV inter_first_normal(const SceneView<R>& s, const Shape& sh, const double* pos0,
+                                                                           const double* pos1) {
+  const NV none = nv_none();
+  int adepth, bdepth;
+  double u;
+  const double delta[3] = {pos1[0] - pos0[0], pos1[1] - pos0[1], pos1[2] - pos0[2]};
+  NV nva = FirstNormal<R, D - 1>::eval(s, sh.a, pos0, pos1);
+  if (nva.u <= 1.) adepth = ((delta[0] * nva.n[0]) + (delta[1] * nva.n[1]) + (delta[2] * nva.n[2])) > 0 ? 1 : 0;
+  else {
+    if (!shape_contains2(s, sh.a, pos0, pos1)) return none;
+    adepth = 1;
+  }
+  NV nvb = FirstNormal<R, D - 1>::eval(s, sh.b, pos0, pos1);
+  if (nvb.u <= 1.) bdepth = ((delta[0] * nvb.n[0]) + (delta[1] * nvb.n[1]) + (delta[2] * nvb.n[2])) > 0 ? 1 : 0;
+  else {
+    if (!shape_contains2(s, sh.b, pos0, pos1)) return none;
+    if (adepth == 1) return nva;
+    bdepth = 1;
+  }
+  int cdepth = adepth + bdepth;
+  const double EXTRAU = 1.e-10;
+  for (int guard = 0; guard < 4096; ++guard) {
+    if (nva.u < nvb.u) {
+      if (bdepth == 1) return nva;
+      cdepth ^= 1;
+      u = nva.u + EXTRAU;
+      const double tmp[3] = {pos0[0] + (u * delta[0]), pos0[1] + (u * delta[1]), pos0[2] + (u * delta[2])};
+      nva = FirstNormal<R, D - 1>::eval(s, sh.a, tmp, pos1);
+      if (nva.u < INFINITY) nva.u = (nva.u * (1. - u)) + u;
+      if (nva.u > 1) return cdepth == 0 ? none : nvb;
+      adepth ^= 1;
+    } else if (nva.u > nvb.u) {
+      if (adepth == 1) return nvb;
+      cdepth ^= 1;
+      u = nvb.u + EXTRAU;
+      const double tmp[3] = {pos0[0] + (u * delta[0]), pos0[1] + (u * delta[1]), pos0[2] + (u * delta[2])};
+      nvb = FirstNormal<R, D - 1>::eval(s, sh.b, tmp, pos1);
+      if (nvb.u < INFINITY) nvb.u = (nvb.u * (1. - u)) + u;
+      if (nvb.u > 1) return cdepth == 0 ? none : nva;
+      bdepth ^= 1;
+    } else {
+      const int depthchange = (((adepth ^ 1) - adepth) + (bdepth ^ 1)) - bdepth;
+      if (depthchange == 0) {
+        u = nva.u + EXTRAU;
+        const double t1[3] = {pos0[0] + (u * delta[0]), pos0[1] + (u * delta[1]), pos0[2] + (u * delta[2])};
+        nva = FirstNormal<R, D - 1>::eval(s, sh.a, t1, pos1);
+        if (nva.u < INFINITY) nva.u = (nva.u * (1. - u)) + u;
+        u = nvb.u + EXTRAU;
+        const double t2[3] = {pos0[0] + (u * delta[0]), pos0[1] + (u * delta[1]), pos0[2] + (u * delta[2])};
+        nvb = FirstNormal<R, D - 1>::eval(s, sh.b, t2, pos1);
+        if (nvb.u < INFINITY) nvb.u = (nvb.u * (1. - u)) + u;
+        if (nva.u > 1) return adepth == 0 ? nvb : none;
+        if (nvb.u > 1) return bdepth == 0 ? nva : none;
+        adepth ^= 1;
+        bdepth ^= 1;
+      } else {
+        NV r;
+        r.n[0] = (nva.n[0] + nvb.n[0]) / 2.;
+        r.n[1] = (nva.n[1] + nvb.n[1]) / 2.;
+        r.n[2] = (nva.n[2] + nvb.n[2]) / 2.;
+        r.u = nva.u;
+        return r;
+      }
+    }
+  }
+  return none;
+}
+
+template <typename R, int D> struct FirstNormal {
+  static CM_D NV eval(const SceneView<R>& s, int id, const double* p0, const double* p1) {
+    const Shape& sh = s.shapes[id];
+    if (sh.kind == SHAPE_PLANES) return planes_first_normal(s.planes + sh.plane0, sh.np, p0, p1);
+    if (sh.kind == SHAPE_INTERSECTION) return inter_first_normal<R, D>(s, sh, p0, p1);
+    NV r = nv_none();
+    if (sh.kind == SHAPE_SPHERE) r.u = sphere_first_intersection(sh, p0, p1);
+    return r;
+  }
+};
+
+template <typename R> struct FirstNormal<R, 0> {
+  static CM_D NV eval(const SceneView<R>& s, int id, const double* p0, const double* p1) {
+    const Shape& sh = s.shapes[id];
+    if (sh.kind == SHAPE_PLANES) return planes_first_normal(s.planes + sh.plane0, sh.np, p0, p1);
+    NV r = nv_none();
+    if (sh.kind == SHAPE_SPHERE) r.u = sphere_first_intersection(sh, p0, p1);
+    return r;
+  }
+};
+
+template <typename R> CM_D NV shape_first_normal(const SceneView<R>& s, int id, const double* p0, const double* p1) {
+  return FirstNormal<R, kMaxShapeDepth>::eval(s, id, p0, p1);
+}
+
+// RegionBase.cu:50-60, iterative: the first child whose shape holds p owns it
+template <typename R> CM_D int containing_subregion(const SceneView<R>& s, int reg, const double* p) {
+  if (!shape_contains(s, s.regions[reg].shape, p)) return -1;
+  for (int depth = 0; depth < 64; ++depth) {
+    const Region& r = s.regions[reg];
+    int found = -1;
+    for (int i = 0; i < r.nchild; ++i) {
+      const int c = s.children[r.child0 + i];
+      if (shape_contains(s, s.regions[c].shape, p)) { found = c; break; }
+    }
+    if (found < 0) return reg;
+    reg = found;
+  }
+  return reg;
+}
+
+template <typename R> CM_D bool is_containing_region(const SceneView<R>& s, int reg, int target) {
+  // target lies below reg iff walking up from target reaches reg
+  int t = s.regions[target].parent;
+  for (int depth = 0; depth < 64 && t >= 0; ++depth) {
+    if (t == reg) return true;
+    t = s.regions[t].parent;
+  }
+  return false;
+}
+
+// RegionBase.cu:74-119.  p1 is clipped to the boundary; returns the region just
+// over it (-1: outside the chamber) and the struck boundary's normal.
+template <typename R> CM_D int find_end_of_step(const SceneView<R>& s, int reg, const double* p0, double* p1, double* hitn) {
+  const Region& r = s.regions[reg];
+  int base = reg;
+  NV nv = shape_first_normal(s, r.shape, p0, p1);
+  double t = nv.u;
+  hitn[0] = nv.n[0]; hitn[1] = nv.n[1]; hitn[2] = nv.n[2];
+  if ((t <= 1.0) && r.parent >= 0) base = r.parent;
+  for (int i = 0; i < r.nchild; ++i) {
+    const int c = s.children[r.child0 + i];
+    NV cn = shape_first_normal(s, s.regions[c].shape, p0, p1);
+    if ((cn.u <= 1.0) && (cn.u < t)) {
+      t = cn.u;
+      base = c;
+      hitn[0] = cn.n[0]; hitn[1] = cn.n[1]; hitn[2] = cn.n[2];
+    }
+  }
+  if (t <= 1.0) {
+    const double delta[3] = {p1[0] - p0[0], p1[1] - p0[1], p1[2] - p0[2]};
+    p1[0] = p0[0] + (t * delta[0]);
+    p1[1] = p0[1] + (t * delta[1]);
+    p1[2] = p0[2] + (t * delta[2]);
+    const double mag = sqrt(delta[0] * delta[0] + delta[1] * delta[1] + delta[2] * delta[2]);
+    const double over[3] = {p1[0] + kSmallDispNm * (delta[0] / mag), p1[1] + kSmallDispNm * (delta[1] / mag),
+                            p1[2] + kSmallDispNm * (delta[2] / mag)};
+    for (int depth = 0; depth < 64 && base >= 0; ++depth) {
+      const int res = containing_subregion(s, base, over);
+      if (res >= 0) return res;
+      base = s.regions[base].parent;
+    }
+    return -1;
+  }
+  return reg;
+}
+
+}  // namespace cm

@@ -1,0 +1,1717 @@
+// cm_engine.cu -- wavefront electron-transport engine for sm_100a and its C ABI.
+//
+// Replaces MonteCarloSS::runMultipleTrajectories (NISTMonte/MonteCarloSS.cu:
+// 107-231) for a batch of beam landing points.  One "wave" of live electrons
+// is kept as structure-of-arrays in HBM.  Each iteration runs
+//
+//   flight   : region check, scatter rates, free path, boundary search, CSD
+//              loss, escape tally; classifies every electron's step end and
+//              appends it (warp-aggregated) to one event queue
+//   elastic  : SelectableElasticSM/NISTMottRS events
+//   inelastic: TabulatedInelasticSM events (secondaries -> pool)
+//   misc     : barrier crossings, FittedInelSM, phonon, pass-through
+//   spawn    : refill the next wave from the secondary pool, then primaries
+//   tail     : swap counters
+//
+// Survivors of every event kernel are appended compactly into the other wave
+// buffer, so the next flight reads fully coalesced SoA.  Every electron draws
+// from its own Philox stream (key = primary or parent lineage, counter =
+// step), so results do not depend on scheduling or on what else is in the wave.
+#include <cooperative_groups.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/cudamonsel_b200.h"
+#include "cm_physics.cuh"
+
+namespace cg = cooperative_groups;
+
+namespace cm {
+
+// ------------------------------------------------------------------ units
+static const double kEV = 1.60217653e-19;          // PhysicalConstants::ElectronCharge
+static const double kFromSIeV = 1.0 / 1.60217653e-19;  // FromSI::EV
+static const double kToSIkeV = 1.60217653e-19 * 1.0e3;
+static const double kBohr = 5.291772083e-11;
+static const double kAvogadro = 6.0221415e23;
+static const double kBoltzmann = 1.3806505e-23;
+static const double kElectronMass = 9.1093826e-31;
+static const double kHbar = 1.05457266e-34;
+
+static thread_local std::string g_err;
+
+static int fail(int code, const std::string& msg) {
+  g_err = msg;
+  return code;
+}
+
+#define CM_CUDA(call)                                                                            \
+  do {                                                                                           \
+    cudaError_t _e = (call);                                                                     \
+    if (_e != cudaSuccess) return fail(CM_ECUDA, std::string(#call) + ": " + cudaGetErrorString(_e)); \
+  } while (0)
+
+// ------------------------------------------------------------------ host scene registry (SI)
+struct HTable {
+  int dim;
+  int n[3];
+  std::vector<double> x[3];
+  std::vector<double> v;
+  double domain[3][2];
+  double range[2];
+  int role;  // 0 none, 1 IIMFP, 2 reduced dE, 3 theta, 4 SE E0
+};
+
+struct HMaterial {
+  std::vector<int> Z;
+  std::vector<double> A, wf, core;
+  double density, workfunction, ecb, bandgap;
+};
+
+struct HMech {
+  int kind;
+  int method;
+  double energyOffset;
+  int tables[4];
+  double energySEgen, breakE;
+  double ratemult, phononE, temperature, eps0, epsInf;
+  double prefactor, extinction;
+};
+
+struct HMsm {
+  int material;
+  std::vector<HMech> mechs;
+  int csd;
+  double breakE;
+  bool minSet;
+  double minE;
+  int classical;
+  double lambda;
+};
+
+struct HShape {
+  int kind;
+  double c[3], r;
+  std::vector<double> n, p;  // planes
+  int a, b;
+};
+
+struct HRegion {
+  int parent, msm, shape;
+  std::vector<int> children;
+};
+
+struct HMott {
+  std::vector<double> spwem, x1;
+};
+
+template <typename R>
+struct DevScene {
+  std::vector<void*> allocs;
+  SceneView<R> view;
+  bool valid = false;
+  void release() {
+    for (void* p : allocs) cudaFree(p);
+    allocs.clear();
+    valid = false;
+  }
+};
+
+template <typename R>
+struct Wave {
+  double *px, *py, *pz;
+  R *dx, *dy, *dz;
+  R *E, *Ep;
+  int *region, *pixel, *aux;
+  uint32_t* step;
+  unsigned long long* key;
+  R *hx, *hy, *hz;
+};
+
+struct Counters {
+  int n[2];
+  int pool;
+  int q[3];
+  int error;
+  int done;
+  unsigned long long next_primary, total_primaries;
+  unsigned long long steps, scatters, barriers, escapes, secondaries;
+  unsigned long long iterations;
+};
+
+template <typename R>
+struct RunBuffers {
+  int cap = 0, poolCap = 0;
+  std::vector<void*> allocs;
+  Wave<R> w[2], pool;
+  int* q[3] = {nullptr, nullptr, nullptr};
+  void release() {
+    for (void* p : allocs) cudaFree(p);
+    allocs.clear();
+    cap = poolCap = 0;
+  }
+};
+
+}  // namespace cm
+
+using namespace cm;
+
+struct cm_context {
+  int device = 0;
+  int options = 0;
+  int nsm = 148;
+  std::map<int, HMott> mott;
+  std::vector<HTable> tables;
+  std::vector<HMaterial> mats;
+  std::vector<HMsm> msms;
+  std::vector<HShape> shapes;
+  std::vector<HRegion> regions;
+  DevScene<double> d64;
+  DevScene<float> d32;
+  RunBuffers<double> rb64;
+  RunBuffers<float> rb32;
+  Counters* counters = nullptr;
+  Counters* counters_host = nullptr;
+  cudaStream_t stream = nullptr;
+  void dirty() {
+    d64.release();
+    d32.release();
+  }
+};
+
+// ------------------------------------------------------------------ scene upload
+namespace cm {
+
+template <typename T>
+static int dev_copy(std::vector<void*>& allocs, const std::vector<T>& v, const T** out) {
+  void* p = nullptr;
+  size_t bytes = std::max<size_t>(1, v.size()) * sizeof(T);
+  CM_CUDA(cudaMalloc(&p, bytes));
+  allocs.push_back(p);
+  if (!v.empty()) CM_CUDA(cudaMemcpy(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+  *out = (const T*)p;
+  return 0;
+}
+
+// JoyLuoNieminenCSD::init (JMONSEL/JoyLuoNieminenCSD.cu:42-82) in SI, converted to eV/nm
+static Jln make_jln(const HMaterial& mt, double breakE) {
+  Jln c;
+  memset(&c, 0, sizeof(c));
+  c.nce = (int)mt.Z.size();
+  double bh = -mt.ecb;
+  c.minE = bh * kFromSIeV;
+  if (c.nce == 0) return c;
+  double bhplus1eV = bh + kEV * 1.;
+  if (breakE < bhplus1eV) breakE = bhplus1eV;
+  double gamma = 0.;
+  for (int i = 0; i < c.nce; ++i) {
+    double z = mt.Z[i];
+    double J = mt.Z[i] < 13 ? kEV * (11.5 * z) : kEV * (9.76 * z + 58.8 * pow(z, -0.19));
+    double recipJ = 1.166 / J;
+    double beta = 1. - (recipJ * bhplus1eV);
+    double coef = 2.01507E-28 * mt.density * mt.wf[i] * mt.Z[i] / mt.A[i];
+    gamma += coef * log((recipJ * breakE) + beta);
+    c.coef[i] = coef * 1e-9 / (kEV * kEV);
+    c.recipJ[i] = recipJ * kEV;
+    c.beta[i] = beta;
+  }
+  gamma /= pow(breakE, 3.5);
+  c.gamma = gamma * 1e-9 * pow(kEV, 1.5);
+  c.breakE = breakE * kFromSIeV;
+  return c;
+}
+
+static double efermi(const HMaterial& m) { return -m.ecb - m.workfunction; }
+
+// NISTMottRS constructor members (JMONSEL/NISTMottRS.cu:76-91), method 1, SI
+static void mott_constants(int Z, const HMott& hm, Mott& m) {
+  m.Z = Z;
+  m.zp17 = pow(Z, 1.7);
+  m.zp2 = pow(Z, 2.0);
+  m.zp3 = pow(Z, 3.0);
+  const double ext = kEV * 50.;
+  const double dl50 = log(0.050 * kToSIkeV);
+  const double param = (log(20.0 * kToSIkeV) - dl50) / 60.0;
+  // ULagrangeInterpolation::d1 at the extrapolation energy, in double on the host
+  const double x = log(ext);
+  const double reducedx = (x - dl50) / param;
+  int index0 = (int)reducedx - 1;
+  if (index0 < 0) index0 = 0;
+  if (index0 > 61 - 4) index0 = 61 - 4;
+  double xx = reducedx - index0;
+  const double* f = hm.spwem.data() + index0;
+  int ns = (int)round(xx);
+  if (ns < 0) ns = 0;
+  else if (ns > 3) ns = 3;
+  double c[4] = {f[0], f[1], f[2], f[3]}, d[4] = {f[0], f[1], f[2], f[3]};
+  double y = c[ns--], dy = 0;
+  for (int mm = 1; mm <= 3; mm++) {
+    for (int i = 0; i <= 3 - mm; i++) {
+      double ho = i - xx, hp = i + mm - xx, w = c[i + 1] - d[i];
+      d[i] = -hp * w / mm;
+      c[i] = -ho * w / mm;
+    }
+    dy = (2 * ns < (3 - 1 - mm)) ? c[ns + 1] : d[ns--];
+    y += dy;
+  }
+  const double mottXS = (kBohr * kBohr) * y;
+  const double e = ext * (1.0 / (1.60217653e-19 * 1.0e3));
+  const double re = sqrt(e);
+  const double browning = 3.0e-22 * m.zp17 / (e + 0.005 * m.zp17 * re + 0.0007 * m.zp2 / re);
+  m.sfBrowning = mottXS / browning;
+  m.extrapolateBelowEnergy = ext * kFromSIeV;
+  const double zz = Z;
+  const double zp = pow(zz, 1.0 / 3.0);
+  m.rutherfordA = 7.670843088080456e-38 * zp * (1.0 + zz) * kFromSIeV;
+  m.rutherfordB = 5.44967975966321e-19 * zp * zp * kFromSIeV;
+  m.rutherfordAlpha = 5.44968e-19 * pow(Z, 2.0 / 3.0) * kFromSIeV;
+}
+
+template <typename R>
+static int build_scene(cm_context* ctx, DevScene<R>& ds) {
+  if (ds.valid) return 0;
+  ds.release();
+  std::vector<R> blob;
+  // tables, converted by role to eV / nm units
+  std::vector<Table> tabs;
+  for (auto& t : ctx->tables) {
+    Table d;
+    memset(&d, 0, sizeof(d));
+    d.dim = t.dim;
+    const double ax0 = (t.role >= 1) ? kFromSIeV : 1.0;
+    const double vf = t.role == 1 ? 1e-9 : t.role == 4 ? kFromSIeV : 1.0;
+    for (int k = 0; k < t.dim; ++k) {
+      d.n[k] = t.n[k];
+      d.off_x[k] = (int)blob.size();
+      const double f = k == 0 ? ax0 : 1.0;
+      for (double v : t.x[k]) blob.push_back((R)(v * f));
+      d.domain[k][0] = t.domain[k][0] * f;
+      d.domain[k][1] = t.domain[k][1] * f;
+    }
+    d.off_v = (int)blob.size();
+    for (double v : t.v) blob.push_back((R)(v * vf));
+    d.range[0] = t.range[0] * vf;
+    d.range[1] = t.range[1] * vf;
+    tabs.push_back(d);
+  }
+  // NIST Mott elements
+  std::vector<Mott> motts;
+  std::map<int, int> mottIndex;
+  for (auto& kv : ctx->mott) {
+    Mott m;
+    memset(&m, 0, sizeof(m));
+    mott_constants(kv.first, kv.second, m);
+    m.off_spwem = (int)blob.size();
+    for (double v : kv.second.spwem) blob.push_back((R)v);
+    m.off_x1 = (int)blob.size();
+    for (double v : kv.second.x1) blob.push_back((R)v);
+    mottIndex[kv.first] = (int)motts.size();
+    motts.push_back(m);
+  }
+  // scatter models
+  std::vector<Msm> msms;
+  std::vector<Mech> mechs;
+  for (auto& hm : ctx->msms) {
+    const HMaterial& mt = ctx->mats[hm.material];
+    Msm m;
+    memset(&m, 0, sizeof(m));
+    m.material = hm.material;
+    m.vacuum = mt.Z.empty();
+    double minE = m.vacuum ? -INFINITY : std::max(0.0, -mt.ecb);
+    if (hm.minSet) minE = hm.minE;
+    m.minE = minE * kFromSIeV;
+    m.ecb = mt.ecb * kFromSIeV;
+    m.u0 = mt.ecb * kFromSIeV;
+    m.classical = hm.classical;
+    m.lambda = hm.lambda * 1e9;
+    m.lambdaFactor = (kPi * hm.lambda * sqrt(kElectronMass / 2.)) / kHbar * sqrt(kEV);
+    m.csd = hm.csd;
+    if (hm.csd) m.jln = make_jln(mt, hm.breakE);
+    m.mech0 = (int)mechs.size();
+    m.nmech = (int)hm.mechs.size();
+    for (auto& hk : hm.mechs) {
+      Mech k;
+      memset(&k, 0, sizeof(k));
+      k.kind = hk.kind;
+      if (hk.kind == MECH_NISTMOTT) {
+        k.nel = (int)mt.Z.size();
+        const double densityNa = mt.density * kAvogadro;
+        for (int i = 0; i < k.nel; ++i) {
+          auto it = mottIndex.find(mt.Z[i]);
+          if (it == mottIndex.end()) return fail(CM_ESTATE, "no NIST Mott table for Z=" + std::to_string(mt.Z[i]));
+          k.mott[i] = it->second;
+          const double sf = (1000. * mt.wf[i]) / mt.A[i];
+          k.kbrown[i] = sf * densityNa * 1e-9;
+          k.kel[i] = (kBohr * kBohr) * sf * densityNa * 1e-9;
+        }
+      } else if (hk.kind == MECH_TABULATED) {
+        k.methodSE = (hk.method != 2) && (hk.method != 3) ? 1 : hk.method;
+        k.tIIMFP = hk.tables[0];
+        k.tRed = hk.tables[1];
+        k.tTheta = hk.tables[2];
+        k.tSEE0 = hk.tables[3];
+        k.energyOffset = hk.energyOffset * kFromSIeV;
+        k.minEgenSE = 0.;
+        k.rateMult = 1.;
+        k.energyCBbottom = mt.ecb * kFromSIeV;
+        k.bandgap = mt.bandgap * kFromSIeV;
+        k.energyGap = k.bandgap;
+        k.offsetFermiEnergy = (efermi(mt) + hk.energyOffset) * kFromSIeV;
+        k.bEref = (mt.bandgap > 0. ? -mt.bandgap : efermi(mt)) * kFromSIeV;
+        k.ncore = (int)mt.core.size();
+        for (int i = 0; i < k.ncore && i < kMaxCore; ++i) k.core[i] = mt.core[i] * kFromSIeV;
+        const Table& tr = tabs[k.tRed];
+        const Table& tt = tabs[k.tTheta];
+        k.eiDomain0 = std::max(tr.domain[0][0], tt.domain[0][0]);
+        k.eiDomain1 = std::min(tr.domain[0][1], tt.domain[0][1]);
+        k.iimfpDomain0 = tabs[k.tIIMFP].domain[0][0];
+        if (k.methodSE >= 2) {
+          k.rangeSE0lo = tabs[k.tSEE0].range[0];
+          k.rangeSE0hi = tabs[k.tSEE0].range[1];
+        }
+      } else if (hk.kind == MECH_FITTED) {
+        k.energySEgen = hk.energySEgen * kFromSIeV;
+        k.eFermi = efermi(mt) * kFromSIeV;
+        k.csd = make_jln(mt, hk.breakE);
+      } else if (hk.kind == MECH_PHONON) {
+        k.phononE = hk.phononE * kFromSIeV;
+        double occ = 0.5 * (1. + (1. / (exp(hk.phononE / (kBoltzmann * hk.temperature)) - 1.)));
+        double epsRatio = (hk.eps0 - hk.epsInf) / hk.eps0 / hk.epsInf;
+        k.prefactor = (hk.ratemult * occ * epsRatio) / kBohr * 1e-9;
+      } else if (hk.kind == MECH_POLARON) {
+        k.prefactor = hk.prefactor * 1e-9;
+        k.extinction = hk.extinction * kEV;
+        k.cutoff = (-log(10. / hk.prefactor) / hk.extinction) * kFromSIeV;
+      }
+      mechs.push_back(k);
+    }
+    msms.push_back(m);
+  }
+  // geometry in nm
+  std::vector<Shape> shapes;
+  std::vector<Plane> planes;
+  for (auto& hs : ctx->shapes) {
+    Shape s;
+    memset(&s, 0, sizeof(s));
+    s.kind = hs.kind;
+    s.a = hs.a;
+    s.b = hs.b;
+    for (int k = 0; k < 3; ++k) s.c[k] = hs.c[k] * 1e9;
+    s.r = hs.r * 1e9;
+    if (hs.kind == SHAPE_PLANES) {
+      s.plane0 = (int)planes.size();
+      s.np = (int)hs.n.size() / 3;
+      for (int i = 0; i < s.np; ++i) {
+        Plane p;
+        for (int k = 0; k < 3; ++k) {
+          p.n[k] = hs.n[3 * i + k];
+          p.p[k] = hs.p[3 * i + k] * 1e9;
+        }
+        planes.push_back(p);
+      }
+    }
+    shapes.push_back(s);
+  }
+  std::vector<Region> regions;
+  std::vector<int> children;
+  for (auto& hr : ctx->regions) {
+    Region r;
+    r.parent = hr.parent;
+    r.msm = hr.msm;
+    r.shape = hr.shape;
+    r.child0 = (int)children.size();
+    r.nchild = (int)hr.children.size();
+    for (int c : hr.children) children.push_back(c);
+    regions.push_back(r);
+  }
+  SceneView<R>& v = ds.view;
+  int rc = 0;
+  if ((rc = dev_copy(ds.allocs, shapes, &v.shapes)) || (rc = dev_copy(ds.allocs, planes, &v.planes)) ||
+      (rc = dev_copy(ds.allocs, regions, &v.regions)) || (rc = dev_copy(ds.allocs, children, &v.children)) ||
+      (rc = dev_copy(ds.allocs, msms, &v.msms)) || (rc = dev_copy(ds.allocs, mechs, &v.mechs)) ||
+      (rc = dev_copy(ds.allocs, motts, &v.mott)) || (rc = dev_copy(ds.allocs, tabs, &v.tables)) ||
+      (rc = dev_copy(ds.allocs, blob, &v.blob)))
+    return rc;
+  v.chamber = 0;
+  v.options = ctx->options;
+  v.dl50 = log(0.050 * kToSIkeV * kFromSIeV);
+  v.param = (log(20.0 * kToSIkeV) - log(0.050 * kToSIkeV)) / 60.0;
+  v.maxMott = 20.0 * kToSIkeV * kFromSIeV;
+  ds.valid = true;
+  return 0;
+}
+
+template <typename R> static DevScene<R>& scene_of(cm_context* c);
+template <> DevScene<double>& scene_of<double>(cm_context* c) { return c->d64; }
+template <> DevScene<float>& scene_of<float>(cm_context* c) { return c->d32; }
+template <typename R> static RunBuffers<R>& buffers_of(cm_context* c);
+template <> RunBuffers<double>& buffers_of<double>(cm_context* c) { return c->rb64; }
+template <> RunBuffers<float>& buffers_of<float>(cm_context* c) { return c->rb32; }
+
+// ------------------------------------------------------------------ wave state access
+template <typename R>
+struct El {
+  double p[3];
+  R d[3];
+  R E, Ep;
+  int region, pixel, aux;
+  uint32_t step;
+  unsigned long long key;
+  R h[3];
+};
+
+template <typename R> CM_D El<R> load(const Wave<R>& w, int i) {
+  El<R> e;
+  e.p[0] = w.px[i]; e.p[1] = w.py[i]; e.p[2] = w.pz[i];
+  e.d[0] = w.dx[i]; e.d[1] = w.dy[i]; e.d[2] = w.dz[i];
+  e.E = w.E[i]; e.Ep = w.Ep[i];
+  e.region = w.region[i]; e.pixel = w.pixel[i]; e.aux = w.aux[i];
+  e.step = w.step[i]; e.key = w.key[i];
+  e.h[0] = w.hx[i]; e.h[1] = w.hy[i]; e.h[2] = w.hz[i];
+  return e;
+}
+
+template <typename R> CM_D void store(const Wave<R>& w, int i, const El<R>& e) {
+  w.px[i] = e.p[0]; w.py[i] = e.p[1]; w.pz[i] = e.p[2];
+  w.dx[i] = e.d[0]; w.dy[i] = e.d[1]; w.dz[i] = e.d[2];
+  w.E[i] = e.E; w.Ep[i] = e.Ep;
+  w.region[i] = e.region; w.pixel[i] = e.pixel; w.aux[i] = e.aux;
+  w.step[i] = e.step; w.key[i] = e.key;
+  w.hx[i] = e.h[0]; w.hy[i] = e.h[1]; w.hz[i] = e.h[2];
+}
+
+// warp-aggregated append: one atomic per group of converged lanes
+CM_D int append_slot(int* counter) {
+  cg::coalesced_group g = cg::coalesced_threads();
+  int base = 0;
+  if (g.thread_rank() == 0) base = atomicAdd(counter, (int)g.size());
+  base = g.shfl(base, 0);
+  return base + (int)g.thread_rank();
+}
+
+enum { Q_EL = 0, Q_TAB = 1, Q_MISC = 2 };
+enum { AUX_MECH = 1, AUX_BARRIER = 2, AUX_PASS = 3 };
+CM_HD int aux_pack(int kind, int v) { return (kind << 24) | (v & 0xffffff); }
+CM_HD int aux_kind(int a) { return a >> 24; }
+CM_HD int aux_val(int a) { return a & 0xffffff; }
+
+template <typename R>
+struct RunView {
+  SceneView<R> s;
+  Wave<R> w[2];
+  Wave<R> pool;
+  int* q[3];
+  Counters* c;
+  int W, poolCap;
+  const double* pc;      // pixel centres, nm
+  const double* pe0;     // beam energy, eV
+  const double* pe0ref;  // histogram top edge: FromSI::eV(ToSI::eV(E0)) as the reference computes it
+  const int* pnbins;
+  const unsigned long long* prefix;
+  int npix;
+  double width;          // nm
+  unsigned long long seedmix;
+  uint32_t *back, *fwd;
+  int stride;
+};
+
+// Histogram::bin (Utility/Histogram.cu:73-80) over bins min + i*delta with
+// Algorithm::binarySearch (Amphibian/Algorithm.cu:5-14): exact match or the
+// insertion point.
+CM_D int hist_bin(double max, int nbins, double val) {
+  const double delta = max / nbins;
+  int l = 0, r = nbins;
+  while (l <= r) {
+    const int mid = l + (r - l) / 2;
+    const double bm = mid == 0 ? 0.0 : 0.0 + mid * delta;
+    if (bm == val) return mid;
+    if (bm < val) l = mid + 1;
+    else r = mid - 1;
+  }
+  return l;
+}
+
+// BackscatterStats::actionPerformed for a BackscatterEvent (NISTMonte/BackscatterStats.cu:147-170)
+template <typename R> CM_D void tally_escape(const RunView<R>& v, const El<R>& e) {
+  const int px = e.pixel;
+  const double E0ref = v.pe0ref[px];
+  double val = (double)e.E;
+  if (e.E == (R)v.pe0[px]) val = E0ref;  // electrons that never lost energy carry E0 exactly, as in the reference
+  const double elevation = (kPi / 2) - atan2(e.p[2], sqrt((e.p[0] * e.p[0]) + (e.p[1] * e.p[1])));
+  const int nb = v.pnbins[px];
+  const int b = hist_bin(E0ref, nb, val) + 1;
+  if (b > nb + 1) return;  // past the overflow slot: the reference writes out of bounds and never counts it
+  uint32_t* h = elevation < (kPi / 2.0) ? v.fwd : v.back;
+  atomicAdd(h + (size_t)px * v.stride + b, 1u);
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256) k_flight(RunView<R> v, int cur) {
+  const SceneView<R>& s = v.s;
+  const int n = v.c->n[cur];
+  const Wave<R> W = v.w[cur];
+  unsigned long long nsteps = 0, nscat = 0, nbar = 0, nesc = 0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    El<R> e = load(W, i);
+    int reg = e.region;
+    // MonteCarloSS::takeStep (MonteCarloSS.cu:109-119)
+    if (reg < 0 || !shape_contains(s, s.regions[reg].shape, e.p)) reg = containing_subregion(s, s.chamber, e.p);
+    if (reg < 0) continue;
+    const Msm& m = s.msms[s.regions[reg].msm];
+    Rng<R> g(e.key, e.step, 0);
+    // MONSEL_MaterialScatterModel::randomMeanPathLength (:64-91)
+    R cum[kMaxMech];
+    R total = 0;
+    const R logE = mlog(e.E);
+    for (int k = 0; k < m.nmech; ++k) {
+      total += mech_rate(s, s.mechs[m.mech0 + k], e.E, logE);
+      cum[k] = total;
+    }
+    bool complete = false;
+    double fp = 2.0 * kChamberRadiusNm;
+    if (total != R(0)) {
+      const R f = -mlog(g.next()) / total;
+      if ((double)f < fp) fp = (double)f;
+    } else if (e.step > 1000000u) {
+      complete = true;
+    }
+    double p1[3] = {e.p[0] + fp * (double)e.d[0], e.p[1] + fp * (double)e.d[1], e.p[2] + fp * (double)e.d[2]};
+    double hn[3];
+    const int next = find_end_of_step(s, reg, e.p, p1, hn);
+    const double dd = sqrt((p1[0] - e.p[0]) * (p1[0] - e.p[0]) + (p1[1] - e.p[1]) * (p1[1] - e.p[1]) +
+                           (p1[2] - e.p[2]) * (p1[2] - e.p[2]));
+    const R dE = m.csd ? jln_compute(m.jln, (R)dd, e.E) : R(0);
+    e.p[0] = p1[0]; e.p[1] = p1[1]; e.p[2] = p1[2];
+    e.Ep = e.E;
+    e.E += dE;
+    e.step += 1;
+    e.region = reg;
+    ++nsteps;
+    if ((e.E < (R)m.minE) || complete) continue;
+    int queue;
+    if (next == reg) {
+      ++nscat;
+      if (total == R(0)) {
+        queue = Q_MISC;
+        e.aux = aux_pack(AUX_PASS, 0);
+      } else {
+        // MONSEL_MaterialScatterModel::scatter (:93-134): the cache holds the step's starting energy
+        const R r = g.next() * total;
+        int idx = 0;
+        while (idx < m.nmech - 1 && cum[idx] < r) ++idx;
+        const int kind = s.mechs[m.mech0 + idx].kind;
+        if (kind == MECH_POLARON) continue;  // GanachaudMokraniPolaronTrapSM::scatter: trapped, E = 0
+        queue = kind == MECH_NISTMOTT ? Q_EL : kind == MECH_TABULATED ? Q_TAB : Q_MISC;
+        e.aux = aux_pack(AUX_MECH, idx);
+      }
+    } else if (next >= 0) {
+      ++nbar;
+      queue = Q_MISC;
+      e.aux = aux_pack(AUX_BARRIER, next);
+      e.h[0] = (R)hn[0]; e.h[1] = (R)hn[1]; e.h[2] = (R)hn[2];
+    } else {
+      ++nesc;
+      tally_escape(v, e);
+      continue;
+    }
+    store(W, i, e);
+    const int slot = append_slot(&v.c->q[queue]);
+    v.q[queue][slot] = i;
+  }
+  // counters: one atomic per warp
+  for (int off = 16; off > 0; off >>= 1) {
+    nsteps += __shfl_down_sync(0xffffffffu, nsteps, off);
+    nscat += __shfl_down_sync(0xffffffffu, nscat, off);
+    nbar += __shfl_down_sync(0xffffffffu, nbar, off);
+    nesc += __shfl_down_sync(0xffffffffu, nesc, off);
+  }
+  if ((threadIdx.x & 31) == 0 && nsteps) {
+    atomicAdd(&v.c->steps, nsteps);
+    atomicAdd(&v.c->scatters, nscat);
+    atomicAdd(&v.c->barriers, nbar);
+    atomicAdd(&v.c->escapes, nesc);
+  }
+}
+
+// append a surviving electron to the next wave
+template <typename R> CM_D void keep(const RunView<R>& v, int nxt, const El<R>& e) {
+  const int slot = append_slot(&v.c->n[nxt]);
+  store(v.w[nxt], slot, e);
+}
+
+// push a secondary to the pool when MonteCarloSS::trackSecondaryElectron (:165-174) would track it
+template <typename R> CM_D void push_secondary(const RunView<R>& v, const El<R>& pe, const R sd[3], R sE, int* nsec) {
+  const Msm& m = v.s.msms[v.s.regions[pe.region].msm];
+  if (!(sE > (R)m.minE)) return;
+  El<R> se;
+  se.p[0] = pe.p[0]; se.p[1] = pe.p[1]; se.p[2] = pe.p[2];
+  se.d[0] = sd[0]; se.d[1] = sd[1]; se.d[2] = sd[2];
+  se.E = sE; se.Ep = sE;
+  se.region = pe.region;
+  se.pixel = pe.pixel;
+  se.aux = 0;
+  se.step = 0;
+  se.key = mix64(pe.key ^ (0x9E3779B97F4A7C15ULL * (unsigned long long)pe.step));
+  se.h[0] = se.h[1] = se.h[2] = 0;
+  const int slot = append_slot(&v.c->pool);
+  if (slot >= v.poolCap) {
+    atomicExch(&v.c->error, CM_EOVERFLOW);
+    return;
+  }
+  store(v.pool, slot, se);
+  ++*nsec;
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256) k_elastic(RunView<R> v, int cur) {
+  const SceneView<R>& s = v.s;
+  const int n = v.c->q[Q_EL];
+  const int nxt = cur ^ 1;
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+    El<R> e = load(v.w[cur], v.q[Q_EL][j]);
+    const Msm& m = s.msms[s.regions[e.region].msm];
+    const Mech& k = s.mechs[m.mech0 + aux_val(e.aux)];
+    Rng<R> g(e.key, e.step - 1, 1);
+    elastic_scatter(s, k, e.d, e.Ep, g);
+    if (!(e.E < (R)m.minE)) keep(v, nxt, e);
+  }
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256) k_inelastic(RunView<R> v, int cur) {
+  const SceneView<R>& s = v.s;
+  const int n = v.c->q[Q_TAB];
+  const int nxt = cur ^ 1;
+  int nsec = 0;
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+    El<R> e = load(v.w[cur], v.q[Q_TAB][j]);
+    const Msm& m = s.msms[s.regions[e.region].msm];
+    const Mech& k = s.mechs[m.mech0 + aux_val(e.aux)];
+    Rng<R> g(e.key, e.step - 1, 1);
+    R sd[3], sE;
+    const bool made = tabulated_scatter(s, k, e.d, e.E, sd, sE, g);
+    if (!(e.E < (R)m.minE)) keep(v, nxt, e);
+    if (made) push_secondary(v, e, sd, sE, &nsec);
+  }
+  for (int off = 16; off > 0; off >>= 1) nsec += __shfl_down_sync(0xffffffffu, nsec, off);
+  if ((threadIdx.x & 31) == 0 && nsec) atomicAdd(&v.c->secondaries, (unsigned long long)nsec);
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256) k_misc(RunView<R> v, int cur) {
+  const SceneView<R>& s = v.s;
+  const int n = v.c->q[Q_MISC];
+  const int nxt = cur ^ 1;
+  int nsec = 0;
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+    El<R> e = load(v.w[cur], v.q[Q_MISC][j]);
+    const Msm& m = s.msms[s.regions[e.region].msm];
+    const int kind = aux_kind(e.aux);
+    Rng<R> g(e.key, e.step - 1, 1);
+    if (kind == AUX_BARRIER) {
+      // MonteCarloSS::takeStep (:143-156): barrierScatter, a nudge along the new direction, region update
+      const double hn[3] = {(double)e.h[0], (double)e.h[1], (double)e.h[2]};
+      e.region = barrier_scatter(s, m, e.p, e.d, e.E, e.region, aux_val(e.aux), hn, g);
+      e.p[0] += kSmallDispNm * (double)e.d[0];
+      e.p[1] += kSmallDispNm * (double)e.d[1];
+      e.p[2] += kSmallDispNm * (double)e.d[2];
+      if (!shape_contains(s, s.regions[e.region].shape, e.p)) e.region = containing_subregion(s, s.chamber, e.p);
+      keep(v, nxt, e);
+      continue;
+    }
+    if (kind == AUX_MECH) {
+      const Mech& k = s.mechs[m.mech0 + aux_val(e.aux)];
+      if (k.kind == MECH_FITTED) {  // FittedInelSM::scatter (FittedInelSM.cu:13-18)
+        const R phi = R(2) * R(kPi) * g.next();
+        const R theta = macos(R(1) - (R(2) * g.next()));
+        R sd[3];
+        dir_from_angles(sd, theta, phi);
+        push_secondary(v, e, sd, (R)(k.energySEgen + k.eFermi), &nsec);
+      } else if (k.kind == MECH_PHONON) {
+        phonon_scatter(k, e.d, e.E, e.Ep, g);
+      }
+    }
+    if (!(e.E < (R)m.minE)) keep(v, nxt, e);
+  }
+  for (int off = 16; off > 0; off >>= 1) nsec += __shfl_down_sync(0xffffffffu, nsec, off);
+  if ((threadIdx.x & 31) == 0 && nsec) atomicAdd(&v.c->secondaries, (unsigned long long)nsec);
+}
+
+// refill the next wave: secondaries from the pool first, then new primaries
+CM_D void refill_plan(const Counters* c, int nxt, int W, int& nn, int& take_se, int& take_p) {
+  nn = c->n[nxt];
+  const int room = W - nn > 0 ? W - nn : 0;
+  take_se = c->pool < room ? c->pool : room;
+  const unsigned long long rem = c->total_primaries - c->next_primary;
+  const int left = room - take_se;
+  take_p = rem < (unsigned long long)left ? (int)rem : left;
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256) k_spawn(RunView<R> v, int cur) {
+  const int nxt = cur ^ 1;
+  int nn, take_se, take_p;
+  refill_plan(v.c, nxt, v.W, nn, take_se, take_p);
+  const int poolTop = v.c->pool;
+  const unsigned long long first = v.c->next_primary;
+  const SceneView<R>& s = v.s;
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < take_se + take_p; j += gridDim.x * blockDim.x) {
+    if (j < take_se) {
+      store(v.w[nxt], nn + j, load(v.pool, poolTop - 1 - j));
+      continue;
+    }
+    // GaussianBeam::createElectron (NISTMonte/GaussianBeam.cu:52-65) + initializeTrajectory (MonteCarloSS.cu:99-105)
+    const unsigned long long gi = first + (unsigned long long)(j - take_se);
+    int lo = 0, hi = v.npix;
+    while (hi - lo > 1) {
+      const int mid = (lo + hi) >> 1;
+      if (v.prefix[mid] <= gi) lo = mid;
+      else hi = mid;
+    }
+    const int px = lo;
+    const unsigned long long k = gi - v.prefix[px];
+    El<R> e;
+    e.key = mix64(v.seedmix ^ mix64(((unsigned long long)px << 32) | k));
+    Rng<R> g(e.key, 0xFFFFFFFFu, 0);
+    const double u1 = (double)g.next(), u2 = (double)g.next();
+    const double r = sqrt(-2. * log(u1)) * v.width;
+    const double th = 2.0 * kPi * u2;
+    e.p[0] = v.pc[3 * px] + r * cos(th);
+    e.p[1] = v.pc[3 * px + 1] + r * sin(th);
+    e.p[2] = v.pc[3 * px + 2];
+    e.d[0] = 0; e.d[1] = 0; e.d[2] = 1;
+    e.E = (R)v.pe0[px];
+    e.Ep = e.E;
+    e.region = containing_subregion(s, s.chamber, e.p);
+    e.pixel = px;
+    e.aux = 0;
+    e.step = 0;
+    e.h[0] = e.h[1] = e.h[2] = 0;
+    store(v.w[nxt], nn + j, e);
+  }
+}
+
+template <typename R>
+__global__ void k_tail(RunView<R> v, int cur) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  const int nxt = cur ^ 1;
+  Counters* c = v.c;
+  int nn, take_se, take_p;
+  refill_plan(c, nxt, v.W, nn, take_se, take_p);
+  c->n[nxt] = nn + take_se + take_p;
+  c->pool -= take_se;
+  c->next_primary += (unsigned long long)take_p;
+  c->n[cur] = 0;
+  c->q[0] = c->q[1] = c->q[2] = 0;
+  c->iterations += 1;
+  c->done = (c->n[nxt] == 0 && c->pool == 0 && c->next_primary == c->total_primaries) ? 1 : 0;
+}
+
+template <typename R>
+static int alloc_wave(std::vector<void*>& allocs, Wave<R>& w, int cap) {
+  auto A = [&](void** p, size_t bytes) -> int {
+    CM_CUDA(cudaMalloc(p, bytes));
+    allocs.push_back(*p);
+    return 0;
+  };
+  int rc = 0;
+  size_t n = (size_t)cap;
+  if ((rc = A((void**)&w.px, n * 8)) || (rc = A((void**)&w.py, n * 8)) || (rc = A((void**)&w.pz, n * 8)) ||
+      (rc = A((void**)&w.dx, n * sizeof(R))) || (rc = A((void**)&w.dy, n * sizeof(R))) ||
+      (rc = A((void**)&w.dz, n * sizeof(R))) || (rc = A((void**)&w.E, n * sizeof(R))) ||
+      (rc = A((void**)&w.Ep, n * sizeof(R))) || (rc = A((void**)&w.region, n * 4)) ||
+      (rc = A((void**)&w.pixel, n * 4)) || (rc = A((void**)&w.aux, n * 4)) || (rc = A((void**)&w.step, n * 4)) ||
+      (rc = A((void**)&w.key, n * 8)) || (rc = A((void**)&w.hx, n * sizeof(R))) ||
+      (rc = A((void**)&w.hy, n * sizeof(R))) || (rc = A((void**)&w.hz, n * sizeof(R))))
+    return rc;
+  return 0;
+}
+
+template <typename R>
+static int ensure_buffers(cm_context* ctx, int W) {
+  RunBuffers<R>& rb = buffers_of<R>(ctx);
+  const int poolCap = 4 * W;
+  if (rb.cap >= W && rb.poolCap >= poolCap) return 0;
+  rb.release();
+  int rc;
+  if ((rc = alloc_wave(rb.allocs, rb.w[0], W)) || (rc = alloc_wave(rb.allocs, rb.w[1], W)) ||
+      (rc = alloc_wave(rb.allocs, rb.pool, poolCap)))
+    return rc;
+  for (int k = 0; k < 3; ++k) {
+    void* p;
+    CM_CUDA(cudaMalloc(&p, (size_t)W * 4));
+    rb.allocs.push_back(p);
+    rb.q[k] = (int*)p;
+  }
+  rb.cap = W;
+  rb.poolCap = poolCap;
+  return 0;
+}
+
+// Transport loop.  Inputs are device arrays.
+template <typename R>
+static int run_device(cm_context* ctx, const cm_run_desc* d, uint32_t* back, uint32_t* fwd, cm_run_stats* st,
+                      cudaStream_t stream, const unsigned long long* prefix_dev, const double* e0ref_dev,
+                      unsigned long long total) {
+  int rc;
+  if ((rc = build_scene<R>(ctx, scene_of<R>(ctx)))) return rc;
+  const int W = d->wave > 0 ? d->wave : (sizeof(R) == 8 ? (1 << 20) : (1 << 21));
+  if ((rc = ensure_buffers<R>(ctx, W))) return rc;
+  RunBuffers<R>& rb = buffers_of<R>(ctx);
+  RunView<R> v;
+  v.s = scene_of<R>(ctx).view;
+  v.s.chamber = d->chamber;
+  v.w[0] = rb.w[0];
+  v.w[1] = rb.w[1];
+  v.pool = rb.pool;
+  for (int k = 0; k < 3; ++k) v.q[k] = rb.q[k];
+  v.c = ctx->counters;
+  v.W = W;
+  v.poolCap = rb.poolCap;
+  v.pc = d->pixel_center;
+  v.pe0 = d->pixel_energy;
+  v.pe0ref = e0ref_dev;
+  v.pnbins = d->pixel_nbins;
+  v.prefix = prefix_dev;
+  v.npix = d->npix;
+  v.width = d->beam_width;
+  v.seedmix = mix64(d->seed ^ 0x243F6A8885A308D3ULL);
+  v.back = back;
+  v.fwd = fwd;
+  v.stride = d->hist_stride;
+
+  Counters c0;
+  memset(&c0, 0, sizeof(c0));
+  c0.total_primaries = total;
+  CM_CUDA(cudaMemcpyAsync(ctx->counters, &c0, sizeof(c0), cudaMemcpyHostToDevice, stream));
+  const int grid = ctx->nsm * 8;
+  const int maxIt = d->max_iterations > 0 ? d->max_iterations : 2000000;
+  cudaEvent_t e0, e1;
+  CM_CUDA(cudaEventCreate(&e0));
+  CM_CUDA(cudaEventCreate(&e1));
+  // capture 2*K iterations once, replay until done
+  const int K = 8;
+  cudaGraph_t graph;
+  cudaGraphExec_t exec;
+  CM_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+  for (int it = 0; it < 2 * K; ++it) {
+    const int cur = it & 1;
+    k_flight<R><<<grid, 256, 0, stream>>>(v, cur);
+    k_elastic<R><<<grid, 256, 0, stream>>>(v, cur);
+    k_inelastic<R><<<grid, 256, 0, stream>>>(v, cur);
+    k_misc<R><<<grid, 256, 0, stream>>>(v, cur);
+    k_spawn<R><<<grid, 256, 0, stream>>>(v, cur);
+    k_tail<R><<<1, 32, 0, stream>>>(v, cur);
+  }
+  CM_CUDA(cudaStreamEndCapture(stream, &graph));
+  CM_CUDA(cudaGraphInstantiate(&exec, graph, 0));
+  CM_CUDA(cudaEventRecord(e0, stream));
+  int iters = 0;
+  int status = 0;
+  for (;;) {
+    CM_CUDA(cudaGraphLaunch(exec, stream));
+    iters += 2 * K;
+    CM_CUDA(cudaMemcpyAsync(ctx->counters_host, ctx->counters, sizeof(Counters), cudaMemcpyDeviceToHost, stream));
+    CM_CUDA(cudaStreamSynchronize(stream));
+    if (ctx->counters_host->error) {
+      status = fail(ctx->counters_host->error, "secondary pool overflow; raise the wave size");
+      break;
+    }
+    if (ctx->counters_host->done) break;
+    if (iters >= maxIt) {
+      status = fail(CM_ELIMIT, "iteration limit reached");
+      break;
+    }
+  }
+  CM_CUDA(cudaEventRecord(e1, stream));
+  CM_CUDA(cudaEventSynchronize(e1));
+  float ms = 0;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaGraphExecDestroy(exec);
+  cudaGraphDestroy(graph);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  CM_CUDA(cudaGetLastError());
+  if (st) {
+    const Counters& c = *ctx->counters_host;
+    st->primaries = (int64_t)c.next_primary;
+    st->steps = (int64_t)c.steps;
+    st->scatter_events = (int64_t)c.scatters;
+    st->barrier_events = (int64_t)c.barriers;
+    st->escapes = (int64_t)c.escapes;
+    st->secondaries = (int64_t)c.secondaries;
+    st->iterations = (int64_t)c.iterations;
+    st->device_ms = ms;
+  }
+  return status;
+}
+
+// ------------------------------------------------------------------ per-function kernels
+template <typename R> __global__ void k_eval_nistmott(SceneView<R> s, int mi, int n, const double* E, const double* u, double* sig,
+                                                      double* th) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const Mott& m = s.mott[mi];
+  const R e = (R)(E[i] * kFromSIeV);
+  // cross section in m^2 (rate factor 1/kbrown folded back): kel = a0^2, kbrown = 1
+  sig[i] = (double)nistmott_rate(s, m, (R)(kBohr * kBohr), R(1), e, mlog(e));
+  FixedRng<R> g{u + 2 * i, 2, 0};
+  th[i] = (double)nistmott_angle(s, m, e, g);
+}
+
+template <typename R> __global__ void k_eval_table(SceneView<R> s, int t, int n, const double* x, double f0, double vf, int order,
+                                                   double* out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  out[i] = (double)table_interp(s, t, (R)(x[3 * i] * f0), (R)x[3 * i + 1], (R)x[3 * i + 2], order) / vf;
+}
+
+template <typename R> __global__ void k_eval_tabulated(SceneView<R> s, int mech, int n, const double* in, double* out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const Mech& k = s.mechs[mech];
+  const double* q = in + 9 * i;
+  double* o = out + 12 * i;
+  R E = (R)(q[0] * kFromSIeV);
+  R d[3];
+  dir_from_angles(d, (R)q[1], (R)q[2]);
+  o[0] = (double)tabulated_rate(s, k, E) * 1e9;
+  FixedRng<R> g{q + 3, 6, 0};
+  R sd[3] = {0, 0, 0}, sE = 0;
+  const bool made = tabulated_scatter(s, k, d, E, sd, sE, g);
+  o[1] = (double)E * kEV;
+  o[2] = d[0]; o[3] = d[1]; o[4] = d[2];
+  o[5] = made;
+  o[6] = made ? (double)sE * kEV : 0.;
+  o[7] = sd[0]; o[8] = sd[1]; o[9] = sd[2];
+  o[10] = g.used;
+  o[11] = 0;
+}
+
+template <typename R> __global__ void k_eval_elastic(SceneView<R> s, int mech, int n, const double* in, double* out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const Mech& k = s.mechs[mech];
+  const double* q = in + 7 * i;
+  double* o = out + 6 * i;
+  const R E = (R)(q[0] * kFromSIeV);
+  R d[3];
+  dir_from_angles(d, (R)q[1], (R)q[2]);
+  o[0] = (double)mech_rate(s, k, E, mlog(E)) * 1e9;
+  FixedRng<R> g{q + 3, 4, 0};
+  const int el = elastic_scatter(s, k, d, E, g);
+  o[1] = d[0]; o[2] = d[1]; o[3] = d[2];
+  o[4] = s.mott[k.mott[el]].Z;
+  o[5] = g.used;
+}
+
+template <typename R> __global__ void k_eval_csd(SceneView<R> s, int msm, int n, const double* in, double* out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const Msm& m = s.msms[msm];
+  const R E = (R)(in[2 * i] * kFromSIeV);
+  const R len = (R)(in[2 * i + 1] * 1e9);
+  out[3 * i] = m.csd ? (double)jln_compute(m.jln, len, E) * kEV : 0.;
+  double fr = 0, pr = 0;
+  for (int k = 0; k < m.nmech; ++k) {
+    const Mech& mk = s.mechs[m.mech0 + k];
+    if (mk.kind == MECH_FITTED) fr = (double)mech_rate(s, mk, E, mlog(E)) * 1e9;
+    if (mk.kind == MECH_POLARON) pr = (double)mech_rate(s, mk, E, mlog(E)) * 1e9;
+  }
+  out[3 * i + 1] = fr;
+  out[3 * i + 2] = pr;
+}
+
+template <typename R> __global__ void k_eval_phonon(SceneView<R> s, int mech, int n, const double* in, double* out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const Mech& k = s.mechs[mech];
+  const double* q = in + 5 * i;
+  double* o = out + 6 * i;
+  R E = (R)(q[0] * kFromSIeV), Ep = E;
+  R d[3];
+  dir_from_angles(d, (R)q[1], (R)q[2]);
+  o[0] = (double)phonon_rate(k, E) * 1e9;
+  FixedRng<R> g{q + 3, 2, 0};
+  phonon_scatter(k, d, E, Ep, g);
+  o[1] = (double)E * kEV;
+  o[2] = d[0]; o[3] = d[1]; o[4] = d[2];
+  o[5] = (double)Ep * kEV;
+}
+
+__global__ void k_eval_shape(SceneView<double> s, int shape, int n, const double* p01, double* out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double p0[3] = {p01[6 * i] * 1e9, p01[6 * i + 1] * 1e9, p01[6 * i + 2] * 1e9};
+  const double p1[3] = {p01[6 * i + 3] * 1e9, p01[6 * i + 4] * 1e9, p01[6 * i + 5] * 1e9};
+  NV r = shape_first_normal(s, shape, p0, p1);
+  out[5 * i] = r.n[0];
+  out[5 * i + 1] = r.n[1];
+  out[5 * i + 2] = r.n[2];
+  out[5 * i + 3] = r.u;
+  out[5 * i + 4] = shape_contains(s, shape, p0) ? 1. : 0.;
+}
+
+template <typename R> __global__ void k_eval_barrier(SceneView<R> s, int from, int to, int n, const double* in, double* out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double* q = in + 6 * i;
+  double* o = out + 8 * i;
+  R E = (R)(q[0] * kFromSIeV);
+  R d[3];
+  dir_from_angles(d, (R)q[1], (R)q[2]);
+  double p[3] = {q[3] * 1e9, q[4] * 1e9, q[5] * 1e9};
+  const double hn[3] = {0., 0., -1.};
+  FixedRng<R> g{nullptr, 0, 0};
+  const int reg = barrier_scatter(s, s.msms[s.regions[from].msm], p, d, E, from, to, hn, g);
+  o[0] = (double)E * kEV;
+  o[1] = d[0]; o[2] = d[1]; o[3] = d[2];
+  o[4] = p[0] * 1e-9; o[5] = p[1] * 1e-9; o[6] = p[2] * 1e-9;
+  o[7] = reg;
+}
+
+template <typename R> __global__ void k_eval_freepath(SceneView<R> s, int msm, int n, const double* in, double* out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const Msm& m = s.msms[msm];
+  const R E = (R)(in[2 * i] * kFromSIeV);
+  R total = 0;
+  const R logE = mlog(E);
+  for (int k = 0; k < m.nmech; ++k) total += mech_rate(s, s.mechs[m.mech0 + k], E, logE);
+  double fp = 2.0 * kChamberRadiusNm;
+  if (total != R(0)) {
+    const R f = -mlog((R)in[2 * i + 1]) / total;
+    if ((double)f < fp) fp = (double)f;
+  }
+  out[i] = fp * 1e-9;
+}
+
+}  // namespace cm
+
+// ================================================================== C ABI
+extern "C" {
+
+const char* cm_last_error(void) { return g_err.c_str(); }
+int cm_version(void) { return 1; }
+
+int cm_context_create(int device, cm_context** out) {
+  if (!out) return fail(CM_EINVAL, "out is null");
+  int n = 0;
+  CM_CUDA(cudaGetDeviceCount(&n));
+  if (device < 0 || device >= n) return fail(CM_EINVAL, "no such CUDA device");
+  CM_CUDA(cudaSetDevice(device));
+  cudaDeviceProp prop;
+  CM_CUDA(cudaGetDeviceProperties(&prop, device));
+  if (prop.major < 10) return fail(CM_ECUDA, "this build targets sm_100a (B200); device is sm_" +
+                                                 std::to_string(prop.major) + std::to_string(prop.minor));
+  std::unique_ptr<cm_context> c(new cm_context());
+  c->device = device;
+  c->nsm = prop.multiProcessorCount;
+  CM_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+  CM_CUDA(cudaMalloc(&c->counters, sizeof(Counters)));
+  CM_CUDA(cudaMallocHost(&c->counters_host, sizeof(Counters)));
+  *out = c.release();
+  return 0;
+}
+
+int cm_context_destroy(cm_context* ctx) {
+  if (!ctx) return 0;
+  cudaSetDevice(ctx->device);
+  ctx->dirty();
+  ctx->rb64.release();
+  ctx->rb32.release();
+  cudaFree(ctx->counters);
+  cudaFreeHost(ctx->counters_host);
+  if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+  return 0;
+}
+
+int cm_set_options(cm_context* ctx, int options) {
+  if (!ctx) return fail(CM_EINVAL, "null context");
+  ctx->options = options;
+  ctx->dirty();
+  return 0;
+}
+
+int cm_add_mott_element(cm_context* ctx, int Z, const double* spwem, const double* x1) {
+  if (!ctx || Z < 1 || Z > 96 || !spwem || !x1) return fail(CM_EINVAL, "bad Mott element arguments");
+  HMott m;
+  m.spwem.assign(spwem, spwem + 61);
+  m.x1.assign(x1, x1 + 61 * 201);
+  ctx->mott[Z] = m;
+  ctx->dirty();
+  return 0;
+}
+
+int cm_add_table(cm_context* ctx, int dim, const int* n, const double* axes, const double* values, int* out) {
+  if (!ctx || dim < 1 || dim > 3 || !n || !axes || !values || !out) return fail(CM_EINVAL, "bad table arguments");
+  HTable t;
+  memset(t.n, 0, sizeof(t.n));
+  t.dim = dim;
+  t.role = 0;
+  t.range[0] = INFINITY;
+  t.range[1] = -INFINITY;
+  size_t total = 1, off = 0;
+  for (int k = 0; k < dim; ++k) {
+    if (n[k] < 4) return fail(CM_EINVAL, "table axes need at least 4 points");
+    t.n[k] = n[k];
+    t.x[k].assign(axes + off, axes + off + n[k]);
+    off += n[k];
+    total *= n[k];
+    // NUTableInterpolation::ReadTable (:152-159)
+    if (t.x[k][0] < t.x[k][n[k] - 1]) {
+      t.domain[k][0] = t.x[k][0];
+      t.domain[k][1] = t.x[k][n[k] - 1];
+    } else {
+      t.domain[k][1] = t.x[k][0];
+      t.domain[k][0] = t.x[k][n[k] - 1];
+    }
+  }
+  t.v.assign(values, values + total);
+  for (double v : t.v) {  // (:169-172): if / else-if, as written
+    if (v < t.range[0]) t.range[0] = v;
+    else if (v > t.range[1]) t.range[1] = v;
+  }
+  *out = (int)ctx->tables.size();
+  ctx->tables.push_back(t);
+  ctx->dirty();
+  return 0;
+}
+
+int cm_add_material(cm_context* ctx, int nel, const int* Z, const double* A, const double* wf, double density,
+                    double workfunction, double ecb, double bandgap, int ncore, const double* core, int* out) {
+  if (!ctx || nel < 0 || nel > kMaxElem || ncore < 0 || ncore > kMaxCore || !out) return fail(CM_EINVAL, "bad material");
+  HMaterial m;
+  for (int i = 0; i < nel; ++i) {
+    m.Z.push_back(Z[i]);
+    m.A.push_back(A[i]);
+    m.wf.push_back(wf[i]);
+  }
+  // SEmaterial keeps core energies in a std::set: ascending, unique
+  std::vector<double> c(core, core + ncore);
+  std::sort(c.begin(), c.end());
+  c.erase(std::unique(c.begin(), c.end()), c.end());
+  m.core = c;
+  m.density = density;
+  m.workfunction = workfunction;
+  m.ecb = ecb;
+  m.bandgap = bandgap;
+  *out = (int)ctx->mats.size();
+  ctx->mats.push_back(m);
+  ctx->dirty();
+  return 0;
+}
+
+int cm_add_msm(cm_context* ctx, int material, int* out) {
+  if (!ctx || material < 0 || material >= (int)ctx->mats.size() || !out) return fail(CM_EINVAL, "bad material handle");
+  HMsm m;
+  m.material = material;
+  m.csd = 0;
+  m.breakE = 0;
+  m.minSet = false;
+  m.minE = 0;
+  m.classical = 1;
+  m.lambda = 0;
+  *out = (int)ctx->msms.size();
+  ctx->msms.push_back(m);
+  ctx->dirty();
+  return 0;
+}
+
+static int add_mech(cm_context* ctx, int msm, const HMech& k, int* out) {
+  if (!ctx || msm < 0 || msm >= (int)ctx->msms.size()) return fail(CM_EINVAL, "bad scatter model handle");
+  auto& m = ctx->msms[msm];
+  if ((int)m.mechs.size() >= kMaxMech) return fail(CM_EINVAL, "too many mechanisms");
+  if (out) *out = (int)m.mechs.size();
+  m.mechs.push_back(k);
+  ctx->dirty();
+  return 0;
+}
+
+int cm_msm_add_nistmott(cm_context* ctx, int msm, int method, int* out) {
+  if (method != 1) return fail(CM_EINVAL, "only NISTMottRS method 1 (NISTMottRS::Factory) is supported");
+  HMech k;
+  memset(&k, 0, sizeof(k));
+  k.kind = MECH_NISTMOTT;
+  k.method = method;
+  return add_mech(ctx, msm, k, out);
+}
+
+int cm_msm_add_tabulated(cm_context* ctx, int msm, int method_se, double energy_offset, const int tables[4], int* out) {
+  if (!ctx || !tables) return fail(CM_EINVAL, "null tables");
+  const int roles[4] = {1, 2, 3, 4};
+  const int dims[4] = {1, 2, 3, 2};
+  for (int k = 0; k < 4; ++k) {
+    if (k == 3 && method_se != 2 && method_se != 3) continue;
+    if (tables[k] < 0 || tables[k] >= (int)ctx->tables.size()) return fail(CM_EINVAL, "bad table handle");
+    HTable& t = ctx->tables[tables[k]];
+    if (t.dim != dims[k]) return fail(CM_EINVAL, "table has the wrong dimension for its role");
+    if (t.role && t.role != roles[k]) return fail(CM_EINVAL, "table used in two roles");
+    t.role = roles[k];
+  }
+  HMech k;
+  memset(&k, 0, sizeof(k));
+  k.kind = MECH_TABULATED;
+  k.method = method_se;
+  k.energyOffset = energy_offset;
+  for (int i = 0; i < 4; ++i) k.tables[i] = tables[i];
+  return add_mech(ctx, msm, k, out);
+}
+
+int cm_msm_add_fitted(cm_context* ctx, int msm, double energy_se_gen, double break_e, int* out) {
+  HMech k;
+  memset(&k, 0, sizeof(k));
+  k.kind = MECH_FITTED;
+  k.energySEgen = energy_se_gen;
+  k.breakE = break_e;
+  return add_mech(ctx, msm, k, out);
+}
+
+int cm_msm_add_phonon(cm_context* ctx, int msm, double ratemult, double phonon_e, double temperature, double eps0,
+                      double eps_inf, int* out) {
+  HMech k;
+  memset(&k, 0, sizeof(k));
+  k.kind = MECH_PHONON;
+  k.ratemult = ratemult;
+  k.phononE = phonon_e;
+  k.temperature = temperature;
+  k.eps0 = eps0;
+  k.epsInf = eps_inf;
+  return add_mech(ctx, msm, k, out);
+}
+
+int cm_msm_add_polaron(cm_context* ctx, int msm, double prefactor, double extinction, int* out) {
+  HMech k;
+  memset(&k, 0, sizeof(k));
+  k.kind = MECH_POLARON;
+  k.prefactor = prefactor;
+  k.extinction = extinction;
+  return add_mech(ctx, msm, k, out);
+}
+
+int cm_msm_set_csd_jln(cm_context* ctx, int msm, double break_e) {
+  if (!ctx || msm < 0 || msm >= (int)ctx->msms.size()) return fail(CM_EINVAL, "bad scatter model handle");
+  ctx->msms[msm].csd = 1;
+  ctx->msms[msm].breakE = break_e;
+  ctx->dirty();
+  return 0;
+}
+
+int cm_msm_set_min_e(cm_context* ctx, int msm, double min_e) {
+  if (!ctx || msm < 0 || msm >= (int)ctx->msms.size()) return fail(CM_EINVAL, "bad scatter model handle");
+  ctx->msms[msm].minSet = true;
+  ctx->msms[msm].minE = min_e;
+  ctx->dirty();
+  return 0;
+}
+
+int cm_msm_set_barrier(cm_context* ctx, int msm, int classical, double lambda) {
+  if (!ctx || msm < 0 || msm >= (int)ctx->msms.size()) return fail(CM_EINVAL, "bad scatter model handle");
+  ctx->msms[msm].classical = classical ? 1 : 0;
+  ctx->msms[msm].lambda = lambda;
+  ctx->dirty();
+  return 0;
+}
+
+int cm_shape_sphere(cm_context* ctx, const double center[3], double radius, int* out) {
+  if (!ctx || !center || !out || !(radius > 0)) return fail(CM_EINVAL, "bad sphere");
+  HShape s;
+  s.kind = SHAPE_SPHERE;
+  for (int k = 0; k < 3; ++k) s.c[k] = center[k];
+  s.r = radius;
+  s.a = s.b = -1;
+  *out = (int)ctx->shapes.size();
+  ctx->shapes.push_back(s);
+  ctx->dirty();
+  return 0;
+}
+
+int cm_shape_planes(cm_context* ctx, int n, const double* normals, const double* points, int* out) {
+  if (!ctx || n < 1 || n > 64 || !normals || !points || !out) return fail(CM_EINVAL, "bad plane set");
+  HShape s;
+  s.kind = SHAPE_PLANES;
+  s.n.assign(normals, normals + 3 * n);
+  s.p.assign(points, points + 3 * n);
+  s.a = s.b = -1;
+  s.r = 0;
+  s.c[0] = s.c[1] = s.c[2] = 0;
+  *out = (int)ctx->shapes.size();
+  ctx->shapes.push_back(s);
+  ctx->dirty();
+  return 0;
+}
+
+static int shape_depth(cm_context* ctx, int id) {
+  const HShape& s = ctx->shapes[id];
+  if (s.kind != SHAPE_INTERSECTION) return 0;
+  return 1 + std::max(shape_depth(ctx, s.a), shape_depth(ctx, s.b));
+}
+
+int cm_shape_intersection(cm_context* ctx, int a, int b, int* out) {
+  if (!ctx || !out || a < 0 || b < 0 || a >= (int)ctx->shapes.size() || b >= (int)ctx->shapes.size())
+    return fail(CM_EINVAL, "bad shape handle");
+  if (ctx->shapes[a].kind == SHAPE_SPHERE || ctx->shapes[b].kind == SHAPE_SPHERE)
+    return fail(CM_EINVAL, "a Sphere is not a NormalShape");
+  HShape s;
+  s.kind = SHAPE_INTERSECTION;
+  s.a = a;
+  s.b = b;
+  s.r = 0;
+  s.c[0] = s.c[1] = s.c[2] = 0;
+  *out = (int)ctx->shapes.size();
+  ctx->shapes.push_back(s);
+  if (shape_depth(ctx, *out) > kMaxShapeDepth) {
+    ctx->shapes.pop_back();
+    return fail(CM_EINVAL, "intersection nesting deeper than 4");
+  }
+  ctx->dirty();
+  return 0;
+}
+
+static void translate_rec(cm_context* ctx, int id, const double* d) {
+  HShape& s = ctx->shapes[id];
+  if (s.kind == SHAPE_PLANES) {
+    for (size_t i = 0; i < s.p.size(); ++i) s.p[i] += d[i % 3];  // Plane::translate (MultiPlaneShape.cu:59-64)
+  } else if (s.kind == SHAPE_INTERSECTION) {
+    translate_rec(ctx, s.a, d);
+    translate_rec(ctx, s.b, d);
+  } else {
+    for (int k = 0; k < 3; ++k) s.c[k] += d[k];
+  }
+}
+
+int cm_shape_translate(cm_context* ctx, int shape, const double d[3]) {
+  if (!ctx || !d || shape < 0 || shape >= (int)ctx->shapes.size()) return fail(CM_EINVAL, "bad shape handle");
+  translate_rec(ctx, shape, d);
+  ctx->dirty();
+  return 0;
+}
+
+int cm_shape_line(cm_context* ctx, double topz, double width, double length, double thetal, double thetar, int* out) {
+  if (!ctx || !out) return fail(CM_EINVAL, "null argument");
+  // NShapes::createLine (JMONSEL/NShapes.cu:55-149) with zero corner radii
+  double signz = !topz ? 0 : (topz > 0 ? 1 : -1);
+  if (signz == 0.) signz = 1.;
+  const double en[12] = {0., 0., signz, 0., 0., -signz, 0., 1., 0., 0., -1., 0.};
+  const double ep[12] = {0., 0., topz, 0., 0., 0., 0., length / 2., 0., 0., -length / 2., 0.};
+  int enclosure, right, left, nts, rc;
+  if ((rc = cm_shape_planes(ctx, 4, en, ep, &enclosure))) return rc;
+  const double rn[3] = {cos(thetar), 0., signz * sin(thetar)}, rp[3] = {width / 2, 0., 0.};
+  if ((rc = cm_shape_planes(ctx, 1, rn, rp, &right))) return rc;
+  const double ln[3] = {-cos(thetal), 0., signz * sin(thetal)}, lp[3] = {-width / 2, 0., 0.};
+  if ((rc = cm_shape_planes(ctx, 1, ln, lp, &left))) return rc;
+  if ((rc = cm_shape_intersection(ctx, left, right, &nts))) return rc;
+  return cm_shape_intersection(ctx, nts, enclosure, out);
+}
+
+int cm_region_add(cm_context* ctx, int parent, int msm, int shape, int* out) {
+  if (!ctx || !out || msm < 0 || msm >= (int)ctx->msms.size() || shape < 0 || shape >= (int)ctx->shapes.size() ||
+      parent >= (int)ctx->regions.size() || parent < -1)
+    return fail(CM_EINVAL, "bad region arguments");
+  HRegion r;
+  r.parent = parent;
+  r.msm = msm;
+  r.shape = shape;
+  *out = (int)ctx->regions.size();
+  ctx->regions.push_back(r);
+  if (parent >= 0) ctx->regions[parent].children.push_back(*out);
+  ctx->dirty();
+  return 0;
+}
+
+// ---- runs
+static int check_desc(cm_context* ctx, const cm_run_desc* d) {
+  if (!ctx || !d) return fail(CM_EINVAL, "null argument");
+  if (d->precision != CM_PREC_FP64 && d->precision != CM_PREC_FP32) return fail(CM_EINVAL, "bad precision");
+  if (d->npix < 1) return fail(CM_EINVAL, "npix < 1");
+  if (d->chamber < 0 || d->chamber >= (int)ctx->regions.size()) return fail(CM_EINVAL, "bad chamber handle");
+  if (ctx->regions[d->chamber].parent != -1) return fail(CM_EINVAL, "the chamber must be a root region");
+  if (d->hist_stride < 3 || d->hist_stride > 1026) return fail(CM_EINVAL, "hist_stride out of range");
+  if (!(d->beam_width >= 0)) return fail(CM_EINVAL, "negative beam width");
+  return 0;
+}
+
+struct PixelPrep {
+  std::vector<double> center_nm, e0, e0ref;
+  std::vector<unsigned long long> prefix;
+  unsigned long long total = 0;
+};
+
+static int prep_pixels(const cm_run_desc* d, const double* center, const double* energy, const int* nprim,
+                       const int* nbins, int stride, PixelPrep& p) {
+  p.center_nm.resize(3 * (size_t)d->npix);
+  p.e0.resize(d->npix);
+  p.e0ref.resize(d->npix);
+  p.prefix.resize(d->npix + 1);
+  p.prefix[0] = 0;
+  for (int i = 0; i < d->npix; ++i) {
+    for (int k = 0; k < 3; ++k) p.center_nm[3 * i + k] = center[3 * i + k] * 1e9;
+    if (!(energy[i] > 0)) return fail(CM_EINVAL, "beam energy must be positive");
+    if (nprim[i] < 0) return fail(CM_EINVAL, "negative primary count");
+    if (nbins[i] < 1 || nbins[i] + 2 > stride) return fail(CM_EINVAL, "pixel_nbins out of range");
+    p.e0[i] = energy[i] * kFromSIeV;
+    p.e0ref[i] = energy[i] * kFromSIeV;  // BackscatterStats: FromSI::eV(beam energy)
+    p.prefix[i + 1] = p.prefix[i] + (unsigned long long)nprim[i];
+  }
+  p.total = p.prefix[d->npix];
+  return 0;
+}
+
+extern "C++" {
+template <typename T> static int up(std::vector<void*>& allocs, const std::vector<T>& v, T** out, cudaStream_t s) {
+  void* ptr;
+  CM_CUDA(cudaMalloc(&ptr, std::max<size_t>(1, v.size()) * sizeof(T)));
+  allocs.push_back(ptr);
+  CM_CUDA(cudaMemcpyAsync(ptr, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, s));
+  *out = (T*)ptr;
+  return 0;
+}
+}
+
+static int run_common(cm_context* ctx, const cm_run_desc* d, const double* center_h, const double* energy_h,
+                      const int* nprim_h, const int* nbins_h, int* nbins_dev_in, uint32_t* back_dev, uint32_t* fwd_dev,
+                      cm_run_stats* st, cudaStream_t stream) {
+  PixelPrep p;
+  int rc = prep_pixels(d, center_h, energy_h, nprim_h, nbins_h, d->hist_stride, p);
+  if (rc) return rc;
+  std::vector<void*> allocs;
+  double *c_dev, *e0_dev, *e0ref_dev;
+  unsigned long long* prefix_dev;
+  int* nbins_dev = nbins_dev_in;
+  std::vector<int> nb(nbins_h, nbins_h + d->npix);
+  if ((rc = up(allocs, p.center_nm, &c_dev, stream)) || (rc = up(allocs, p.e0, &e0_dev, stream)) ||
+      (rc = up(allocs, p.e0ref, &e0ref_dev, stream)) || (rc = up(allocs, p.prefix, &prefix_dev, stream)) ||
+      (!nbins_dev && (rc = up(allocs, nb, &nbins_dev, stream)))) {
+    for (void* a : allocs) cudaFree(a);
+    return rc;
+  }
+  cm_run_desc dd = *d;
+  dd.pixel_center = c_dev;
+  dd.pixel_energy = e0_dev;
+  dd.pixel_nbins = nbins_dev;
+  rc = d->precision == CM_PREC_FP64
+           ? run_device<double>(ctx, &dd, back_dev, fwd_dev, st, stream, prefix_dev, e0ref_dev, p.total)
+           : run_device<float>(ctx, &dd, back_dev, fwd_dev, st, stream, prefix_dev, e0ref_dev, p.total);
+  cudaStreamSynchronize(stream);
+  for (void* a : allocs) cudaFree(a);
+  return rc;
+}
+
+int cm_run(cm_context* ctx, const cm_run_desc* d, uint32_t* back, uint32_t* fwd, cm_run_stats* st) {
+  int rc = check_desc(ctx, d);
+  if (rc) return rc;
+  if (!d->pixel_center || !d->pixel_energy || !d->pixel_nprim || !d->pixel_nbins || !back || !fwd)
+    return fail(CM_EINVAL, "null array");
+  CM_CUDA(cudaSetDevice(ctx->device));
+  const size_t hbytes = (size_t)d->npix * d->hist_stride * sizeof(uint32_t);
+  uint32_t *bdev = nullptr, *fdev = nullptr;
+  CM_CUDA(cudaMalloc(&bdev, hbytes));
+  if (cudaMalloc(&fdev, hbytes) != cudaSuccess) {
+    cudaFree(bdev);
+    return fail(CM_ENOMEM, "histogram allocation failed");
+  }
+  cudaMemsetAsync(bdev, 0, hbytes, ctx->stream);
+  cudaMemsetAsync(fdev, 0, hbytes, ctx->stream);
+  rc = run_common(ctx, d, d->pixel_center, d->pixel_energy, d->pixel_nprim, d->pixel_nbins, nullptr, bdev, fdev, st,
+                  ctx->stream);
+  if (!rc) {
+    cudaMemcpyAsync(back, bdev, hbytes, cudaMemcpyDeviceToHost, ctx->stream);
+    cudaMemcpyAsync(fwd, fdev, hbytes, cudaMemcpyDeviceToHost, ctx->stream);
+    cudaStreamSynchronize(ctx->stream);
+  }
+  cudaFree(bdev);
+  cudaFree(fdev);
+  if (!rc) CM_CUDA(cudaGetLastError());
+  return rc;
+}
+
+int cm_run_device(cm_context* ctx, const cm_run_desc* d, uint32_t* back, uint32_t* fwd, cm_run_stats* st, void* stream) {
+  int rc = check_desc(ctx, d);
+  if (rc) return rc;
+  if (!d->pixel_center || !d->pixel_energy || !d->pixel_nprim || !d->pixel_nbins || !back || !fwd)
+    return fail(CM_EINVAL, "null array");
+  CM_CUDA(cudaSetDevice(ctx->device));
+  cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
+  // the small per-pixel arrays are read back to build the primary prefix and the unit conversions
+  std::vector<double> c(3 * (size_t)d->npix), e(d->npix);
+  std::vector<int> np(d->npix), nb(d->npix);
+  CM_CUDA(cudaMemcpyAsync(c.data(), d->pixel_center, c.size() * 8, cudaMemcpyDeviceToHost, s));
+  CM_CUDA(cudaMemcpyAsync(e.data(), d->pixel_energy, e.size() * 8, cudaMemcpyDeviceToHost, s));
+  CM_CUDA(cudaMemcpyAsync(np.data(), d->pixel_nprim, np.size() * 4, cudaMemcpyDeviceToHost, s));
+  CM_CUDA(cudaMemcpyAsync(nb.data(), d->pixel_nbins, nb.size() * 4, cudaMemcpyDeviceToHost, s));
+  CM_CUDA(cudaStreamSynchronize(s));
+  const size_t hbytes = (size_t)d->npix * d->hist_stride * sizeof(uint32_t);
+  CM_CUDA(cudaMemsetAsync(back, 0, hbytes, s));
+  CM_CUDA(cudaMemsetAsync(fwd, 0, hbytes, s));
+  return run_common(ctx, d, c.data(), e.data(), np.data(), nb.data(), (int*)d->pixel_nbins, back, fwd, st, s);
+}
+
+// ---- per-function entry points
+extern "C++" {
+template <typename F>
+static int eval_launch(cm_context* ctx, int n, const double* in, size_t in_per, double* out, size_t out_per, F launch) {
+  if (n < 0) return fail(CM_EINVAL, "n < 0");
+  if (n == 0) return 0;
+  CM_CUDA(cudaSetDevice(ctx->device));
+  double *din = nullptr, *dout = nullptr;
+  CM_CUDA(cudaMalloc(&din, std::max<size_t>(1, n * in_per) * 8));
+  if (cudaMalloc(&dout, n * out_per * 8) != cudaSuccess) {
+    cudaFree(din);
+    return fail(CM_ENOMEM, "eval allocation failed");
+  }
+  if (in_per) cudaMemcpy(din, in, n * in_per * 8, cudaMemcpyHostToDevice);
+  launch(din, dout, (n + 127) / 128);
+  cudaError_t e = cudaDeviceSynchronize();
+  if (e == cudaSuccess) e = cudaMemcpy(out, dout, n * out_per * 8, cudaMemcpyDeviceToHost);
+  cudaFree(din);
+  cudaFree(dout);
+  if (e != cudaSuccess) return fail(CM_ECUDA, cudaGetErrorString(e));
+  CM_CUDA(cudaGetLastError());
+  return 0;
+}
+
+}
+
+static int scene_for(cm_context* ctx, int precision) {
+  if (!ctx) return fail(CM_EINVAL, "null context");
+  CM_CUDA(cudaSetDevice(ctx->device));
+  if (precision == CM_PREC_FP64) return build_scene<double>(ctx, ctx->d64);
+  if (precision == CM_PREC_FP32) return build_scene<float>(ctx, ctx->d32);
+  return fail(CM_EINVAL, "bad precision");
+}
+
+static int mech_index(cm_context* ctx, int msm, int mech, int kind) {
+  if (msm < 0 || msm >= (int)ctx->msms.size()) return -1;
+  if (mech < 0 || mech >= (int)ctx->msms[msm].mechs.size()) return -1;
+  if (kind && ctx->msms[msm].mechs[mech].kind != kind) return -1;
+  int base = 0;
+  for (int i = 0; i < msm; ++i) base += (int)ctx->msms[i].mechs.size();
+  return base + mech;
+}
+
+int cm_eval_nistmott(cm_context* ctx, int Z, int n, const double* E, const double* u, double* sigma, double* theta,
+                     int precision) {
+  int rc = scene_for(ctx, precision);
+  if (rc) return rc;
+  auto it = ctx->mott.find(Z);
+  if (it == ctx->mott.end()) return fail(CM_EINVAL, "element not loaded");
+  const int mi = (int)std::distance(ctx->mott.begin(), it);
+  std::vector<double> in(3 * (size_t)n), out(2 * (size_t)n);
+  for (int i = 0; i < n; ++i) {
+    in[i] = E[i];
+    in[n + 2 * i] = u[2 * i];
+    in[n + 2 * i + 1] = u[2 * i + 1];
+  }
+  rc = eval_launch(ctx, 1, in.data(), 3 * (size_t)n, out.data(), 2 * (size_t)n, [&](double* din, double* dout, int) {
+    const int g = (n + 127) / 128;
+    if (precision == CM_PREC_FP64)
+      k_eval_nistmott<double><<<g, 128>>>(ctx->d64.view, mi, n, din, din + n, dout, dout + n);
+    else
+      k_eval_nistmott<float><<<g, 128>>>(ctx->d32.view, mi, n, din, din + n, dout, dout + n);
+  });
+  if (rc) return rc;
+  for (int i = 0; i < n; ++i) {
+    sigma[i] = out[i];
+    theta[i] = out[n + i];
+  }
+  return 0;
+}
+
+int cm_eval_table(cm_context* ctx, int table, int n, const double* x, int order, double* out, int precision) {
+  int rc = scene_for(ctx, precision);
+  if (rc) return rc;
+  if (table < 0 || table >= (int)ctx->tables.size()) return fail(CM_EINVAL, "bad table handle");
+  const HTable& t = ctx->tables[table];
+  const double f0 = t.role >= 1 ? kFromSIeV : 1.0;
+  const double vf = t.role == 1 ? 1e-9 : t.role == 4 ? kFromSIeV : 1.0;
+  return eval_launch(ctx, n, x, 3, out, 1, [&](double* din, double* dout, int g) {
+    if (precision == CM_PREC_FP64)
+      k_eval_table<double><<<g, 128>>>(ctx->d64.view, table, n, din, f0, vf, order, dout);
+    else
+      k_eval_table<float><<<g, 128>>>(ctx->d32.view, table, n, din, f0, vf, order, dout);
+  });
+}
+
+int cm_eval_tabulated(cm_context* ctx, int msm, int mech, int n, const double* in, double* out, int precision) {
+  int rc = scene_for(ctx, precision);
+  if (rc) return rc;
+  const int k = mech_index(ctx, msm, mech, MECH_TABULATED);
+  if (k < 0) return fail(CM_EINVAL, "not a TabulatedInelasticSM");
+  return eval_launch(ctx, n, in, 9, out, 12, [&](double* din, double* dout, int g) {
+    if (precision == CM_PREC_FP64) k_eval_tabulated<double><<<g, 128>>>(ctx->d64.view, k, n, din, dout);
+    else k_eval_tabulated<float><<<g, 128>>>(ctx->d32.view, k, n, din, dout);
+  });
+}
+
+int cm_eval_elastic(cm_context* ctx, int msm, int mech, int n, const double* in, double* out, int precision) {
+  int rc = scene_for(ctx, precision);
+  if (rc) return rc;
+  const int k = mech_index(ctx, msm, mech, MECH_NISTMOTT);
+  if (k < 0) return fail(CM_EINVAL, "not a SelectableElasticSM");
+  return eval_launch(ctx, n, in, 7, out, 6, [&](double* din, double* dout, int g) {
+    if (precision == CM_PREC_FP64) k_eval_elastic<double><<<g, 128>>>(ctx->d64.view, k, n, din, dout);
+    else k_eval_elastic<float><<<g, 128>>>(ctx->d32.view, k, n, din, dout);
+  });
+}
+
+int cm_eval_csd(cm_context* ctx, int msm, int n, const double* in, double* out, int precision) {
+  int rc = scene_for(ctx, precision);
+  if (rc) return rc;
+  if (msm < 0 || msm >= (int)ctx->msms.size()) return fail(CM_EINVAL, "bad scatter model handle");
+  return eval_launch(ctx, n, in, 2, out, 3, [&](double* din, double* dout, int g) {
+    if (precision == CM_PREC_FP64) k_eval_csd<double><<<g, 128>>>(ctx->d64.view, msm, n, din, dout);
+    else k_eval_csd<float><<<g, 128>>>(ctx->d32.view, msm, n, din, dout);
+  });
+}
+
+int cm_eval_phonon(cm_context* ctx, int msm, int mech, int n, const double* in, double* out, int precision) {
+  int rc = scene_for(ctx, precision);
+  if (rc) return rc;
+  const int k = mech_index(ctx, msm, mech, MECH_PHONON);
+  if (k < 0) return fail(CM_EINVAL, "not a GanachaudMokraniPhononInelasticSM");
+  return eval_launch(ctx, n, in, 5, out, 6, [&](double* din, double* dout, int g) {
+    if (precision == CM_PREC_FP64) k_eval_phonon<double><<<g, 128>>>(ctx->d64.view, k, n, din, dout);
+    else k_eval_phonon<float><<<g, 128>>>(ctx->d32.view, k, n, din, dout);
+  });
+}
+
+int cm_eval_shape(cm_context* ctx, int shape, int n, const double* p01, double* out) {
+  int rc = scene_for(ctx, CM_PREC_FP64);
+  if (rc) return rc;
+  if (shape < 0 || shape >= (int)ctx->shapes.size()) return fail(CM_EINVAL, "bad shape handle");
+  return eval_launch(ctx, n, p01, 6, out, 5, [&](double* din, double* dout, int g) {
+    k_eval_shape<<<g, 128>>>(ctx->d64.view, shape, n, din, dout);
+  });
+}
+
+int cm_eval_barrier(cm_context* ctx, int from, int to, int n, const double* in, double* out, int precision) {
+  int rc = scene_for(ctx, precision);
+  if (rc) return rc;
+  if (from < 0 || to < 0 || from >= (int)ctx->regions.size() || to >= (int)ctx->regions.size())
+    return fail(CM_EINVAL, "bad region handle");
+  return eval_launch(ctx, n, in, 6, out, 8, [&](double* din, double* dout, int g) {
+    if (precision == CM_PREC_FP64) k_eval_barrier<double><<<g, 128>>>(ctx->d64.view, from, to, n, din, dout);
+    else k_eval_barrier<float><<<g, 128>>>(ctx->d32.view, from, to, n, din, dout);
+  });
+}
+
+int cm_eval_freepath(cm_context* ctx, int msm, int n, const double* in, double* out, int precision) {
+  int rc = scene_for(ctx, precision);
+  if (rc) return rc;
+  if (msm < 0 || msm >= (int)ctx->msms.size()) return fail(CM_EINVAL, "bad scatter model handle");
+  return eval_launch(ctx, n, in, 2, out, 1, [&](double* din, double* dout, int g) {
+    if (precision == CM_PREC_FP64) k_eval_freepath<double><<<g, 128>>>(ctx->d64.view, msm, n, din, dout);
+    else k_eval_freepath<float><<<g, 128>>>(ctx->d32.view, msm, n, din, dout);
+  });
+}
+
+}  // extern "C"

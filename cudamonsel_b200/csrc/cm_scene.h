@@ -1,0 +1,124 @@
+// cm_scene.h -- flattened scene description shared by host and device.
+//
+// The host facade records the reference's object graph (Region tree,
+// NormalShapes, MONSEL_MaterialScatterModel with its ScatterMechanisms) and
+// flattens it into these plain arrays.  Device units: energy in eV, length in
+// nm, rates in 1/nm.  Geometry is double precision in every mode.
+#pragma once
+#include <stdint.h>
+
+namespace cm {
+
+constexpr int kMaxMech = 8;
+constexpr int kMaxElem = 8;
+constexpr int kMaxCore = 16;
+constexpr int kMaxShapeDepth = 4;
+
+// NISTMonte/MonteCarloSS.cu:32-33 in nm
+constexpr double kChamberRadiusNm = 0.1e9;
+constexpr double kSmallDispNm = 1.0e-6;
+constexpr double kPi = 3.14159265358979323846;
+
+enum ShapeKind : int { SHAPE_SPHERE = 1, SHAPE_PLANES = 2, SHAPE_INTERSECTION = 3 };
+enum MechKind : int { MECH_NISTMOTT = 1, MECH_TABULATED = 2, MECH_FITTED = 3, MECH_PHONON = 4, MECH_POLARON = 5 };
+
+struct Shape {
+  int kind;
+  int a, b;          // intersection children
+  int plane0, np;    // planes [plane0, plane0+np)
+  double c[3], r;    // sphere (nm)
+};
+
+struct Plane {
+  double n[3];
+  double p[3];       // nm
+};
+
+struct Region {
+  int parent, msm, shape;
+  int child0, nchild;  // children indices in Scene::children
+};
+
+// JoyLuoNieminenCSD (JMONSEL/JoyLuoNieminenCSD.cu:42-121) in eV/nm units
+struct Jln {
+  int nce;
+  double coef[kMaxElem];     // eV^2 / nm
+  double recipJ[kMaxElem];   // 1/eV
+  double beta[kMaxElem];
+  double breakE, gamma, minE;  // eV, eV^-1.5 nm^-1, eV
+};
+
+struct Mech {
+  int kind;
+  // NISTMott via SelectableElasticSM: per element mott index and rate factor
+  int nel;
+  int mott[kMaxElem];        // index into Scene::mott
+  double kel[kMaxElem];      // a0^2 * scalefactor * density * N_A in nm^-1 per (table unit)
+  double kbrown[kMaxElem];   // the same factor for a Browning/Rutherford cross section in nm^2
+  // TabulatedInelasticSM (JMONSEL/TabulatedInelasticSM.cu:461-498), energies in eV
+  int methodSE;
+  int tIIMFP, tRed, tTheta, tSEE0;
+  double energyOffset, minEgenSE, rateMult, energyCBbottom, bandgap, energyGap, offsetFermiEnergy, bEref;
+  double eiDomain0, eiDomain1, iimfpDomain0, rangeSE0lo, rangeSE0hi;
+  int ncore;
+  double core[kMaxCore];
+  // FittedInelSM
+  double energySEgen, eFermi;
+  Jln csd;
+  // phonon / polaron
+  double phononE, prefactor, extinction, cutoff;
+};
+
+struct Msm {
+  int material;
+  int vacuum;
+  int nmech, mech0;          // mechanisms [mech0, mech0+nmech)
+  int csd;                   // 0 = ZeroCSD, 1 = JoyLuoNieminenCSD
+  Jln jln;
+  double minE;               // eV (may be -inf)
+  double ecb;                // E_CB bottom of this material, eV
+  double u0;                 // barrier's u0 (= E_CB of the material it was built for), eV
+  int classical;
+  double lambda, lambdaFactor;  // lambdaFactor in 1/sqrt(eV)
+};
+
+// NISTMottRS (method 1) per element; the tables live in the precision blob
+struct Mott {
+  int Z;
+  int off_spwem, off_x1;     // element offsets into the table blob
+  double extrapolateBelowEnergy;  // eV
+  double sfBrowning;
+  double zp17, zp2, zp3;
+  double rutherfordA, rutherfordB;  // sigma = A / (E + B) in nm^2 with E in eV
+  double rutherfordAlpha;           // alpha = rutherfordAlpha / E
+};
+
+// NUTableInterpolation (dims 1..3) in the precision blob
+struct Table {
+  int dim;
+  int n[3];
+  int off_x[3];
+  int off_v;
+  double domain[3][2];
+  double range[2];
+};
+
+// The whole scene as device pointers (one struct passed by value to kernels)
+template <typename R>
+struct SceneView {
+  const Shape* shapes;
+  const Plane* planes;
+  const Region* regions;
+  const int* children;
+  const Msm* msms;
+  const Mech* mechs;
+  const Mott* mott;
+  const Table* tables;
+  const R* blob;             // table data in compute precision
+  int chamber;
+  int options;               // bit 0: JMONSEL fixes
+  double dl50, param;        // NISTMott log-energy grid (eV)
+  double maxMott;            // NISTMottRS MAX_NISTMOTT in eV
+};
+
+}  // namespace cm

@@ -1,0 +1,256 @@
+"""Scene descriptions in the reference's terms, replayable into the engine.
+
+A SceneSpec records the same construction calls a CudaMONSEL driver makes
+(JMONSELTests/LinesOnLayers.cu:80-282): SEmaterials, MONSEL_MaterialScatterModel
+with its mechanisms, NormalShapes and the Region tree, in SI units.  ``replay``
+sends those calls to a backend object with the same method names; the CUDA
+engine (capi.Engine via EngineBackend) is the product backend.
+
+Standard scenes:
+  * ``halfspace``: a flat Si sample filling z >= 0 in vacuum (the surface plane
+    of LinesOnLayers.cu:245-250), NISTMott + TabulatedInelasticSM(method 3,
+    offset 13.54 eV) + classical ExpQMBarrierSM;
+  * ``lines``: the same Si substrate carrying PMMA trapezoid lines built by
+    NShapes::createLine, PMMA modelled as LinesOnLayers.cu:86-127 (NISTMott,
+    FittedInelSM, polaron trap, Joy-Luo-Nieminen CSD).
+"""
+import math
+
+import numpy as np
+
+from . import data
+
+EV = 1.60217653e-19  # ToSI::eV factor
+
+
+def eV(x):
+    """ToSI::eV (EPQLibrary/ToSI.cu:34-37)."""
+    return EV * x
+
+
+class H:
+    """Placeholder for a handle produced by an earlier recorded call."""
+    __slots__ = ("idx",)
+
+    def __init__(self, idx):
+        self.idx = idx
+
+
+class SceneSpec:
+    def __init__(self):
+        self.ops = []
+        self.elements = set()
+        self.options = 0
+
+    def _op(self, name, *args):
+        self.ops.append((name, args))
+        return H(len(self.ops) - 1)
+
+    def table(self, path):
+        return self._op("table", path)
+
+    def material(self, Z, A, wf, density, workfunction, ecb, bandgap, core=()):
+        self.elements.update(Z)
+        return self._op("material", list(Z), list(A), list(wf), density, workfunction, ecb, bandgap, list(core))
+
+    def msm(self, material):
+        return self._op("msm", material)
+
+    def nistmott(self, msm, method=1):
+        return self._op("nistmott", msm, method)
+
+    def tabulated(self, msm, method_se, offset, tables):
+        return self._op("tabulated", msm, method_se, offset, list(tables))
+
+    def fitted(self, msm, energy_se_gen, break_e):
+        return self._op("fitted", msm, energy_se_gen, break_e)
+
+    def phonon(self, msm, ratemult, phonon_e, temperature, eps0, eps_inf):
+        return self._op("phonon", msm, ratemult, phonon_e, temperature, eps0, eps_inf)
+
+    def polaron(self, msm, prefactor, extinction):
+        return self._op("polaron", msm, prefactor, extinction)
+
+    def csd_jln(self, msm, break_e):
+        return self._op("csd_jln", msm, break_e)
+
+    def min_e(self, msm, e):
+        return self._op("min_e", msm, e)
+
+    def sphere(self, c, r):
+        return self._op("sphere", list(c), r)
+
+    def planes(self, normals, points):
+        return self._op("planes", list(np.ravel(normals)), list(np.ravel(points)))
+
+    def intersection(self, a, b):
+        return self._op("intersection", a, b)
+
+    def translate(self, shape, d):
+        return self._op("translate", shape, list(d))
+
+    def line(self, topz, width, length, thetal, thetar):
+        return self._op("line", topz, width, length, thetal, thetar)
+
+    def region(self, parent, msm, shape):
+        return self._op("region", -1 if parent is None else parent, msm, shape)
+
+
+def _resolve(a, res):
+    if isinstance(a, H):
+        return res[a.idx]
+    if isinstance(a, list):
+        return [_resolve(x, res) for x in a]
+    return a
+
+
+def replay(spec, backend):
+    """Issue the recorded calls on backend; returns the backend handles (index = H.idx)."""
+    backend.begin(spec)
+    res = []
+    for name, args in spec.ops:
+        res.append(getattr(backend, name)(*[_resolve(a, res) for a in args]))
+    return res
+
+
+class EngineBackend:
+    """Adapts capi.Engine: loads the NIST Mott data and parses table files."""
+
+    def __init__(self, engine):
+        self.e = engine
+
+    def begin(self, spec):
+        self.e.set_options(spec.options)
+        for Z in sorted(spec.elements):
+            spwem, x1 = data.read_mott(Z)
+            self.e.mott(Z, spwem, x1)
+
+    def table(self, path):
+        dim, n, axes, vals = data.read_nu_table(path)
+        return self.e.table(dim, n, axes, vals)
+
+    def __getattr__(self, name):
+        return getattr(self.e, name)
+
+
+# ---------------------------------------------------------------- materials (LinesOnLayers.cu)
+def vacuum(spec):
+    """SEmaterial() + ExpQMBarrierSM(vacuum) + MONSEL_MaterialScatterModel (LinesOnLayers.cu:80-84)."""
+    mat = spec.material([], [], [], 0.0, 0.0, 0.0, 0.0)
+    return spec.msm(mat)
+
+
+def silicon(spec, tables=None, phonon=False):
+    """Si as LinesOnLayers.cu:172-205 (phonon mechanism optional)."""
+    workfun, bandgap = 4.85, 1.1
+    efermi = -bandgap
+    potU = -workfun - efermi
+    mat = spec.material([14], [data.atomic_weight(14)], [1.0], 2330.0, eV(workfun), eV(potU), eV(bandgap),
+                        [eV(99.2), eV(99.8), eV(149.7), eV(1839.0)])
+    m = spec.msm(mat)
+    spec.nistmott(m, 1)
+    paths = tables or data.si_tables()
+    t = [spec.table(p) for p in paths]
+    spec.tabulated(m, 3, eV(13.54), t)
+    if phonon:
+        spec.phonon(m, 3.0, eV(0.063), 300.0, 11.7, 1.0)
+    return m
+
+
+# Element order and normalized weight fractions of C5O2H8 as the reference's
+# Composition::defineByMoleFraction yields them (element iteration order of its
+# std::unordered_set<const Element*>: H, O, C).
+PMMA_Z = (1, 8, 6)
+PMMA_WF = (0.080541919183721306, 0.3196178155473462, 0.59984026526893253)
+
+
+def pmma(spec):
+    """PMMA as LinesOnLayers.cu:86-127."""
+    breakE = eV(45.0)
+    workfun, bandgap = 5.5, 5.0
+    efermi = -bandgap
+    potU = -workfun - efermi
+    mat = spec.material(list(PMMA_Z), [data.atomic_weight(z) for z in PMMA_Z], list(PMMA_WF), 1190.0, eV(workfun),
+                        eV(potU), eV(bandgap))
+    m = spec.msm(mat)
+    spec.nistmott(m, 1)
+    spec.fitted(m, eV(65.4), breakE)
+    spec.polaron(m, 2.0e7, 1.0 / eV(4.0))
+    spec.csd_jln(m, breakE)
+    return m
+
+
+class Scene:
+    """A built SceneSpec plus the handles a caller needs."""
+
+    def __init__(self, spec, chamber, **handles):
+        self.spec = spec
+        self.chamber = chamber
+        self.h = handles
+
+
+def halfspace(tables=None):
+    """Flat Si filling z >= 0 (plane normal (0,0,-1) through the origin), in a 0.1 m vacuum chamber."""
+    s = SceneSpec()
+    vac = vacuum(s)
+    si = silicon(s, tables)
+    sphere = s.sphere([0.0, 0.0, 0.0], 0.1)
+    chamber = s.region(None, vac, sphere)
+    surf = s.planes([0.0, 0.0, -1.0], [0.0, 0.0, 0.0])
+    sireg = s.region(chamber, si, surf)
+    return Scene(s, chamber, vac=vac, si=si, si_region=sireg, surface=surf)
+
+
+def lines(nlines=3, pitch=200e-9, height=100e-9, width=40e-9, length=1e-6, angle_deg=3.0, tables=None):
+    """Si substrate carrying nlines PMMA lines (NShapes::createLine) centred at x = (i - (n-1)/2) * pitch."""
+    s = SceneSpec()
+    vac = vacuum(s)
+    si = silicon(s, tables)
+    pm = pmma(s)
+    sphere = s.sphere([0.0, 0.0, 0.0], 0.1)
+    chamber = s.region(None, vac, sphere)
+    surf = s.planes([0.0, 0.0, -1.0], [0.0, 0.0, 0.0])
+    sireg = s.region(chamber, si, surf)
+    th = angle_deg * math.pi / 180.0
+    line_regions = []
+    for i in range(nlines):
+        ln = s.line(-height, width, length, th, th)
+        s.translate(ln, [(i - (nlines - 1) / 2.0) * pitch, 0.0, 0.0])
+        line_regions.append(s.region(chamber, pm, ln))
+    return Scene(s, chamber, vac=vac, si=si, pmma=pm, si_region=sireg, lines=line_regions)
+
+
+def build_engine(scene, engine):
+    """Replay a Scene into a capi.Engine; returns {name: engine handle}."""
+    res = replay(scene.spec, EngineBackend(engine))
+    out = {"chamber": res[scene.chamber.idx]}
+    for k, v in scene.h.items():
+        out[k] = [res[x.idx] for x in v] if isinstance(v, list) else res[v.idx]
+    return out
+
+
+def linescan_pixels(npix=256, step=1e-9, y=0.0, z=-120e-9):
+    """Landing points across the lines: x = (i - (npix-1)/2) * step."""
+    x = (np.arange(npix) - (npix - 1) / 2.0) * step
+    return np.stack([x, np.full(npix, y), np.full(npix, z)], axis=1)
+
+
+def yields(back, nprim, beam_eV, nbins):
+    """BSE and SE yields per pixel as LinesOnLayers.cu:366-376 computes them.
+
+    back is the backscatter energy histogram with under/overflow (index = bin + 1)."""
+    back = np.atleast_2d(back).astype(np.int64)
+    nprim = np.broadcast_to(np.asarray(nprim), (back.shape[0],))
+    beam_eV = np.broadcast_to(np.asarray(beam_eV, dtype=np.float64), (back.shape[0],))
+    nbins = np.broadcast_to(np.asarray(nbins), (back.shape[0],))
+    bse = np.zeros(back.shape[0])
+    se = np.zeros(back.shape[0])
+    for p in range(back.shape[0]):
+        per_bin = beam_eV[p] / nbins[p]
+        max_se_bin = 50.0 / per_bin
+        total_se = int(back[p, 1:1 + int(max_se_bin)].sum())  # counts(j), j < (int)maxSEbin
+        sef = float(np.float32(np.float32(total_se) / np.float32(nprim[p])))
+        total = int(back[p, :nbins[p] + 2].sum())
+        bse[p] = total / float(nprim[p]) - sef
+        se[p] = sef
+    return bse, se

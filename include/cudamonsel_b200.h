@@ -1,0 +1,165 @@
+/*
+ * cudamonsel_b200.h -- C ABI of the B200 electron-transport engine.
+ *
+ * The engine replaces the CPU trajectory loop of CudaMONSEL
+ * (NISTMonte/MonteCarloSS.cu:107-231 and everything it calls) with CUDA
+ * kernels for sm_100a.  A caller describes the same objects the reference's
+ * C++ API builds -- SEmaterial, MONSEL_MaterialScatterModel and its
+ * ScatterMechanism / SlowingDownAlg / BarrierScatterMechanism plug-ins,
+ * NormalShapes, the Region tree, the GaussianBeam and BackscatterStats -- and
+ * then runs trajectories for a list of beam landing points (pixels).
+ *
+ * Conventions
+ *   - Units are the reference's: SI (J, m, m^2, kg/m^3).
+ *   - Every function returns 0 on success and a negative CM_E* code on error;
+ *     cm_last_error() then describes the failure (thread-local).
+ *   - Object handles are small non-negative ints returned through out-params.
+ *   - Pointers are host pointers unless the name says _device.
+ *   - A context is not thread-safe; use one per host thread.
+ *
+ * Reference paths below are relative to CudaMONSEL/CudaMONSEL/gov/nist/.
+ */
+#ifndef CUDAMONSEL_B200_H
+#define CUDAMONSEL_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CM_OK 0
+#define CM_EINVAL -1    /* bad argument or handle */
+#define CM_ECUDA -2     /* CUDA runtime error */
+#define CM_ENOMEM -3    /* device allocation failed */
+#define CM_ESTATE -4    /* scene incomplete or inconsistent */
+#define CM_EOVERFLOW -5 /* a device queue overflowed (secondary pool too small) */
+#define CM_ELIMIT -6    /* iteration limit reached before all trajectories ended */
+
+#define CM_PREC_FP64 0  /* plain form: all transport arithmetic in double */
+#define CM_PREC_FP32 1  /* batched form: float physics, double positions and plane solves */
+
+#define CM_OPT_JMONSEL_FIXES 1 /* refraction at barriers, d3 abscissae; default is the reference as written */
+
+typedef struct cm_context cm_context;
+
+/* ---- context -------------------------------------------------------------- */
+int cm_context_create(int device, cm_context** out);
+int cm_context_destroy(cm_context* ctx);
+const char* cm_last_error(void);
+int cm_set_options(cm_context* ctx, int options);
+int cm_version(void);
+
+/* ---- data ------------------------------------------------------------------- */
+/* NIST SRD-64 elastic table of one element, as NISTMottScatteringAngle::loadData
+ * reads it (EPQLibrary/NISTMottScatteringAngle.cu:44-66): 61 cross sections in
+ * Bohr radii squared, then 61 x 201 quantiles (row = energy node). */
+int cm_add_mott_element(cm_context* ctx, int Z, const double* spwem61, const double* x1_61x201);
+/* A NUTableInterpolation table (JMONSEL/NUTableInterpolation.cu:117-228):
+ * dim in 1..3, n[dim] grid sizes, the axes concatenated, values last index fastest. */
+int cm_add_table(cm_context* ctx, int dim, const int* n, const double* axes, const double* values, int* out_table);
+
+/* ---- materials and scatter models ---------------------------------------- */
+/* SEmaterial (JMONSEL/SEmaterial.cu) with its Composition: nel elements given by
+ * Z, atomic weight (g/mol) and normalized weight fraction.  nel = 0 is vacuum. */
+int cm_add_material(cm_context* ctx, int nel, const int* Z, const double* atomic_weight, const double* weight_fraction,
+                    double density, double workfunction, double energy_cb_bottom, double bandgap, int ncore,
+                    const double* core_energies, int* out_material);
+/* MONSEL_MaterialScatterModel(mat, ExpQMBarrierSM(mat)) (JMONSEL/MONSEL_MaterialScatterModel.cu:13-37) */
+int cm_add_msm(cm_context* ctx, int material, int* out_msm);
+/* SelectableElasticSM(mat, NISTMottRS::Factory) (JMONSEL/SelectableElasticSM.cu:10-18); method 1 only */
+int cm_msm_add_nistmott(cm_context* ctx, int msm, int method, int* out_mech);
+/* TabulatedInelasticSM(mat, methodSE, tables, energyOffset) (JMONSEL/TabulatedInelasticSM.cu:23-66);
+ * tables = {IIMFP, reduced deltaE, theta, SE E0} */
+int cm_msm_add_tabulated(cm_context* ctx, int msm, int method_se, double energy_offset, const int tables[4], int* out_mech);
+/* FittedInelSM(mat, energySEgen, JoyLuoNieminenCSD(mat, breakE)) (JMONSEL/FittedInelSM.cu:8-11) */
+int cm_msm_add_fitted(cm_context* ctx, int msm, double energy_se_gen, double break_e, int* out_mech);
+/* GanachaudMokraniPhononInelasticSM (JMONSEL/GanachaudMokraniPhononInelasticSM.cu:8-17) */
+int cm_msm_add_phonon(cm_context* ctx, int msm, double ratemult, double phonon_e, double temperature, double eps0,
+                      double eps_infinity, int* out_mech);
+/* GanachaudMokraniPolaronTrapSM (JMONSEL/GanachaudMokraniPolaronTrapSM.cu:8-12) */
+int cm_msm_add_polaron(cm_context* ctx, int msm, double prefactor, double extinction, int* out_mech);
+/* MONSEL_MaterialScatterModel::setCSD(JoyLuoNieminenCSD(mat, breakE)) (MONSEL_MaterialScatterModel.cu:146-152) */
+int cm_msm_set_csd_jln(cm_context* ctx, int msm, double break_e);
+/* MONSEL_MaterialScatterModel::setMinEforTracking */
+int cm_msm_set_min_e(cm_context* ctx, int msm, double min_e);
+/* ExpQMBarrierSM(mat) classical (1) or ExpQMBarrierSM(mat, lambda) (0) (JMONSEL/ExpQMBarrierSM.cu:12-28) */
+int cm_msm_set_barrier(cm_context* ctx, int msm, int classical, double lambda);
+
+/* ---- shapes and regions ------------------------------------------------------ */
+int cm_shape_sphere(cm_context* ctx, const double center[3], double radius, int* out_shape);   /* NISTMonte/Sphere.cu */
+/* NormalMultiPlaneShape with n planes (normal, point) (JMONSEL/NormalMultiPlaneShape.cu) */
+int cm_shape_planes(cm_context* ctx, int n, const double* normals, const double* points, int* out_shape);
+int cm_shape_intersection(cm_context* ctx, int a, int b, int* out_shape); /* JMONSEL/NormalIntersectionShape.cu */
+int cm_shape_translate(cm_context* ctx, int shape, const double distance[3]);
+/* NShapes::createLine(topz, width, length, thetal, thetar, 0, 0) (JMONSEL/NShapes.cu:55-149), zero corner radii */
+int cm_shape_line(cm_context* ctx, double topz, double width, double length, double thetal, double thetar, int* out_shape);
+/* Region(parent, msm, shape) (NISTMonte/RegionBase.cu:193-200); parent -1 makes the chamber */
+int cm_region_add(cm_context* ctx, int parent, int msm, int shape, int* out_region);
+
+/* ---- trajectories ---------------------------------------------------------- */
+/* One run: for each pixel p, pixel_nprim[p] trajectories from a GaussianBeam of
+ * width beam_width centred at pixel_center[3p..3p+2] with energy pixel_energy[p],
+ * each tallied by a BackscatterStats(monte, pixel_nbins[p]) attached for that
+ * pixel (NISTMonte/BackscatterStats.cu:107-181). */
+typedef struct {
+  int chamber;                 /* region handle of the chamber */
+  int precision;               /* CM_PREC_FP64 or CM_PREC_FP32 */
+  int npix;
+  double beam_width;           /* m (Gaussian sigma) */
+  const double* pixel_center;  /* [3*npix] m */
+  const double* pixel_energy;  /* [npix] J */
+  const int* pixel_nprim;      /* [npix] */
+  const int* pixel_nbins;      /* [npix], 1..1024 */
+  uint64_t seed;
+  int hist_stride;             /* >= max(pixel_nbins) + 2 */
+  int wave;                    /* electrons per wave; 0 = default */
+  int max_iterations;          /* 0 = default */
+} cm_run_desc;
+
+typedef struct {
+  int64_t primaries, steps, scatter_events, barrier_events, escapes, secondaries, iterations;
+  double device_ms;            /* time of the transport loop on the device */
+} cm_run_stats;
+
+/* back/fwd: [npix * hist_stride] counts, index = histogram bin + 1 (0 = underflow,
+ * nbins + 1 = overflow), exactly Histogram::counts(bin) of the reference
+ * (Utility/Histogram.cu:73-116).  All host pointers. */
+int cm_run(cm_context* ctx, const cm_run_desc* desc, uint32_t* back, uint32_t* fwd, cm_run_stats* stats);
+/* Same with inputs (pixel arrays) and outputs (back, fwd) already in device memory. */
+int cm_run_device(cm_context* ctx, const cm_run_desc* desc_device_arrays, uint32_t* back_device, uint32_t* fwd_device,
+                  cm_run_stats* stats, void* stream);
+
+/* ---- per-function entry points (parity checks; host arrays, SI units) -------
+ * Deviates are injected from u arrays so that each result can be compared
+ * with the reference on the same inputs.  precision selects the kernel. */
+/* NISTMottRS::totalCrossSection / randomScatteringAngle (JMONSEL/NISTMottRS.cu:103-154); u[2n] */
+int cm_eval_nistmott(cm_context* ctx, int Z, int n, const double* E, const double* u, double* sigma, double* theta,
+                     int precision);
+/* NUTableInterpolation::interpolate (JMONSEL/NUTableInterpolation.cu:98-115); x[3n] */
+int cm_eval_table(cm_context* ctx, int table, int n, const double* x, int order, double* out, int precision);
+/* TabulatedInelasticSM::scatterRate + scatter (JMONSEL/TabulatedInelasticSM.cu:209-459);
+ * in[9n] = E theta phi u0..u5, out[12n] = rate E' dx dy dz hasSE ESE sdx sdy sdz ndev 0 */
+int cm_eval_tabulated(cm_context* ctx, int msm, int mech, int n, const double* in, double* out, int precision);
+/* SelectableElasticSM::scatterRate + scatter (JMONSEL/SelectableElasticSM.cu:42-67);
+ * in[7n] = E theta phi u0..u3, out[6n] = rate dx dy dz Z ndev */
+int cm_eval_elastic(cm_context* ctx, int msm, int mech, int n, const double* in, double* out, int precision);
+/* JoyLuoNieminenCSD::compute, FittedInelSM and polaron rates of a PMMA-like model;
+ * in[2n] = E len, out[3n] */
+int cm_eval_csd(cm_context* ctx, int msm, int n, const double* in, double* out, int precision);
+/* GanachaudMokraniPhononInelasticSM (JMONSEL/GanachaudMokraniPhononInelasticSM.cu:19-72);
+ * in[5n] = E theta phi u0 u1, out[6n] = rate E' dx dy dz Eprev */
+int cm_eval_phonon(cm_context* ctx, int msm, int mech, int n, const double* in, double* out, int precision);
+/* NormalShape::getFirstNormal + Shape::contains (double precision); p01[6n], out[5n] = nx ny nz u inside */
+int cm_eval_shape(cm_context* ctx, int shape, int n, const double* p01, double* out);
+/* ExpQMBarrierSM::barrierScatter + the nudge of MonteCarloSS::takeStep
+ * (JMONSEL/ExpQMBarrierSM.cu:50-219); in[6n] = E theta phi x y z, out[7n] = E' dx dy dz x y z ... see implementation */
+int cm_eval_barrier(cm_context* ctx, int from_region, int to_region, int n, const double* in, double* out, int precision);
+/* MONSEL_MaterialScatterModel::randomMeanPathLength (MONSEL_MaterialScatterModel.cu:64-91); in[2n] = E u */
+int cm_eval_freepath(cm_context* ctx, int msm, int n, const double* in, double* out, int precision);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
