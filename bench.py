@@ -1,0 +1,329 @@
+"""Throughput of the electron-transport hot path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (one step): the linescan -- three PMMA trapezoid lines (height 100 nm,
+bottom width 40 nm, 3 deg sidewalls, pitch 200 nm) on a Si substrate, a 500 eV
+Gaussian beam (sigma 1 nm) landing on 256 pixels 1 nm apart across the
+middle line, 2000 primaries per pixel (512 000 primaries), synthetic tables.
+Metric: primary electrons per second, FP32 transport (FP64 positions and
+plane solves), with the linescan yields checked against an FP64 run of the
+same workload.  Under torchrun each rank runs the full linescan with its own
+random streams (weak scaling, no collective on the data path); the time is
+the max over ranks.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+NPIX, NPRIM, BEAM_EV, NBINS = 256, 2000, 500.0, 50
+METRIC = "primary electrons/s at <=1% BSE/SE yield error vs FP64"
+WORKLOAD = ("linescan: 3 PMMA lines (h 100 nm, bottom w 40 nm, 3 deg, pitch 200 nm) on Si, 500 eV Gaussian "
+            "sigma 1 nm, 256 px x 1 nm, 2000 primaries/px (512k primaries)")
+BYTES_PER_STEP = 128  # algorithmic bytes per electron-step: a 64 B SoA record read and written
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+
+    def __init__(self, index):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(index), "--query-gpu=" + q, "--format=csv,noheader,nounits",
+                                       "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        self.p.terminate()
+        try:
+            self.p.wait(5)
+        except subprocess.TimeoutExpired:
+            self.p.kill()
+        self.f.flush()
+        rows = [l.split(",") for l in open(self.f.name).read().splitlines() if l.strip()]
+        os.unlink(self.f.name)
+        sm, mx, reasons = [], 0.0, set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                mx = max(mx, float(r[2]))
+                for n, v in zip(names, r[5:9]):
+                    if "Active" in v and "Not" not in v:
+                        reasons.add(n)
+            except (ValueError, IndexError):
+                continue
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx or None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def linescan_inputs(rank):
+    from cudamonsel_b200 import scenes
+    centers = scenes.linescan_pixels(NPIX, 1e-9, 0.0, -120e-9)
+    keys = (np.arange(NPIX, dtype=np.uint64) + np.uint64(1_000_003 * (rank + 1)))
+    return centers, keys
+
+
+# ------------------------------------------------------------------ CPU arms
+def ref_binary():
+    exe = os.path.join(ROOT, "oracle", "_ref", "ref_driver")
+    data_ok = os.path.isdir(os.path.join(ROOT, "oracle", "_ref", "gov"))
+    return exe if os.path.exists(exe) and data_ok else None
+
+
+def cpu_sample(nproc, pixels_per_proc, nprim, seed):
+    """Run the reference's compiled CPU code (or the oracle port) on nproc processes, each on its
+    own pixels of the linescan; returns (primaries, seconds of the slowest transport loop, kind)."""
+    from cudamonsel_b200 import data
+    exe = ref_binary()
+    x0 = -(NPIX - 1) / 2.0
+    if exe:
+        procs = []
+        for p in range(nproc):
+            start = x0 + (p * 37) % NPIX
+            procs.append(subprocess.Popen([exe, "run2", str(nprim), str(seed + p), data.SI_TABLES, "%g" % start, "1",
+                                           str(pixels_per_proc), "%g" % BEAM_EV], cwd=os.path.dirname(exe),
+                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True))
+        secs = []
+        for pr in procs:
+            out, _ = pr.communicate()
+            if pr.returncode != 0:
+                raise RuntimeError("reference run failed")
+            secs += [float(l.split()[1]) for l in out.splitlines() if l.startswith("seconds")]
+        return nproc * pixels_per_proc * nprim, max(secs), "reference"
+    import multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    args = [(p, pixels_per_proc, nprim, seed) for p in range(nproc)]
+    t0 = time.perf_counter()
+    with ctx.Pool(nproc) as pool:
+        pool.map(_oracle_worker, args)
+    return nproc * pixels_per_proc * nprim, time.perf_counter() - t0, "port"
+
+
+def _oracle_worker(a):
+    p, npx, nprim, seed = a
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+    from cudamonsel_b200 import scenes
+    sc = scenes.lines()
+    centers = scenes.linescan_pixels(NPIX, 1e-9, 0.0, -120e-9)[(p * 37) % NPIX:][:npx]
+    pyoracle.run_scene(sc, centers, 1e-9, scenes.eV(BEAM_EV), nprim, seed + p, NBINS)
+    return 0
+
+
+def reference_arm(a, rank):
+    if rank != 0:
+        return 0
+    nproc = os.cpu_count() or 1
+    for _ in range(a.warmup):
+        cpu_sample(nproc, 1, 100, 7)
+    prim = 0
+    secs = 0.0
+    kind = None
+    for k in range(a.steps):
+        n, s, kind = cpu_sample(nproc, 2, 250, 100 + k * nproc)
+        prim += n
+        secs += s
+    v = prim / secs
+    sample = "%d processes x 2 pixels x 250 primaries per step" % nproc
+    line = {"metric": METRIC, "value": v, "unit": "primaries/s", "n_gpus": a.gpus, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": 1000 * secs / a.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "sample": sample}, "impl": "reference",
+            "cpu_baseline": {"value": v, "unit": "primaries/s", "cores": nproc, "kind": kind, "sample": sample},
+            "e2e": {"value": v, "unit": "primaries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ------------------------------------------------------------------ GPU arm
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    a = ap.parse_args()
+    a.warmup = max(a.warmup, 3) if a.impl == "ours" else a.warmup
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if a.impl == "reference":
+        return reference_arm(a, rank)
+
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+    from cudamonsel_b200 import capi, scenes
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", local))
+    eng = capi.Engine(local)
+    sc = scenes.lines()
+    h = scenes.build_engine(sc, eng)
+    centers, keys = linescan_inputs(rank)
+    dev = torch.device("cuda", local)
+    t_center = torch.tensor(centers.ravel(), dtype=torch.float64, device=dev)
+    t_energy = torch.full((NPIX,), scenes.eV(BEAM_EV), dtype=torch.float64, device=dev)
+    t_nprim = torch.full((NPIX,), NPRIM, dtype=torch.int32, device=dev)
+    t_nbins = torch.full((NPIX,), NBINS, dtype=torch.int32, device=dev)
+    t_keys = torch.tensor(keys.astype(np.int64), dtype=torch.int64, device=dev)
+    stride = NBINS + 2
+    t_back = torch.zeros((NPIX, stride), dtype=torch.int32, device=dev)
+    t_fwd = torch.zeros((NPIX, stride), dtype=torch.int32, device=dev)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MB > 126 MB L2
+    stream = torch.cuda.current_stream(dev)
+    import ctypes as C
+
+    def desc(prec, profile=0):
+        P = lambda t, ty: C.cast(C.c_void_p(t.data_ptr()), C.POINTER(ty))
+        return capi.RunDesc(h["chamber"], prec, NPIX, 1e-9, P(t_center, C.c_double), P(t_energy, C.c_double),
+                            P(t_nprim, C.c_int), P(t_nbins, C.c_int), 0, stride, 0, 0, P(t_keys, C.c_uint64), profile)
+
+    def step(prec, profile=0):
+        return eng.run_device(desc(prec, profile), t_back.data_ptr(), t_fwd.data_ptr(), stream.cuda_stream)
+
+    prec = capi.PREC_FP32
+    for _ in range(a.warmup):
+        step(prec)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clocks = Clocks(local)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(a.steps)]
+    stats = []
+    torch.cuda.synchronize()
+    for k in range(a.steps):
+        flush.zero_()
+        ev[k][0].record(stream)
+        stats.append(step(prec))
+        ev[k][1].record(stream)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clk = clocks.stop()
+    ms = sum(e0.elapsed_time(e1) for e0, e1 in ev)
+    t = torch.tensor([ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms = float(t.item())
+    back32 = t_back.cpu().numpy().astype(np.int64)
+    prim_per_rank = NPIX * NPRIM
+    value = world * prim_per_rank * a.steps / (ms / 1000.0)
+
+    # FP64 plain form on the same workload: throughput and the yield error of FP32 against it
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    flush.zero_()
+    e0.record(stream)
+    st64 = step(capi.PREC_FP64)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms64 = e0.elapsed_time(e1)
+    back64 = t_back.cpu().numpy().astype(np.int64)
+    b32, s32 = scenes.yields(back32.sum(0), prim_per_rank, BEAM_EV, NBINS)
+    b64, s64 = scenes.yields(back64.sum(0), prim_per_rank, BEAM_EV, NBINS)
+    yerr = {"bse_fp32": float(b32[0]), "bse_fp64": float(b64[0]), "se_fp32": float(s32[0]), "se_fp64": float(s64[0]),
+            "bse_rel_err": float(abs(b32[0] - b64[0]) / b64[0]), "se_rel_err": float(abs(s32[0] - s64[0]) / s64[0])}
+
+    # end to end through the C ABI with host buffers: H2D of the pixel arrays, D2H of the tallies
+    e2e_ms = 0.0
+    for k in range(a.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        eng.run(h["chamber"], centers, scenes.eV(BEAM_EV), NPRIM, NBINS, 1e-9, 0, precision=prec, pixel_keys=keys)
+        e2e_ms += 1000 * (time.perf_counter() - t0)
+    te = torch.tensor([e2e_ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+    e2e_value = world * prim_per_rank * a.steps / (float(te.item()) / 1000.0)
+    h2d = NPIX * (3 * 8 + 8 + 4 + 4 + 8)
+    d2h = 2 * NPIX * stride * 4
+
+    steps_total = sum(s.steps for s in stats)
+    launches = sum(6 * int(s.kernel_launches[0]) for s in stats)
+    # roofline of the dominant kernel: one more step of the same workload with CUDA events
+    # between the kernels of every iteration (event nodes inside the captured graph)
+    flush.zero_()
+    prof = [step(prec, profile=1)]
+    torch.cuda.synchronize()
+    kms = np.zeros(6)
+    units = np.zeros(4)
+    for s in prof:
+        kms += np.array(list(s.kernel_ms))
+        units += np.array(list(s.units))
+    names = capi.RunStats.KERNELS
+    dom = int(np.argmax(kms[:4]))
+    nlaunch = sum(int(s.iterations) for s in prof)
+    per_launch_units = units[dom] / max(1, nlaunch)
+    avg_ms = kms[dom] / max(1, sum(int(s.kernel_launches[dom]) for s in prof))
+    achieved = units[dom] * BYTES_PER_STEP / (kms[dom] / 1000.0) / 1e9
+    peak, peak_kind = peaks()
+    traffic = None
+    tf = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tf):
+        traffic = json.load(open(tf)).get(names[dom])
+
+    cpu = None
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        nproc = os.cpu_count() or 1
+        n, secs, kind = cpu_sample(nproc, 4, 500, 1)
+        cpu = {"value": n / secs, "unit": "primaries/s", "cores": nproc, "kind": kind,
+               "sample": "%d processes x 4 linescan pixels x 500 primaries" % nproc}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": "primaries/s", "n_gpus": world, "steps": a.steps,
+                "warmup": a.warmup, "ms_per_step": ms / a.steps, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": {"workload": WORKLOAD, "pixels": NPIX, "primaries_per_pixel": NPRIM, "beam_eV": BEAM_EV,
+                           "precision": "f32 transport, f64 positions and plane solves",
+                           "l2": "flushed between steps (256 MB write)", "parallelism": "replicas x%d" % world},
+                "electron_steps_per_s": world * steps_total / (ms / 1000.0),
+                "fp64": {"value": prim_per_rank / (ms64 / 1000.0), "unit": "primaries/s", "steps": int(st64.steps)},
+                "yield_error_vs_fp64": yerr,
+                "roofline": {"bound": "hbm", "kernel": names[dom], "achieved": achieved, "peak": peak,
+                             "unit": "GB/s", "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
+                             "bytes_per_unit": BYTES_PER_STEP, "units_per_launch": per_launch_units,
+                             "avg_launch_ms": avg_ms},
+                "kernel_ms_share": {n: float(v / kms.sum()) for n, v in zip(names, kms)},
+                "clocks": clk, "gpu_launches": launches,
+                "e2e": {"value": e2e_value, "unit": "primaries/s", "h2d_bytes_per_step": h2d,
+                        "d2h_bytes_per_step": d2h},
+                "cpu_baseline": cpu}
+        print(json.dumps(line), flush=True)
+    eng.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -32,33 +32,40 @@ class RunDesc(C.Structure):
     _fields_ = [("chamber", C.c_int), ("precision", C.c_int), ("npix", C.c_int), ("beam_width", C.c_double),
                 ("pixel_center", C.POINTER(C.c_double)), ("pixel_energy", C.POINTER(C.c_double)),
                 ("pixel_nprim", C.POINTER(C.c_int)), ("pixel_nbins", C.POINTER(C.c_int)), ("seed", C.c_uint64),
-                ("hist_stride", C.c_int), ("wave", C.c_int), ("max_iterations", C.c_int)]
+                ("hist_stride", C.c_int), ("wave", C.c_int), ("max_iterations", C.c_int),
+                ("pixel_key", C.POINTER(C.c_uint64)), ("profile", C.c_int)]
 
 
 class RunStats(C.Structure):
     _fields_ = [("primaries", C.c_int64), ("steps", C.c_int64), ("scatter_events", C.c_int64),
                 ("barrier_events", C.c_int64), ("escapes", C.c_int64), ("secondaries", C.c_int64),
-                ("iterations", C.c_int64), ("device_ms", C.c_double)]
+                ("iterations", C.c_int64), ("device_ms", C.c_double), ("kernel_ms", C.c_double * 6),
+                ("kernel_launches", C.c_int64 * 6), ("units", C.c_int64 * 4)]
+
+    KERNELS = ("flight", "elastic", "inelastic", "misc", "spawn", "tail")
 
     def as_dict(self):
-        return {k: getattr(self, k) for k, _ in self._fields_}
+        d = {k: getattr(self, k) for k, _ in self._fields_[:8]}
+        d["kernel_ms"] = dict(zip(self.KERNELS, list(self.kernel_ms)))
+        d["kernel_launches"] = dict(zip(self.KERNELS, list(self.kernel_launches)))
+        d["units"] = dict(zip(self.KERNELS[:4], list(self.units)))
+        return d
 
 
 class CMError(RuntimeError):
     pass
 
 
-_lib = None
+_libs = {}
 
 
-def load():
+def load(path=LIBPATH):
     """Load the in-tree library (raises if it was not built)."""
-    global _lib
-    if _lib is not None:
-        return _lib
-    if not os.path.exists(LIBPATH):
+    if path in _libs:
+        return _libs[path]
+    if not os.path.exists(path):
         raise CMError("libcudamonsel_b200.so not built; run `python -m cudamonsel_b200.build`")
-    L = C.CDLL(LIBPATH)
+    L = C.CDLL(path)
     d = C.POINTER(C.c_double)
     i = C.POINTER(C.c_int)
     ctx = C.c_void_p
@@ -103,7 +110,7 @@ def load():
     L.cm_last_error.restype = C.c_char_p
     L.cm_last_error.argtypes = []
     L.cm_version.restype = C.c_int
-    _lib = L
+    _libs[path] = L
     return L
 
 
@@ -220,7 +227,7 @@ class Engine:
 
     # ---- runs
     def run(self, chamber, centers, energies, nprim, nbins, beam_width, seed, precision=PREC_FP64, wave=0,
-            max_iterations=0):
+            max_iterations=0, pixel_keys=None, profile=0):
         centers = np.ascontiguousarray(centers, dtype=np.float64).reshape(-1, 3)
         npix = len(centers)
         e, pe = _d(np.broadcast_to(np.asarray(energies, dtype=np.float64), (npix,)).copy())
@@ -228,7 +235,11 @@ class Engine:
         n, pn = _i(np.broadcast_to(np.asarray(nprim), (npix,)).copy())
         b, pb = _i(np.broadcast_to(np.asarray(nbins), (npix,)).copy())
         stride = int(b.max()) + 2
-        desc = RunDesc(chamber, precision, npix, beam_width, pc, pe, pn, pb, seed, stride, wave, max_iterations)
+        keys = None
+        if pixel_keys is not None:
+            keys = np.ascontiguousarray(pixel_keys, dtype=np.uint64)
+        desc = RunDesc(chamber, precision, npix, beam_width, pc, pe, pn, pb, seed, stride, wave, max_iterations,
+                       keys.ctypes.data_as(C.POINTER(C.c_uint64)) if keys is not None else None, profile)
         back = np.zeros((npix, stride), dtype=np.uint32)
         fwd = np.zeros((npix, stride), dtype=np.uint32)
         st = RunStats()

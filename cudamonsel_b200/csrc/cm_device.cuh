@@ -13,7 +13,17 @@
 namespace cm {
 
 #define CM_HD __host__ __device__ __forceinline__
-#define CM_D __device__ __forceinline__
+// every per-event function is host-callable as well, so the same code can be
+// exercised on the CPU by test harnesses
+#define CM_D __host__ __device__ __forceinline__
+
+CM_D uint32_t umulhi32(uint32_t a, uint32_t b) {
+#ifdef __CUDA_ARCH__
+  return __umulhi(a, b);
+#else
+  return (uint32_t)(((uint64_t)a * b) >> 32);
+#endif
+}
 
 // ------------------------------------------------------------ counter-based RNG
 // Philox-4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11), keyed per electron.
@@ -23,8 +33,8 @@ CM_D U4 philox(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3, uint32_t k0, 
   const uint32_t M0 = 0xD2511F53u, M1 = 0xCD9E8D57u, W0 = 0x9E3779B9u, W1 = 0xBB67AE85u;
 #pragma unroll
   for (int r = 0; r < 10; ++r) {
-    uint32_t hi0 = __umulhi(M0, c0), lo0 = M0 * c0;
-    uint32_t hi1 = __umulhi(M1, c2), lo1 = M1 * c2;
+    uint32_t hi0 = umulhi32(M0, c0), lo0 = M0 * c0;
+    uint32_t hi1 = umulhi32(M1, c2), lo1 = M1 * c2;
     uint32_t n0 = hi1 ^ c1 ^ k0, n2 = hi0 ^ c3 ^ k1;
     c0 = n0; c1 = lo1; c2 = n2; c3 = lo0;
     k0 += W0; k1 += W1;
@@ -109,31 +119,65 @@ template <typename R> CM_D R msinh(R x);
 template <> CM_D double msinh(double x) { return sinh(x); }
 template <> CM_D float msinh(float x) { return sinhf(x); }
 
-template <typename R> CM_D R pick4(const R* a, int k) { return k <= 0 ? a[0] : k == 1 ? a[1] : k == 2 ? a[2] : a[3]; }
+// acos(1 - 2 q^2) with the reference's clamps (NISTMottRS.cu:148-149):
+// com > -1 ? (com < 1 ? acos(com) : 0) : pi.  In float the equivalent
+// 2 asin(|q|) keeps full relative precision for small angles.
+template <typename R> CM_D R angle_from_q(R q);
+template <> CM_D double angle_from_q(double q) {
+  const double com = 1.0 - (2.0 * q * q);
+  return com > -1.0 ? (com < 1.0 ? acos(com) : 0.0) : kPi;
+}
+template <> CM_D float angle_from_q(float q) {
+  const float a = fabsf(q);
+  if (a >= 1.0f) return (float)kPi;
+  return 2.0f * asinf(a);
+}
+
+// acos(1 - t) for t >= 0; float uses 2 asin(sqrt(t / 2)), which keeps its
+// relative precision for the small angles of screened Rutherford scattering
+template <typename R> CM_D R acos_1m(R t);
+template <> CM_D double acos_1m(double t) { return acos(1.0 - t); }
+template <> CM_D float acos_1m(float t) { return 2.0f * asinf(sqrtf(fminf(fmaxf(0.5f * t, 0.0f), 1.0f))); }
+
+// acos(1 - 2 r) for r in (0, 1) (isotropic polar angle); float uses 2 asin(sqrt(r))
+template <typename R> CM_D R iso_angle(R r);
+template <> CM_D double iso_angle(double r) { return acos(1 - 2.0 * r); }
+template <> CM_D float iso_angle(float r) { return 2.0f * asinf(sqrtf(r)); }
+
+// select by value (no address of a local array is taken: keeps the values in registers)
+template <typename R> CM_D R sel4(R a0, R a1, R a2, R a3, int k) { return k <= 0 ? a0 : k == 1 ? a1 : k == 2 ? a2 : a3; }
 
 // ------------------------------------------------------------ uniform-grid Lagrange
-// JMONSELutils/ULagrangeInterpolation.cu:5-33, order 3; f points at 4 values.
+// JMONSELutils/ULagrangeInterpolation.cu:5-33, order 3, written out with
+// scalars: Neville's tableau on f0..f3 at reduced x, starting from the nearest
+// node and walking the correction path the reference walks.
 template <typename R> CM_D R uneville3(R f0, R f1, R f2, R f3, R x) {
   int ns = (int)mround(x);
   if (ns < 0) ns = 0;
   else if (ns > 3) ns = 3;
-  R c[4] = {f0, f1, f2, f3}, d[4] = {f0, f1, f2, f3};
-  R y = pick4(c, ns--);
-  R dy = 0;
-#pragma unroll
-  for (int m = 1; m <= 3; m++) {
-#pragma unroll
-    for (int i = 0; i <= 3 - m; i++) {
-      R ho = (R)i - x;
-      R hp = (R)(i + m) - x;
-      R w = c[i + 1] - d[i];
-      d[i] = -hp * w / (R)m;
-      c[i] = -ho * w / (R)m;
-    }
-    if (2 * ns < (3 - 1 - m)) dy = pick4(c, ns + 1);
-    else dy = pick4(d, ns--);
-    y += dy;
-  }
+  R c0 = f0, c1 = f1, c2 = f2, c3 = f3;
+  R d0 = f0, d1 = f1, d2 = f2;
+  R y = sel4(c0, c1, c2, c3, ns);
+  --ns;
+  R dy, w;
+  // m = 1
+  w = c1 - d0; d0 = -((R)1 - x) * w / (R)1; c0 = -((R)0 - x) * w / (R)1;
+  w = c2 - d1; d1 = -((R)2 - x) * w / (R)1; c1 = -((R)1 - x) * w / (R)1;
+  w = c3 - d2; d2 = -((R)3 - x) * w / (R)1; c2 = -((R)2 - x) * w / (R)1;
+  if (2 * ns < 1) dy = sel4(c0, c1, c2, c3, ns + 1);
+  else { dy = sel4(d0, d1, d2, d2, ns); --ns; }
+  y += dy;
+  // m = 2
+  w = c1 - d0; d0 = -((R)2 - x) * w / (R)2; c0 = -((R)0 - x) * w / (R)2;
+  w = c2 - d1; d1 = -((R)3 - x) * w / (R)2; c1 = -((R)1 - x) * w / (R)2;
+  if (2 * ns < 0) dy = sel4(c0, c1, c2, c2, ns + 1);
+  else { dy = sel4(d0, d1, d1, d1, ns); --ns; }
+  y += dy;
+  // m = 3
+  w = c1 - d0; d0 = -((R)3 - x) * w / (R)3; c0 = -((R)0 - x) * w / (R)3;
+  if (2 * ns < -1) dy = c0;
+  else dy = d0;
+  y += dy;
   return y;
 }
 
@@ -186,26 +230,33 @@ template <typename R> CM_D void nu_locate(R x, const R* xs, int n, int order, in
   else first = firstInd;
 }
 
-// NULagrangeInterpolation.cu:85-112 with order 3 (4 values, their abscissae)
+// NULagrangeInterpolation.cu:85-112 with order 3: Neville on (xv[i], fv[i]),
+// i = 0..3, from the nearest node ns, written out with scalars
 template <typename R> CM_D R nu_neville3(const R* fv, const R* xv, int ns, R x) {
-  R c[4] = {fv[0], fv[1], fv[2], fv[3]}, d[4] = {fv[0], fv[1], fv[2], fv[3]};
-  R y = pick4(c, ns--);
-  R dy = 0;
-#pragma unroll
-  for (int m = 1; m <= 3; m++) {
-#pragma unroll
-    for (int i = 0; i <= 3 - m; i++) {
-      R ho = xv[i] - x;
-      R hp = xv[i + m] - x;
-      R w = c[i + 1] - d[i];
-      R den = w / (ho - hp);
-      d[i] = hp * den;
-      c[i] = ho * den;
-    }
-    if ((2 * ns) < (3 - 1 - m)) dy = pick4(c, ns + 1);
-    else dy = pick4(d, ns--);
-    y += dy;
-  }
+  const R x0 = xv[0], x1 = xv[1], x2 = xv[2], x3 = xv[3];
+  R c0 = fv[0], c1 = fv[1], c2 = fv[2], c3 = fv[3];
+  R d0 = c0, d1 = c1, d2 = c2;
+  R y = sel4(c0, c1, c2, c3, ns);
+  --ns;
+  R dy, w, ho, hp, den;
+  // m = 1
+  ho = x0 - x; hp = x1 - x; w = c1 - d0; den = w / (ho - hp); d0 = hp * den; c0 = ho * den;
+  ho = x1 - x; hp = x2 - x; w = c2 - d1; den = w / (ho - hp); d1 = hp * den; c1 = ho * den;
+  ho = x2 - x; hp = x3 - x; w = c3 - d2; den = w / (ho - hp); d2 = hp * den; c2 = ho * den;
+  if ((2 * ns) < 1) dy = sel4(c0, c1, c2, c3, ns + 1);
+  else { dy = sel4(d0, d1, d2, d2, ns); --ns; }
+  y += dy;
+  // m = 2
+  ho = x0 - x; hp = x2 - x; w = c1 - d0; den = w / (ho - hp); d0 = hp * den; c0 = ho * den;
+  ho = x1 - x; hp = x3 - x; w = c2 - d1; den = w / (ho - hp); d1 = hp * den; c1 = ho * den;
+  if ((2 * ns) < 0) dy = sel4(c0, c1, c2, c2, ns + 1);
+  else { dy = sel4(d0, d1, d1, d1, ns); --ns; }
+  y += dy;
+  // m = 3
+  ho = x0 - x; hp = x3 - x; w = c1 - d0; den = w / (ho - hp); d0 = hp * den; c0 = ho * den;
+  if ((2 * ns) < -1) dy = c0;
+  else dy = d0;
+  y += dy;
   return y;
 }
 
@@ -313,15 +364,15 @@ template <typename R> CM_D R browning_sigma(const Mott& m, R E) {
 // `fixes` uses the element's atomic number.
 template <typename R, typename G> CM_D R browning_angle(const Mott& m, R E, G& g, bool fixes) {
   const R r1 = g.next(), r2 = g.next();
-  if (!fixes) return macos(1 - R(2.0) * r2);
+  if (!fixes) return iso_angle(r2);
   const R z = (R)m.Z;
   const R e = E / R(1000);
   const R r = (R(300.0) * e / z) + ((R)m.zp3 / (R(3.0e5) * e));
   if (r1 <= r / (r + 1)) {
     const R alpha = R(7.0e-3) / e;
-    return macos(R(1.0) - ((R(2.0) * alpha * r2) / (alpha - r2 + 1)));
+    return acos_1m((R(2.0) * alpha * r2) / (alpha - r2 + 1));
   }
-  return macos(1 - R(2.0) * r2);
+  return iso_angle(r2);
 }
 
 // JMONSEL/NISTMottRS.cu:103-119 times the SelectableElasticSM rate factor (1/nm)
@@ -341,13 +392,12 @@ template <typename R, typename G> CM_D R nistmott_angle(const SceneView<R>& s, c
     const R lg = mlog(E);
     const R u = g.next();
     const R q = ulagrange_d2(s.blob + m.off_x1, 61, 201, (R)s.dl50, R(0), (R)s.param, R(0.005), lg, u);
-    const R com = R(1.0) - (R(2.0) * q * q);
-    return com > R(-1.0) ? (com < R(1.0) ? macos(com) : R(0)) : R(kPi);
+    return angle_from_q(q);
   }
   // ScreenedRutherfordScatteringAngle.cu:32-39
   const R alpha = (R)m.rutherfordAlpha / E;
   const R r = g.next();
-  return macos(1 - R(2.0) * alpha * r / (1 + alpha - r));
+  return acos_1m(R(2.0) * alpha * r / (1 + alpha - r));
 }
 
 // ------------------------------------------------------------ direction algebra
@@ -378,31 +428,42 @@ template <typename R> CM_D void dir_from_angles(R d[3], R theta, R phi) {
   d[0] = st * cp; d[1] = st * sp; d[2] = ct;
 }
 
+// kE / (1 + x)^(2/3) - kE, the Nieminen loss of JoyLuoNieminenCSD.cu:104.  In
+// float the difference of two nearly equal numbers loses everything for
+// short steps; kE * expm1(-2/3 log1p(x)) is the same quantity without the
+// cancellation.
+template <typename R> CM_D R nieminen_loss(R kE, R x);
+template <> CM_D double nieminen_loss(double kE, double x) { return (kE / pow(1. + x, 2. / 3.)) - kE; }
+template <> CM_D float nieminen_loss(float kE, float x) { return kE * expm1f(-(2.0f / 3.0f) * log1pf(x)); }
+
 // ------------------------------------------------------------ slowing down
 // JMONSEL/JoyLuoNieminenCSD.cu:91-121; the recursive halving is run with an
 // explicit stack in the same order (first half, then second half at the
 // energy reached after the first).
 template <typename R> CM_D R jln_compute(const Jln& c, R len, R kE) {
   if ((c.nce == 0) || (kE < (R)c.minE) || (kE <= R(0))) return 0;
-  if (kE <= (R)c.breakE) return (kE / mpow(R(1) + (R(1.5) * (R)c.gamma * len * kE * msqrt(kE)), R(2) / R(3))) - kE;
-  R stack[48];
+  if (kE <= (R)c.breakE) return nieminen_loss(kE, R(1.5) * (R)c.gamma * len * kE * msqrt(kE));
+  // pending segments are len / 2^depth; keep only their depths
+  unsigned char stack[48];
   int sp = 0;
-  stack[sp++] = len;
+  stack[sp++] = 0;
   R total = 0;
   while (sp > 0) {
-    const R l = stack[--sp];
+    const int depth = stack[--sp];
+    R l = len;
+    for (int k = 0; k < depth; ++k) l = l / 2;
     const R e = kE + total;
     if ((e < (R)c.minE) || (e <= R(0))) continue;
     if (e <= (R)c.breakE) {
-      total += (e / mpow(R(1) + (R(1.5) * (R)c.gamma * l * e * msqrt(e)), R(2) / R(3))) - e;
+      total += nieminen_loss(e, R(1.5) * (R)c.gamma * l * e * msqrt(e));
       continue;
     }
     R loss = 0;
     for (int i = 0; i < c.nce; i++) loss += (R)c.coef[i] * mlog(((R)c.recipJ[i] * e) + (R)c.beta[i]);
     loss *= l / e;
-    if (loss <= (R(0.1) * e) || sp >= 46) { total += -loss; continue; }
-    stack[sp++] = l / 2;   // second half, processed after the first
-    stack[sp++] = l / 2;   // first half
+    if (loss <= (R(0.1) * e) || sp >= 46 || depth >= 120) { total += -loss; continue; }
+    stack[sp++] = (unsigned char)(depth + 1);  // second half, processed after the first
+    stack[sp++] = (unsigned char)(depth + 1);  // first half
   }
   return total;
 }
@@ -576,7 +637,7 @@ template <typename R> CM_D bool shape_contains2(const SceneView<R>& s, int id, c
 template <typename R, int D> struct FirstNormal;
 
 // NormalIntersectionShape.cu:19-239
-template <typename R, int D> __device__ __noinline__ NV inter_first_normal(const SceneView<R>& s, const Shape& sh, const double* pos0,
+template <typename R, int D> __host__ __device__ __noinline__ NV inter_first_normal(const SceneView<R>& s, const Shape& sh, const double* pos0,
                                                                            const double* pos1) {
   const NV none = nv_none();
   int adepth, bdepth;

@@ -30,7 +30,7 @@
 #include <vector>
 
 #include "../../include/cudamonsel_b200.h"
-#include "cm_physics.cuh"
+#include "cm_wave.cuh"
 
 namespace cg = cooperative_groups;
 
@@ -118,33 +118,12 @@ struct DevScene {
   std::vector<void*> allocs;
   SceneView<R> view;
   bool valid = false;
+  bool host = false;  // tables in host memory (only for host-side checks of the device code)
   void release() {
-    for (void* p : allocs) cudaFree(p);
+    for (void* p : allocs) host ? free(p) : (void)cudaFree(p);
     allocs.clear();
     valid = false;
   }
-};
-
-template <typename R>
-struct Wave {
-  double *px, *py, *pz;
-  R *dx, *dy, *dz;
-  R *E, *Ep;
-  int *region, *pixel, *aux;
-  uint32_t* step;
-  unsigned long long* key;
-  R *hx, *hy, *hz;
-};
-
-struct Counters {
-  int n[2];
-  int pool;
-  int q[3];
-  int error;
-  int done;
-  unsigned long long next_primary, total_primaries;
-  unsigned long long steps, scatters, barriers, escapes, secondaries;
-  unsigned long long iterations;
 };
 
 template <typename R>
@@ -191,9 +170,16 @@ struct cm_context {
 namespace cm {
 
 template <typename T>
-static int dev_copy(std::vector<void*>& allocs, const std::vector<T>& v, const T** out) {
+static int dev_copy(std::vector<void*>& allocs, const std::vector<T>& v, const T** out, bool host = false) {
   void* p = nullptr;
   size_t bytes = std::max<size_t>(1, v.size()) * sizeof(T);
+  if (host) {
+    p = malloc(bytes);
+    allocs.push_back(p);
+    if (!v.empty()) memcpy(p, v.data(), v.size() * sizeof(T));
+    *out = (const T*)p;
+    return 0;
+  }
   CM_CUDA(cudaMalloc(&p, bytes));
   allocs.push_back(p);
   if (!v.empty()) CM_CUDA(cudaMemcpy(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
@@ -434,11 +420,12 @@ static int build_scene(cm_context* ctx, DevScene<R>& ds) {
   }
   SceneView<R>& v = ds.view;
   int rc = 0;
-  if ((rc = dev_copy(ds.allocs, shapes, &v.shapes)) || (rc = dev_copy(ds.allocs, planes, &v.planes)) ||
-      (rc = dev_copy(ds.allocs, regions, &v.regions)) || (rc = dev_copy(ds.allocs, children, &v.children)) ||
-      (rc = dev_copy(ds.allocs, msms, &v.msms)) || (rc = dev_copy(ds.allocs, mechs, &v.mechs)) ||
-      (rc = dev_copy(ds.allocs, motts, &v.mott)) || (rc = dev_copy(ds.allocs, tabs, &v.tables)) ||
-      (rc = dev_copy(ds.allocs, blob, &v.blob)))
+  const bool h = ds.host;
+  if ((rc = dev_copy(ds.allocs, shapes, &v.shapes, h)) || (rc = dev_copy(ds.allocs, planes, &v.planes, h)) ||
+      (rc = dev_copy(ds.allocs, regions, &v.regions, h)) || (rc = dev_copy(ds.allocs, children, &v.children, h)) ||
+      (rc = dev_copy(ds.allocs, msms, &v.msms, h)) || (rc = dev_copy(ds.allocs, mechs, &v.mechs, h)) ||
+      (rc = dev_copy(ds.allocs, motts, &v.mott, h)) || (rc = dev_copy(ds.allocs, tabs, &v.tables, h)) ||
+      (rc = dev_copy(ds.allocs, blob, &v.blob, h)))
     return rc;
   v.chamber = 0;
   v.options = ctx->options;
@@ -456,364 +443,102 @@ template <typename R> static RunBuffers<R>& buffers_of(cm_context* c);
 template <> RunBuffers<double>& buffers_of<double>(cm_context* c) { return c->rb64; }
 template <> RunBuffers<float>& buffers_of<float>(cm_context* c) { return c->rb32; }
 
-// ------------------------------------------------------------------ wave state access
-template <typename R>
-struct El {
-  double p[3];
-  R d[3];
-  R E, Ep;
-  int region, pixel, aux;
-  uint32_t step;
-  unsigned long long key;
-  R h[3];
-};
-
-template <typename R> CM_D El<R> load(const Wave<R>& w, int i) {
-  El<R> e;
-  e.p[0] = w.px[i]; e.p[1] = w.py[i]; e.p[2] = w.pz[i];
-  e.d[0] = w.dx[i]; e.d[1] = w.dy[i]; e.d[2] = w.dz[i];
-  e.E = w.E[i]; e.Ep = w.Ep[i];
-  e.region = w.region[i]; e.pixel = w.pixel[i]; e.aux = w.aux[i];
-  e.step = w.step[i]; e.key = w.key[i];
-  e.h[0] = w.hx[i]; e.h[1] = w.hy[i]; e.h[2] = w.hz[i];
-  return e;
-}
-
-template <typename R> CM_D void store(const Wave<R>& w, int i, const El<R>& e) {
-  w.px[i] = e.p[0]; w.py[i] = e.p[1]; w.pz[i] = e.p[2];
-  w.dx[i] = e.d[0]; w.dy[i] = e.d[1]; w.dz[i] = e.d[2];
-  w.E[i] = e.E; w.Ep[i] = e.Ep;
-  w.region[i] = e.region; w.pixel[i] = e.pixel; w.aux[i] = e.aux;
-  w.step[i] = e.step; w.key[i] = e.key;
-  w.hx[i] = e.h[0]; w.hy[i] = e.h[1]; w.hz[i] = e.h[2];
-}
-
+// ------------------------------------------------------------------ kernels
 // warp-aggregated append: one atomic per group of converged lanes
-CM_D int append_slot(int* counter) {
-  cg::coalesced_group g = cg::coalesced_threads();
-  int base = 0;
-  if (g.thread_rank() == 0) base = atomicAdd(counter, (int)g.size());
-  base = g.shfl(base, 0);
-  return base + (int)g.thread_rank();
-}
-
-enum { Q_EL = 0, Q_TAB = 1, Q_MISC = 2 };
-enum { AUX_MECH = 1, AUX_BARRIER = 2, AUX_PASS = 3 };
-CM_HD int aux_pack(int kind, int v) { return (kind << 24) | (v & 0xffffff); }
-CM_HD int aux_kind(int a) { return a >> 24; }
-CM_HD int aux_val(int a) { return a & 0xffffff; }
-
-template <typename R>
-struct RunView {
-  SceneView<R> s;
-  Wave<R> w[2];
-  Wave<R> pool;
-  int* q[3];
-  Counters* c;
-  int W, poolCap;
-  const double* pc;      // pixel centres, nm
-  const double* pe0;     // beam energy, eV
-  const double* pe0ref;  // histogram top edge: FromSI::eV(ToSI::eV(E0)) as the reference computes it
-  const int* pnbins;
-  const unsigned long long* prefix;
-  int npix;
-  double width;          // nm
-  unsigned long long seedmix;
-  uint32_t *back, *fwd;
-  int stride;
+struct DeviceSink {
+  __device__ __forceinline__ int append(int* counter) {
+    cg::coalesced_group g = cg::coalesced_threads();
+    int base = 0;
+    if (g.thread_rank() == 0) base = atomicAdd(counter, (int)g.size());
+    base = g.shfl(base, 0);
+    return base + (int)g.thread_rank();
+  }
+  // lanes may target different counters (one per event queue): group them by
+  // queue first, then one atomic per group
+  __device__ __forceinline__ int append_q(int* counters, int q) {
+    cg::coalesced_group g = cg::coalesced_threads();
+    cg::coalesced_group part = cg::labeled_partition(g, q);
+    int base = 0;
+    if (part.thread_rank() == 0) base = atomicAdd(counters + q, (int)part.size());
+    base = part.shfl(base, 0);
+    return base + (int)part.thread_rank();
+  }
+  __device__ __forceinline__ void count(uint32_t* h) { atomicAdd(h, 1u); }
+  __device__ __forceinline__ void error(int* e, int code) { atomicExch(e, code); }
 };
 
-// Histogram::bin (Utility/Histogram.cu:73-80) over bins min + i*delta with
-// Algorithm::binarySearch (Amphibian/Algorithm.cu:5-14): exact match or the
-// insertion point.
-CM_D int hist_bin(double max, int nbins, double val) {
-  const double delta = max / nbins;
-  int l = 0, r = nbins;
-  while (l <= r) {
-    const int mid = l + (r - l) / 2;
-    const double bm = mid == 0 ? 0.0 : 0.0 + mid * delta;
-    if (bm == val) return mid;
-    if (bm < val) l = mid + 1;
-    else r = mid - 1;
+__device__ __forceinline__ void flush_counts(Counters* c, StepCounts& sc) {
+  for (int off = 16; off > 0; off >>= 1) {
+    sc.steps += __shfl_down_sync(0xffffffffu, sc.steps, off);
+    sc.scat += __shfl_down_sync(0xffffffffu, sc.scat, off);
+    sc.bar += __shfl_down_sync(0xffffffffu, sc.bar, off);
+    sc.esc += __shfl_down_sync(0xffffffffu, sc.esc, off);
+    sc.sec += __shfl_down_sync(0xffffffffu, sc.sec, off);
   }
-  return l;
-}
-
-// BackscatterStats::actionPerformed for a BackscatterEvent (NISTMonte/BackscatterStats.cu:147-170)
-template <typename R> CM_D void tally_escape(const RunView<R>& v, const El<R>& e) {
-  const int px = e.pixel;
-  const double E0ref = v.pe0ref[px];
-  double val = (double)e.E;
-  if (e.E == (R)v.pe0[px]) val = E0ref;  // electrons that never lost energy carry E0 exactly, as in the reference
-  const double elevation = (kPi / 2) - atan2(e.p[2], sqrt((e.p[0] * e.p[0]) + (e.p[1] * e.p[1])));
-  const int nb = v.pnbins[px];
-  const int b = hist_bin(E0ref, nb, val) + 1;
-  if (b > nb + 1) return;  // past the overflow slot: the reference writes out of bounds and never counts it
-  uint32_t* h = elevation < (kPi / 2.0) ? v.fwd : v.back;
-  atomicAdd(h + (size_t)px * v.stride + b, 1u);
+  if ((threadIdx.x & 31) == 0) {
+    if (sc.steps) atomicAdd(&c->steps, sc.steps);
+    if (sc.scat) atomicAdd(&c->scatters, sc.scat);
+    if (sc.bar) atomicAdd(&c->barriers, sc.bar);
+    if (sc.esc) atomicAdd(&c->escapes, sc.esc);
+    if (sc.sec) atomicAdd(&c->secondaries, sc.sec);
+  }
 }
 
 template <typename R>
 __global__ void __launch_bounds__(256) k_flight(RunView<R> v, int cur) {
-  const SceneView<R>& s = v.s;
+  DeviceSink sink;
+  StepCounts sc;
   const int n = v.c->n[cur];
-  const Wave<R> W = v.w[cur];
-  unsigned long long nsteps = 0, nscat = 0, nbar = 0, nesc = 0;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    El<R> e = load(W, i);
-    int reg = e.region;
-    // MonteCarloSS::takeStep (MonteCarloSS.cu:109-119)
-    if (reg < 0 || !shape_contains(s, s.regions[reg].shape, e.p)) reg = containing_subregion(s, s.chamber, e.p);
-    if (reg < 0) continue;
-    const Msm& m = s.msms[s.regions[reg].msm];
-    Rng<R> g(e.key, e.step, 0);
-    // MONSEL_MaterialScatterModel::randomMeanPathLength (:64-91)
-    R cum[kMaxMech];
-    R total = 0;
-    const R logE = mlog(e.E);
-    for (int k = 0; k < m.nmech; ++k) {
-      total += mech_rate(s, s.mechs[m.mech0 + k], e.E, logE);
-      cum[k] = total;
-    }
-    bool complete = false;
-    double fp = 2.0 * kChamberRadiusNm;
-    if (total != R(0)) {
-      const R f = -mlog(g.next()) / total;
-      if ((double)f < fp) fp = (double)f;
-    } else if (e.step > 1000000u) {
-      complete = true;
-    }
-    double p1[3] = {e.p[0] + fp * (double)e.d[0], e.p[1] + fp * (double)e.d[1], e.p[2] + fp * (double)e.d[2]};
-    double hn[3];
-    const int next = find_end_of_step(s, reg, e.p, p1, hn);
-    const double dd = sqrt((p1[0] - e.p[0]) * (p1[0] - e.p[0]) + (p1[1] - e.p[1]) * (p1[1] - e.p[1]) +
-                           (p1[2] - e.p[2]) * (p1[2] - e.p[2]));
-    const R dE = m.csd ? jln_compute(m.jln, (R)dd, e.E) : R(0);
-    e.p[0] = p1[0]; e.p[1] = p1[1]; e.p[2] = p1[2];
-    e.Ep = e.E;
-    e.E += dE;
-    e.step += 1;
-    e.region = reg;
-    ++nsteps;
-    if ((e.E < (R)m.minE) || complete) continue;
-    int queue;
-    if (next == reg) {
-      ++nscat;
-      if (total == R(0)) {
-        queue = Q_MISC;
-        e.aux = aux_pack(AUX_PASS, 0);
-      } else {
-        // MONSEL_MaterialScatterModel::scatter (:93-134): the cache holds the step's starting energy
-        const R r = g.next() * total;
-        int idx = 0;
-        while (idx < m.nmech - 1 && cum[idx] < r) ++idx;
-        const int kind = s.mechs[m.mech0 + idx].kind;
-        if (kind == MECH_POLARON) continue;  // GanachaudMokraniPolaronTrapSM::scatter: trapped, E = 0
-        queue = kind == MECH_NISTMOTT ? Q_EL : kind == MECH_TABULATED ? Q_TAB : Q_MISC;
-        e.aux = aux_pack(AUX_MECH, idx);
-      }
-    } else if (next >= 0) {
-      ++nbar;
-      queue = Q_MISC;
-      e.aux = aux_pack(AUX_BARRIER, next);
-      e.h[0] = (R)hn[0]; e.h[1] = (R)hn[1]; e.h[2] = (R)hn[2];
-    } else {
-      ++nesc;
-      tally_escape(v, e);
-      continue;
-    }
-    store(W, i, e);
-    const int slot = append_slot(&v.c->q[queue]);
-    v.q[queue][slot] = i;
-  }
-  // counters: one atomic per warp
-  for (int off = 16; off > 0; off >>= 1) {
-    nsteps += __shfl_down_sync(0xffffffffu, nsteps, off);
-    nscat += __shfl_down_sync(0xffffffffu, nscat, off);
-    nbar += __shfl_down_sync(0xffffffffu, nbar, off);
-    nesc += __shfl_down_sync(0xffffffffu, nesc, off);
-  }
-  if ((threadIdx.x & 31) == 0 && nsteps) {
-    atomicAdd(&v.c->steps, nsteps);
-    atomicAdd(&v.c->scatters, nscat);
-    atomicAdd(&v.c->barriers, nbar);
-    atomicAdd(&v.c->escapes, nesc);
-  }
-}
-
-// append a surviving electron to the next wave
-template <typename R> CM_D void keep(const RunView<R>& v, int nxt, const El<R>& e) {
-  const int slot = append_slot(&v.c->n[nxt]);
-  store(v.w[nxt], slot, e);
-}
-
-// push a secondary to the pool when MonteCarloSS::trackSecondaryElectron (:165-174) would track it
-template <typename R> CM_D void push_secondary(const RunView<R>& v, const El<R>& pe, const R sd[3], R sE, int* nsec) {
-  const Msm& m = v.s.msms[v.s.regions[pe.region].msm];
-  if (!(sE > (R)m.minE)) return;
-  El<R> se;
-  se.p[0] = pe.p[0]; se.p[1] = pe.p[1]; se.p[2] = pe.p[2];
-  se.d[0] = sd[0]; se.d[1] = sd[1]; se.d[2] = sd[2];
-  se.E = sE; se.Ep = sE;
-  se.region = pe.region;
-  se.pixel = pe.pixel;
-  se.aux = 0;
-  se.step = 0;
-  se.key = mix64(pe.key ^ (0x9E3779B97F4A7C15ULL * (unsigned long long)pe.step));
-  se.h[0] = se.h[1] = se.h[2] = 0;
-  const int slot = append_slot(&v.c->pool);
-  if (slot >= v.poolCap) {
-    atomicExch(&v.c->error, CM_EOVERFLOW);
-    return;
-  }
-  store(v.pool, slot, se);
-  ++*nsec;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) flight_one(v, cur, i, sink, sc);
+  flush_counts(v.c, sc);
 }
 
 template <typename R>
 __global__ void __launch_bounds__(256) k_elastic(RunView<R> v, int cur) {
-  const SceneView<R>& s = v.s;
+  DeviceSink sink;
   const int n = v.c->q[Q_EL];
-  const int nxt = cur ^ 1;
-  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
-    El<R> e = load(v.w[cur], v.q[Q_EL][j]);
-    const Msm& m = s.msms[s.regions[e.region].msm];
-    const Mech& k = s.mechs[m.mech0 + aux_val(e.aux)];
-    Rng<R> g(e.key, e.step - 1, 1);
-    elastic_scatter(s, k, e.d, e.Ep, g);
-    if (!(e.E < (R)m.minE)) keep(v, nxt, e);
-  }
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) elastic_one(v, cur, j, sink);
 }
 
 template <typename R>
 __global__ void __launch_bounds__(256) k_inelastic(RunView<R> v, int cur) {
-  const SceneView<R>& s = v.s;
+  DeviceSink sink;
+  StepCounts sc;
   const int n = v.c->q[Q_TAB];
-  const int nxt = cur ^ 1;
-  int nsec = 0;
-  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
-    El<R> e = load(v.w[cur], v.q[Q_TAB][j]);
-    const Msm& m = s.msms[s.regions[e.region].msm];
-    const Mech& k = s.mechs[m.mech0 + aux_val(e.aux)];
-    Rng<R> g(e.key, e.step - 1, 1);
-    R sd[3], sE;
-    const bool made = tabulated_scatter(s, k, e.d, e.E, sd, sE, g);
-    if (!(e.E < (R)m.minE)) keep(v, nxt, e);
-    if (made) push_secondary(v, e, sd, sE, &nsec);
-  }
-  for (int off = 16; off > 0; off >>= 1) nsec += __shfl_down_sync(0xffffffffu, nsec, off);
-  if ((threadIdx.x & 31) == 0 && nsec) atomicAdd(&v.c->secondaries, (unsigned long long)nsec);
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) inelastic_one(v, cur, j, sink, sc);
+  flush_counts(v.c, sc);
 }
 
 template <typename R>
 __global__ void __launch_bounds__(256) k_misc(RunView<R> v, int cur) {
-  const SceneView<R>& s = v.s;
+  DeviceSink sink;
+  StepCounts sc;
   const int n = v.c->q[Q_MISC];
-  const int nxt = cur ^ 1;
-  int nsec = 0;
-  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
-    El<R> e = load(v.w[cur], v.q[Q_MISC][j]);
-    const Msm& m = s.msms[s.regions[e.region].msm];
-    const int kind = aux_kind(e.aux);
-    Rng<R> g(e.key, e.step - 1, 1);
-    if (kind == AUX_BARRIER) {
-      // MonteCarloSS::takeStep (:143-156): barrierScatter, a nudge along the new direction, region update
-      const double hn[3] = {(double)e.h[0], (double)e.h[1], (double)e.h[2]};
-      e.region = barrier_scatter(s, m, e.p, e.d, e.E, e.region, aux_val(e.aux), hn, g);
-      e.p[0] += kSmallDispNm * (double)e.d[0];
-      e.p[1] += kSmallDispNm * (double)e.d[1];
-      e.p[2] += kSmallDispNm * (double)e.d[2];
-      if (!shape_contains(s, s.regions[e.region].shape, e.p)) e.region = containing_subregion(s, s.chamber, e.p);
-      keep(v, nxt, e);
-      continue;
-    }
-    if (kind == AUX_MECH) {
-      const Mech& k = s.mechs[m.mech0 + aux_val(e.aux)];
-      if (k.kind == MECH_FITTED) {  // FittedInelSM::scatter (FittedInelSM.cu:13-18)
-        const R phi = R(2) * R(kPi) * g.next();
-        const R theta = macos(R(1) - (R(2) * g.next()));
-        R sd[3];
-        dir_from_angles(sd, theta, phi);
-        push_secondary(v, e, sd, (R)(k.energySEgen + k.eFermi), &nsec);
-      } else if (k.kind == MECH_PHONON) {
-        phonon_scatter(k, e.d, e.E, e.Ep, g);
-      }
-    }
-    if (!(e.E < (R)m.minE)) keep(v, nxt, e);
-  }
-  for (int off = 16; off > 0; off >>= 1) nsec += __shfl_down_sync(0xffffffffu, nsec, off);
-  if ((threadIdx.x & 31) == 0 && nsec) atomicAdd(&v.c->secondaries, (unsigned long long)nsec);
-}
-
-// refill the next wave: secondaries from the pool first, then new primaries
-CM_D void refill_plan(const Counters* c, int nxt, int W, int& nn, int& take_se, int& take_p) {
-  nn = c->n[nxt];
-  const int room = W - nn > 0 ? W - nn : 0;
-  take_se = c->pool < room ? c->pool : room;
-  const unsigned long long rem = c->total_primaries - c->next_primary;
-  const int left = room - take_se;
-  take_p = rem < (unsigned long long)left ? (int)rem : left;
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) misc_one(v, cur, j, sink, sc);
+  flush_counts(v.c, sc);
 }
 
 template <typename R>
 __global__ void __launch_bounds__(256) k_spawn(RunView<R> v, int cur) {
   const int nxt = cur ^ 1;
   int nn, take_se, take_p;
-  refill_plan(v.c, nxt, v.W, nn, take_se, take_p);
-  const int poolTop = v.c->pool;
+  refill_plan(v.c, nxt, v.W, v.poolCap, nn, take_se, take_p);
+  const int poolTop = v.c->pool < v.poolCap ? v.c->pool : v.poolCap;
   const unsigned long long first = v.c->next_primary;
-  const SceneView<R>& s = v.s;
-  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < take_se + take_p; j += gridDim.x * blockDim.x) {
-    if (j < take_se) {
-      store(v.w[nxt], nn + j, load(v.pool, poolTop - 1 - j));
-      continue;
-    }
-    // GaussianBeam::createElectron (NISTMonte/GaussianBeam.cu:52-65) + initializeTrajectory (MonteCarloSS.cu:99-105)
-    const unsigned long long gi = first + (unsigned long long)(j - take_se);
-    int lo = 0, hi = v.npix;
-    while (hi - lo > 1) {
-      const int mid = (lo + hi) >> 1;
-      if (v.prefix[mid] <= gi) lo = mid;
-      else hi = mid;
-    }
-    const int px = lo;
-    const unsigned long long k = gi - v.prefix[px];
-    El<R> e;
-    e.key = mix64(v.seedmix ^ mix64(((unsigned long long)px << 32) | k));
-    Rng<R> g(e.key, 0xFFFFFFFFu, 0);
-    const double u1 = (double)g.next(), u2 = (double)g.next();
-    const double r = sqrt(-2. * log(u1)) * v.width;
-    const double th = 2.0 * kPi * u2;
-    e.p[0] = v.pc[3 * px] + r * cos(th);
-    e.p[1] = v.pc[3 * px + 1] + r * sin(th);
-    e.p[2] = v.pc[3 * px + 2];
-    e.d[0] = 0; e.d[1] = 0; e.d[2] = 1;
-    e.E = (R)v.pe0[px];
-    e.Ep = e.E;
-    e.region = containing_subregion(s, s.chamber, e.p);
-    e.pixel = px;
-    e.aux = 0;
-    e.step = 0;
-    e.h[0] = e.h[1] = e.h[2] = 0;
-    store(v.w[nxt], nn + j, e);
-  }
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < take_se + take_p; j += gridDim.x * blockDim.x)
+    spawn_one(v, nxt, j, nn, take_se, poolTop, first);
 }
 
 template <typename R>
 __global__ void k_tail(RunView<R> v, int cur) {
-  if (blockIdx.x != 0 || threadIdx.x != 0) return;
-  const int nxt = cur ^ 1;
-  Counters* c = v.c;
-  int nn, take_se, take_p;
-  refill_plan(c, nxt, v.W, nn, take_se, take_p);
-  c->n[nxt] = nn + take_se + take_p;
-  c->pool -= take_se;
-  c->next_primary += (unsigned long long)take_p;
-  c->n[cur] = 0;
-  c->q[0] = c->q[1] = c->q[2] = 0;
-  c->iterations += 1;
-  c->done = (c->n[nxt] == 0 && c->pool == 0 && c->next_primary == c->total_primaries) ? 1 : 0;
+  if (blockIdx.x == 0 && threadIdx.x == 0) tail_update(v.c, cur, v.W, v.poolCap);
 }
+
+#ifdef CM_TRACE
+static TraceRec* g_trace = nullptr;
+static int* g_ntrace = nullptr;
+static int g_tracecap = 0;
+#endif
 
 template <typename R>
 static int alloc_wave(std::vector<void*>& allocs, Wave<R>& w, int cap) {
@@ -836,10 +561,9 @@ static int alloc_wave(std::vector<void*>& allocs, Wave<R>& w, int cap) {
 }
 
 template <typename R>
-static int ensure_buffers(cm_context* ctx, int W) {
+static int ensure_buffers(cm_context* ctx, int W, int poolCap) {
   RunBuffers<R>& rb = buffers_of<R>(ctx);
-  const int poolCap = 4 * W;
-  if (rb.cap >= W && rb.poolCap >= poolCap) return 0;
+  if (rb.cap == W && rb.poolCap >= poolCap) return 0;
   rb.release();
   int rc;
   if ((rc = alloc_wave(rb.allocs, rb.w[0], W)) || (rc = alloc_wave(rb.allocs, rb.w[1], W)) ||
@@ -858,15 +582,22 @@ static int ensure_buffers(cm_context* ctx, int W) {
 
 // Transport loop.  Inputs are device arrays.
 template <typename R>
-static int run_device(cm_context* ctx, const cm_run_desc* d, uint32_t* back, uint32_t* fwd, cm_run_stats* st,
+static int run_device_once(cm_context* ctx, const cm_run_desc* d, uint32_t* back, uint32_t* fwd, cm_run_stats* st,
                       cudaStream_t stream, const unsigned long long* prefix_dev, const double* e0ref_dev,
-                      unsigned long long total) {
+                      const unsigned long long* pkey_dev, unsigned long long total) {
   int rc;
   if ((rc = build_scene<R>(ctx, scene_of<R>(ctx)))) return rc;
   const int W = d->wave > 0 ? d->wave : (sizeof(R) == 8 ? (1 << 20) : (1 << 21));
-  if ((rc = ensure_buffers<R>(ctx, W))) return rc;
+  RunBuffers<R>& rb0 = buffers_of<R>(ctx);
+  const int poolWant = rb0.cap == W && rb0.poolCap > 8 * W ? rb0.poolCap : 8 * W;
+  if ((rc = ensure_buffers<R>(ctx, W, poolWant))) return rc;
   RunBuffers<R>& rb = buffers_of<R>(ctx);
   RunView<R> v;
+#ifdef CM_TRACE
+  v.trace = g_trace;
+  v.ntrace = g_ntrace;
+  v.tracecap = g_tracecap;
+#endif
   v.s = scene_of<R>(ctx).view;
   v.s.chamber = d->chamber;
   v.w[0] = rb.w[0];
@@ -882,8 +613,8 @@ static int run_device(cm_context* ctx, const cm_run_desc* d, uint32_t* back, uin
   v.pnbins = d->pixel_nbins;
   v.prefix = prefix_dev;
   v.npix = d->npix;
-  v.width = d->beam_width;
-  v.seedmix = mix64(d->seed ^ 0x243F6A8885A308D3ULL);
+  v.width = d->beam_width * 1e9;  // m -> nm
+  v.pkey = pkey_dev;
   v.back = back;
   v.fwd = fwd;
   v.stride = d->hist_stride;
@@ -893,7 +624,7 @@ static int run_device(cm_context* ctx, const cm_run_desc* d, uint32_t* back, uin
   c0.total_primaries = total;
   CM_CUDA(cudaMemcpyAsync(ctx->counters, &c0, sizeof(c0), cudaMemcpyHostToDevice, stream));
   const int grid = ctx->nsm * 8;
-  const int maxIt = d->max_iterations > 0 ? d->max_iterations : 2000000;
+  const int maxIt = d->max_iterations > 0 ? d->max_iterations : 500000;
   cudaEvent_t e0, e1;
   CM_CUDA(cudaEventCreate(&e0));
   CM_CUDA(cudaEventCreate(&e1));
@@ -901,15 +632,30 @@ static int run_device(cm_context* ctx, const cm_run_desc* d, uint32_t* back, uin
   const int K = 8;
   cudaGraph_t graph;
   cudaGraphExec_t exec;
+  // profile: an event before the first kernel and after each kernel of every iteration
+  std::vector<cudaEvent_t> pev;
+  if (d->profile) {
+    pev.resize((size_t)2 * K * 6 + 1);
+    for (auto& ev : pev) CM_CUDA(cudaEventCreate(&ev));
+  }
+  double kms[6] = {0, 0, 0, 0, 0, 0};
   CM_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+  if (d->profile) cudaEventRecordWithFlags(pev[0], stream, cudaEventRecordExternal);
   for (int it = 0; it < 2 * K; ++it) {
     const int cur = it & 1;
+    cudaEvent_t* ev = d->profile ? &pev[(size_t)it * 6 + 1] : nullptr;
     k_flight<R><<<grid, 256, 0, stream>>>(v, cur);
+    if (ev) cudaEventRecordWithFlags(ev[0], stream, cudaEventRecordExternal);
     k_elastic<R><<<grid, 256, 0, stream>>>(v, cur);
+    if (ev) cudaEventRecordWithFlags(ev[1], stream, cudaEventRecordExternal);
     k_inelastic<R><<<grid, 256, 0, stream>>>(v, cur);
+    if (ev) cudaEventRecordWithFlags(ev[2], stream, cudaEventRecordExternal);
     k_misc<R><<<grid, 256, 0, stream>>>(v, cur);
+    if (ev) cudaEventRecordWithFlags(ev[3], stream, cudaEventRecordExternal);
     k_spawn<R><<<grid, 256, 0, stream>>>(v, cur);
+    if (ev) cudaEventRecordWithFlags(ev[4], stream, cudaEventRecordExternal);
     k_tail<R><<<1, 32, 0, stream>>>(v, cur);
+    if (ev) cudaEventRecordWithFlags(ev[5], stream, cudaEventRecordExternal);
   }
   CM_CUDA(cudaStreamEndCapture(stream, &graph));
   CM_CUDA(cudaGraphInstantiate(&exec, graph, 0));
@@ -921,13 +667,43 @@ static int run_device(cm_context* ctx, const cm_run_desc* d, uint32_t* back, uin
     iters += 2 * K;
     CM_CUDA(cudaMemcpyAsync(ctx->counters_host, ctx->counters, sizeof(Counters), cudaMemcpyDeviceToHost, stream));
     CM_CUDA(cudaStreamSynchronize(stream));
+    if (d->profile) {
+      for (int it = 0; it < 2 * K; ++it)
+        for (int k = 0; k < 6; ++k) {
+          float t = 0;
+          cudaEventElapsedTime(&t, pev[(size_t)it * 6 + k], pev[(size_t)it * 6 + k + 1]);
+          kms[k] += t;
+        }
+    }
     if (ctx->counters_host->error) {
       status = fail(ctx->counters_host->error, "secondary pool overflow; raise the wave size");
       break;
     }
     if (ctx->counters_host->done) break;
     if (iters >= maxIt) {
-      status = fail(CM_ELIMIT, "iteration limit reached");
+      const Counters& hc = *ctx->counters_host;
+      char msg[256];
+      snprintf(msg, sizeof(msg), "iteration limit reached (live %d %d, pool %d, primaries %llu of %llu)", hc.n[0],
+               hc.n[1], hc.pool, hc.next_primary, hc.total_primaries);
+      status = fail(CM_ELIMIT, msg);
+      if (getenv("CM_DEBUG_DUMP")) {  // print a few of the electrons still alive
+        const int cur = hc.n[0] ? 0 : 1;
+        const int k = std::min(8, hc.n[cur]);
+        std::vector<double> px(k), py(k), pz(k);
+        std::vector<R> E(k), dz(k);
+        std::vector<int> reg(k);
+        std::vector<uint32_t> stp(k);
+        cudaMemcpy(px.data(), rb.w[cur].px, k * 8, cudaMemcpyDeviceToHost);
+        cudaMemcpy(py.data(), rb.w[cur].py, k * 8, cudaMemcpyDeviceToHost);
+        cudaMemcpy(pz.data(), rb.w[cur].pz, k * 8, cudaMemcpyDeviceToHost);
+        cudaMemcpy(E.data(), rb.w[cur].E, k * sizeof(R), cudaMemcpyDeviceToHost);
+        cudaMemcpy(dz.data(), rb.w[cur].dz, k * sizeof(R), cudaMemcpyDeviceToHost);
+        cudaMemcpy(reg.data(), rb.w[cur].region, k * 4, cudaMemcpyDeviceToHost);
+        cudaMemcpy(stp.data(), rb.w[cur].step, k * 4, cudaMemcpyDeviceToHost);
+        for (int i = 0; i < k; ++i)
+          fprintf(stderr, "live[%d] pos %g %g %g nm E %g eV dz %g region %d step %u\n", i, px[i], py[i], pz[i],
+                  (double)E[i], (double)dz[i], reg[i], stp[i]);
+      }
       break;
     }
   }
@@ -937,6 +713,7 @@ static int run_device(cm_context* ctx, const cm_run_desc* d, uint32_t* back, uin
   cudaEventElapsedTime(&ms, e0, e1);
   cudaGraphExecDestroy(exec);
   cudaGraphDestroy(graph);
+  for (auto& ev : pev) cudaEventDestroy(ev);
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   CM_CUDA(cudaGetLastError());
@@ -950,8 +727,36 @@ static int run_device(cm_context* ctx, const cm_run_desc* d, uint32_t* back, uin
     st->secondaries = (int64_t)c.secondaries;
     st->iterations = (int64_t)c.iterations;
     st->device_ms = ms;
+    for (int k = 0; k < 6; ++k) {
+      st->kernel_ms[k] = kms[k];
+      st->kernel_launches[k] = (int64_t)iters;
+    }
+    for (int k = 0; k < 4; ++k) st->units[k] = (int64_t)c.units[k];
   }
   return status;
+}
+
+// Every electron's random stream is keyed by its lineage, so a run that
+// overflowed the secondary pool is repeated with a larger pool and gives the
+// same tallies it would have given the first time.
+template <typename R>
+static int run_device(cm_context* ctx, const cm_run_desc* d, uint32_t* back, uint32_t* fwd, cm_run_stats* st,
+                      cudaStream_t stream, const unsigned long long* prefix_dev, const double* e0ref_dev,
+                      const unsigned long long* pkey_dev, unsigned long long total) {
+  const size_t hbytes = (size_t)d->npix * d->hist_stride * sizeof(uint32_t);
+  for (int attempt = 0; attempt < 4; ++attempt) {
+    const int rc = run_device_once<R>(ctx, d, back, fwd, st, stream, prefix_dev, e0ref_dev, pkey_dev, total);
+    if (rc != CM_EOVERFLOW) return rc;
+    RunBuffers<R>& rb = buffers_of<R>(ctx);
+    const int W = rb.cap;
+    const long long want = 2LL * rb.poolCap;
+    if (want > (1LL << 30)) return rc;
+    int e;
+    if ((e = ensure_buffers<R>(ctx, W, (int)want))) return e;
+    CM_CUDA(cudaMemsetAsync(back, 0, hbytes, stream));
+    CM_CUDA(cudaMemsetAsync(fwd, 0, hbytes, stream));
+  }
+  return fail(CM_EOVERFLOW, "secondary pool overflow");
 }
 
 // ------------------------------------------------------------------ per-function kernels
@@ -985,15 +790,15 @@ template <typename R> __global__ void k_eval_tabulated(SceneView<R> s, int mech,
   dir_from_angles(d, (R)q[1], (R)q[2]);
   o[0] = (double)tabulated_rate(s, k, E) * 1e9;
   FixedRng<R> g{q + 3, 6, 0};
-  R sd[3] = {0, 0, 0}, sE = 0;
-  const bool made = tabulated_scatter(s, k, d, E, sd, sE, g);
+  R sd[3] = {0, 0, 0}, sE = 0, th = 0;
+  const bool made = tabulated_scatter(s, k, d, E, sd, sE, g, &th);
   o[1] = (double)E * kEV;
   o[2] = d[0]; o[3] = d[1]; o[4] = d[2];
   o[5] = made;
   o[6] = made ? (double)sE * kEV : 0.;
   o[7] = sd[0]; o[8] = sd[1]; o[9] = sd[2];
   o[10] = g.used;
-  o[11] = 0;
+  o[11] = th;
 }
 
 template <typename R> __global__ void k_eval_elastic(SceneView<R> s, int mech, int n, const double* in, double* out) {
@@ -1115,6 +920,8 @@ int cm_context_create(int device, cm_context** out) {
   std::unique_ptr<cm_context> c(new cm_context());
   c->device = device;
   c->nsm = prop.multiProcessorCount;
+  // the flight kernel's call tree through nested NormalIntersectionShapes needs a few KB of local stack
+  CM_CUDA(cudaDeviceSetLimit(cudaLimitStackSize, 8192));
   CM_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
   CM_CUDA(cudaMalloc(&c->counters, sizeof(Counters)));
   CM_CUDA(cudaMallocHost(&c->counters_host, sizeof(Counters)));
@@ -1442,7 +1249,7 @@ static int check_desc(cm_context* ctx, const cm_run_desc* d) {
 
 struct PixelPrep {
   std::vector<double> center_nm, e0, e0ref;
-  std::vector<unsigned long long> prefix;
+  std::vector<unsigned long long> prefix, key;
   unsigned long long total = 0;
 };
 
@@ -1462,6 +1269,10 @@ static int prep_pixels(const cm_run_desc* d, const double* center, const double*
     p.e0ref[i] = energy[i] * kFromSIeV;  // BackscatterStats: FromSI::eV(beam energy)
     p.prefix[i + 1] = p.prefix[i] + (unsigned long long)nprim[i];
   }
+  p.key.resize(d->npix);
+  for (int i = 0; i < d->npix; ++i)
+    p.key[i] = d->pixel_key ? (unsigned long long)d->pixel_key[i]
+                            : mix64(mix64(d->seed ^ 0x243F6A8885A308D3ULL) + (unsigned long long)i);
   p.total = p.prefix[d->npix];
   return 0;
 }
@@ -1485,11 +1296,12 @@ static int run_common(cm_context* ctx, const cm_run_desc* d, const double* cente
   if (rc) return rc;
   std::vector<void*> allocs;
   double *c_dev, *e0_dev, *e0ref_dev;
-  unsigned long long* prefix_dev;
+  unsigned long long *prefix_dev, *key_dev;
   int* nbins_dev = nbins_dev_in;
   std::vector<int> nb(nbins_h, nbins_h + d->npix);
   if ((rc = up(allocs, p.center_nm, &c_dev, stream)) || (rc = up(allocs, p.e0, &e0_dev, stream)) ||
       (rc = up(allocs, p.e0ref, &e0ref_dev, stream)) || (rc = up(allocs, p.prefix, &prefix_dev, stream)) ||
+      (rc = up(allocs, p.key, &key_dev, stream)) ||
       (!nbins_dev && (rc = up(allocs, nb, &nbins_dev, stream)))) {
     for (void* a : allocs) cudaFree(a);
     return rc;
@@ -1499,8 +1311,8 @@ static int run_common(cm_context* ctx, const cm_run_desc* d, const double* cente
   dd.pixel_energy = e0_dev;
   dd.pixel_nbins = nbins_dev;
   rc = d->precision == CM_PREC_FP64
-           ? run_device<double>(ctx, &dd, back_dev, fwd_dev, st, stream, prefix_dev, e0ref_dev, p.total)
-           : run_device<float>(ctx, &dd, back_dev, fwd_dev, st, stream, prefix_dev, e0ref_dev, p.total);
+           ? run_device<double>(ctx, &dd, back_dev, fwd_dev, st, stream, prefix_dev, e0ref_dev, key_dev, p.total)
+           : run_device<float>(ctx, &dd, back_dev, fwd_dev, st, stream, prefix_dev, e0ref_dev, key_dev, p.total);
   cudaStreamSynchronize(stream);
   for (void* a : allocs) cudaFree(a);
   return rc;
@@ -1540,7 +1352,16 @@ int cm_run_device(cm_context* ctx, const cm_run_desc* d, uint32_t* back, uint32_
   if (!d->pixel_center || !d->pixel_energy || !d->pixel_nprim || !d->pixel_nbins || !back || !fwd)
     return fail(CM_EINVAL, "null array");
   CM_CUDA(cudaSetDevice(ctx->device));
-  cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
+  // the loop is captured into a graph on the engine's own stream; the caller's
+  // stream (possibly the legacy default stream, which cannot be captured) is
+  // ordered before and after it with events
+  cudaStream_t caller = (cudaStream_t)stream;
+  cudaStream_t s = ctx->stream;
+  cudaEvent_t ein, eout;
+  CM_CUDA(cudaEventCreateWithFlags(&ein, cudaEventDisableTiming));
+  CM_CUDA(cudaEventCreateWithFlags(&eout, cudaEventDisableTiming));
+  CM_CUDA(cudaEventRecord(ein, caller));
+  CM_CUDA(cudaStreamWaitEvent(s, ein, 0));
   // the small per-pixel arrays are read back to build the primary prefix and the unit conversions
   std::vector<double> c(3 * (size_t)d->npix), e(d->npix);
   std::vector<int> np(d->npix), nb(d->npix);
@@ -1548,11 +1369,24 @@ int cm_run_device(cm_context* ctx, const cm_run_desc* d, uint32_t* back, uint32_
   CM_CUDA(cudaMemcpyAsync(e.data(), d->pixel_energy, e.size() * 8, cudaMemcpyDeviceToHost, s));
   CM_CUDA(cudaMemcpyAsync(np.data(), d->pixel_nprim, np.size() * 4, cudaMemcpyDeviceToHost, s));
   CM_CUDA(cudaMemcpyAsync(nb.data(), d->pixel_nbins, nb.size() * 4, cudaMemcpyDeviceToHost, s));
+  std::vector<uint64_t> keys;
+  cm_run_desc dh = *d;
+  if (d->pixel_key) {
+    keys.resize(d->npix);
+    CM_CUDA(cudaMemcpyAsync(keys.data(), d->pixel_key, keys.size() * 8, cudaMemcpyDeviceToHost, s));
+    dh.pixel_key = keys.data();
+  }
   CM_CUDA(cudaStreamSynchronize(s));
+  d = &dh;
   const size_t hbytes = (size_t)d->npix * d->hist_stride * sizeof(uint32_t);
   CM_CUDA(cudaMemsetAsync(back, 0, hbytes, s));
   CM_CUDA(cudaMemsetAsync(fwd, 0, hbytes, s));
-  return run_common(ctx, d, c.data(), e.data(), np.data(), nb.data(), (int*)d->pixel_nbins, back, fwd, st, s);
+  rc = run_common(ctx, d, c.data(), e.data(), np.data(), nb.data(), (int*)d->pixel_nbins, back, fwd, st, s);
+  cudaEventRecord(eout, s);
+  cudaStreamWaitEvent(caller, eout, 0);
+  cudaEventDestroy(ein);
+  cudaEventDestroy(eout);
+  return rc;
 }
 
 // ---- per-function entry points

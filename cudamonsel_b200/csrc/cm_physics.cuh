@@ -59,7 +59,7 @@ template <typename R> CM_D R pick_be(const Mech& k, R deltaE) {
 // the primary (updated in place); returns true with sd/sE set when a
 // secondary is generated.  Deviates come in the reference's order.
 template <typename R, typename G>
-CM_D bool tabulated_scatter(const SceneView<R>& s, const Mech& k, R d[3], R& E, R sd[3], R& sE, G& g) {
+CM_D bool tabulated_scatter(const SceneView<R>& s, const Mech& k, R d[3], R& E, R sd[3], R& sE, G& g, R* theta_out = nullptr) {
   const R kE0 = E;
   const R kE = kE0 + (R)k.energyOffset;
   if (kE < (R)k.eiDomain0) return false;
@@ -75,6 +75,7 @@ CM_D bool tabulated_scatter(const SceneView<R>& s, const Mech& k, R d[3], R& E, 
     if (red > R(1)) red = 1;
     else if (red < R(0)) red = 0;
     theta = table_interp(s, k.tTheta, kE, red, randoms[1], 3);
+    if (theta_out) *theta_out = theta;
     phi = R(2) * R(kPi) * randoms[2];
     update_dir(d, theta, phi);
   }
@@ -103,7 +104,7 @@ CM_D bool tabulated_scatter(const SceneView<R>& s, const Mech& k, R d[3], R& E, 
   if (be > 0) {  // core level: isotropic
     energySE = (deltaE + bEref) - be;
     if ((energySE + ecb) < minGen) return false;
-    const R thetaSE = macos(R(1) - (R(2) * g.next()));
+    const R thetaSE = iso_angle(g.next());
     const R phiSE = R(2) * R(kPi) * g.next();
     dir_from_angles(sd, thetaSE, phiSE);
     sE = energySE;
@@ -139,7 +140,7 @@ CM_D bool tabulated_scatter(const SceneView<R>& s, const Mech& k, R d[3], R& E, 
   else if (e0 > (R)k.rangeSE0hi) e0 = (R)k.rangeSE0hi;
   energySE = (deltaE + e0) - off;
   if ((energySE + ecb) < minGen) return false;
-  const R thetaSE = macos(R(1) - (R(2) * g.next()));
+  const R thetaSE = iso_angle(g.next());
   const R phiSE = R(2) * R(kPi) * g.next();
   dir_from_angles(sd, thetaSE, phiSE);
   sE = energySE;

@@ -1,0 +1,394 @@
+// cm_wave.cuh -- the wavefront: electron records, queues and the per-electron
+// work of each event kernel.
+//
+// Every function here handles one electron and is host-callable; the kernels
+// in cm_engine.cu are grid-stride loops over them with a DeviceSink that does
+// warp-aggregated appends.  Reference paths relative to
+// CudaMONSEL/CudaMONSEL/gov/nist/.
+#pragma once
+#include "cm_physics.cuh"
+
+namespace cm {
+
+// structure-of-arrays electron records (one per wave slot)
+template <typename R>
+struct Wave {
+  double *px, *py, *pz;
+  R *dx, *dy, *dz;
+  R *E, *Ep;
+  int *region, *pixel, *aux;
+  uint32_t* step;
+  unsigned long long* key;
+  R *hx, *hy, *hz;
+};
+
+struct Counters {
+  int n[2];
+  int pool;
+  int q[3];
+  int error;
+  int done;
+  unsigned long long next_primary, total_primaries;
+  unsigned long long steps, scatters, barriers, escapes, secondaries;
+  unsigned long long iterations;
+  unsigned long long units[4];
+};
+
+template <typename R>
+struct El {
+  double p[3];
+  R d[3];
+  R E, Ep;
+  int region, pixel, aux;
+  uint32_t step;
+  unsigned long long key;
+  R h[3];
+};
+
+template <typename R> CM_D El<R> load(const Wave<R>& w, int i) {
+  El<R> e;
+  e.p[0] = w.px[i]; e.p[1] = w.py[i]; e.p[2] = w.pz[i];
+  e.d[0] = w.dx[i]; e.d[1] = w.dy[i]; e.d[2] = w.dz[i];
+  e.E = w.E[i]; e.Ep = w.Ep[i];
+  e.region = w.region[i]; e.pixel = w.pixel[i]; e.aux = w.aux[i];
+  e.step = w.step[i]; e.key = w.key[i];
+  e.h[0] = w.hx[i]; e.h[1] = w.hy[i]; e.h[2] = w.hz[i];
+  return e;
+}
+
+template <typename R> CM_D void store(const Wave<R>& w, int i, const El<R>& e) {
+  w.px[i] = e.p[0]; w.py[i] = e.p[1]; w.pz[i] = e.p[2];
+  w.dx[i] = e.d[0]; w.dy[i] = e.d[1]; w.dz[i] = e.d[2];
+  w.E[i] = e.E; w.Ep[i] = e.Ep;
+  w.region[i] = e.region; w.pixel[i] = e.pixel; w.aux[i] = e.aux;
+  w.step[i] = e.step; w.key[i] = e.key;
+  w.hx[i] = e.h[0]; w.hy[i] = e.h[1]; w.hz[i] = e.h[2];
+}
+
+enum { Q_EL = 0, Q_TAB = 1, Q_MISC = 2 };
+enum { AUX_MECH = 1, AUX_BARRIER = 2, AUX_PASS = 3 };
+CM_HD int aux_pack(int kind, int v) { return (kind << 24) | (v & 0xffffff); }
+CM_HD int aux_kind(int a) { return a >> 24; }
+CM_HD int aux_val(int a) { return a & 0xffffff; }
+
+#ifdef CM_TRACE
+// step records of a debugging build (never compiled into the library)
+struct TraceRec {
+  unsigned long long key;
+  unsigned int step;
+  int region, next, kind;
+  double E, p[3], d[3];
+};
+#endif
+
+template <typename R>
+struct RunView {
+#ifdef CM_TRACE
+  TraceRec* trace;
+  int* ntrace;
+  int tracecap;
+#endif
+  SceneView<R> s;
+  Wave<R> w[2];
+  Wave<R> pool;
+  int* q[3];
+  Counters* c;
+  int W, poolCap;
+  const double* pc;      // pixel centres, nm
+  const double* pe0;     // beam energy, eV
+  const double* pe0ref;  // histogram top edge in eV as the reference computes it
+  const int* pnbins;
+  const unsigned long long* prefix;
+  const unsigned long long* pkey;  // per-pixel stream key
+  int npix;
+  double width;          // nm
+  uint32_t *back, *fwd;
+  int stride;
+};
+
+// per-thread event counts, reduced once per warp by the kernels
+struct StepCounts {
+  unsigned long long steps = 0, scat = 0, bar = 0, esc = 0, sec = 0;
+};
+
+// Histogram::bin (Utility/Histogram.cu:73-80) over bins min + i*delta with
+// Algorithm::binarySearch (Amphibian/Algorithm.cu:5-14): exact match or the
+// insertion point.
+CM_D int hist_bin(double max, int nbins, double val) {
+  const double delta = max / nbins;
+  int l = 0, r = nbins;
+  while (l <= r) {
+    const int mid = l + (r - l) / 2;
+    const double bm = mid == 0 ? 0.0 : 0.0 + mid * delta;
+    if (bm == val) return mid;
+    if (bm < val) l = mid + 1;
+    else r = mid - 1;
+  }
+  return l;
+}
+
+// BackscatterStats::actionPerformed for a BackscatterEvent (NISTMonte/BackscatterStats.cu:147-170)
+template <typename R, typename Sink> CM_D void tally_escape(const RunView<R>& v, const El<R>& e, Sink& sink) {
+  const int px = e.pixel;
+  const double E0ref = v.pe0ref[px];
+  double val = (double)e.E;
+  if (e.E == (R)v.pe0[px]) val = E0ref;  // electrons that never lost energy carry E0 exactly, as in the reference
+  const double elevation = (kPi / 2) - atan2(e.p[2], sqrt((e.p[0] * e.p[0]) + (e.p[1] * e.p[1])));
+  const int nb = v.pnbins[px];
+  const int b = hist_bin(E0ref, nb, val) + 1;
+  if (b > nb + 1) return;  // past the overflow slot: the reference writes out of bounds and never counts it
+  uint32_t* h = elevation < (kPi / 2.0) ? v.fwd : v.back;
+  sink.count(h + (size_t)px * v.stride + b);
+}
+
+#ifdef CM_TRACE
+template <typename R, typename Sink> CM_D void cm_trace(const RunView<R>& v, const El<R>& e, int next, int kind, Sink& sink) {
+  const int k = sink.append(v.ntrace);
+  if (k >= v.tracecap) return;
+  TraceRec& t = v.trace[k];
+  t.key = e.key; t.step = e.step; t.region = e.region; t.next = next; t.kind = kind; t.E = (double)e.E;
+  for (int j = 0; j < 3; ++j) { t.p[j] = e.p[j]; t.d[j] = (double)e.d[j]; }
+}
+#endif
+
+// ---------------------------------------------------------------- flight
+// MonteCarloSS::takeStep (NISTMonte/MonteCarloSS.cu:107-163) up to the event:
+// region check, MONSEL_MaterialScatterModel::randomMeanPathLength, the
+// candidate point, RegionBase::findEndOfStep, the slowing-down loss, the
+// tracking cut; the step's end is queued for its event kernel, escapes are tallied.
+template <typename R, typename Sink> CM_D void flight_one(const RunView<R>& v, int cur, int i, Sink& sink, StepCounts& sc) {
+  const SceneView<R>& s = v.s;
+  const Wave<R>& W = v.w[cur];
+  El<R> e = load(W, i);
+  int reg = e.region;
+  if (reg < 0 || !shape_contains(s, s.regions[reg].shape, e.p)) reg = containing_subregion(s, s.chamber, e.p);
+  if (reg < 0) return;
+  const Msm& m = s.msms[s.regions[reg].msm];
+  Rng<R> g(e.key, e.step, 0);
+  R cum[kMaxMech];
+  R total = 0;
+  const R logE = mlog(e.E);
+  for (int k = 0; k < m.nmech; ++k) {
+    total += mech_rate(s, s.mechs[m.mech0 + k], e.E, logE);
+    cum[k] = total;
+  }
+  bool complete = false;
+  double fp = 2.0 * kChamberRadiusNm;
+  if (total != R(0)) {
+    const R f = -mlog(g.next()) / total;
+    if ((double)f < fp) fp = (double)f;
+  } else if (e.step > 1000000u) {
+    complete = true;
+  }
+  double p1[3] = {e.p[0] + fp * (double)e.d[0], e.p[1] + fp * (double)e.d[1], e.p[2] + fp * (double)e.d[2]};
+  double hn[3];
+  const int next = find_end_of_step(s, reg, e.p, p1, hn);
+  const double dd = sqrt((p1[0] - e.p[0]) * (p1[0] - e.p[0]) + (p1[1] - e.p[1]) * (p1[1] - e.p[1]) +
+                         (p1[2] - e.p[2]) * (p1[2] - e.p[2]));
+  const R dE = m.csd ? jln_compute(m.jln, (R)dd, e.E) : R(0);
+  e.p[0] = p1[0]; e.p[1] = p1[1]; e.p[2] = p1[2];
+  e.Ep = e.E;
+  e.E += dE;
+  e.step += 1;
+  e.region = reg;
+  ++sc.steps;
+  if ((e.E < (R)m.minE) || complete) return;
+  int queue;
+  if (next == reg) {
+    ++sc.scat;
+    if (total == R(0)) {
+      queue = Q_MISC;
+      e.aux = aux_pack(AUX_PASS, 0);
+    } else {
+      // MONSEL_MaterialScatterModel::scatter (:93-134): the cache holds the step's starting energy
+      const R r = g.next() * total;
+      int idx = 0;
+      while (idx < m.nmech - 1 && cum[idx] < r) ++idx;
+      const int kind = s.mechs[m.mech0 + idx].kind;
+      if (kind == MECH_POLARON) return;  // GanachaudMokraniPolaronTrapSM::scatter: trapped, E = 0
+      queue = kind == MECH_NISTMOTT ? Q_EL : kind == MECH_TABULATED ? Q_TAB : Q_MISC;
+      e.aux = aux_pack(AUX_MECH, idx);
+    }
+  } else if (next >= 0) {
+    ++sc.bar;
+    queue = Q_MISC;
+    e.aux = aux_pack(AUX_BARRIER, next);
+    e.h[0] = (R)hn[0]; e.h[1] = (R)hn[1]; e.h[2] = (R)hn[2];
+  } else {
+    ++sc.esc;
+    tally_escape(v, e, sink);
+#ifdef CM_TRACE
+    queue = 9;
+    cm_trace(v, e, next, queue, sink);
+#endif
+    return;
+  }
+#ifdef CM_TRACE
+  cm_trace(v, e, next, queue * 100 + aux_kind(e.aux) * 10 + aux_val(e.aux) % 10, sink);
+#endif
+  store(W, i, e);
+  const int slot = sink.append_q(v.c->q, queue);
+  v.q[queue][slot] = i;
+}
+
+// append a surviving electron to the next wave
+template <typename R, typename Sink> CM_D void keep(const RunView<R>& v, int nxt, const El<R>& e, Sink& sink) {
+  const int slot = sink.append(&v.c->n[nxt]);
+  store(v.w[nxt], slot, e);
+}
+
+// push a secondary to the pool when MonteCarloSS::trackSecondaryElectron (:165-174) would track it
+template <typename R, typename Sink>
+CM_D void push_secondary(const RunView<R>& v, const El<R>& pe, const R sd[3], R sE, Sink& sink, StepCounts& sc) {
+  const Msm& m = v.s.msms[v.s.regions[pe.region].msm];
+  if (!(sE > (R)m.minE)) return;
+  El<R> se;
+  se.p[0] = pe.p[0]; se.p[1] = pe.p[1]; se.p[2] = pe.p[2];
+  se.d[0] = sd[0]; se.d[1] = sd[1]; se.d[2] = sd[2];
+  se.E = sE; se.Ep = sE;
+  se.region = pe.region;
+  se.pixel = pe.pixel;
+  se.aux = 0;
+  se.step = 0;
+  se.key = mix64(pe.key ^ (0x9E3779B97F4A7C15ULL * (unsigned long long)pe.step));
+  se.h[0] = se.h[1] = se.h[2] = 0;
+  const int slot = sink.append(&v.c->pool);
+  if (slot >= v.poolCap) {
+    sink.error(&v.c->error, -5 /* CM_EOVERFLOW */);
+    return;
+  }
+  store(v.pool, slot, se);
+  ++sc.sec;
+}
+
+// SelectableElasticSM events
+template <typename R, typename Sink> CM_D void elastic_one(const RunView<R>& v, int cur, int j, Sink& sink) {
+  const SceneView<R>& s = v.s;
+  El<R> e = load(v.w[cur], v.q[Q_EL][j]);
+  const Msm& m = s.msms[s.regions[e.region].msm];
+  const Mech& k = s.mechs[m.mech0 + aux_val(e.aux)];
+  Rng<R> g(e.key, e.step - 1, 1);
+  elastic_scatter(s, k, e.d, e.Ep, g);
+  if (!(e.E < (R)m.minE)) keep(v, cur ^ 1, e, sink);
+}
+
+// TabulatedInelasticSM events
+template <typename R, typename Sink> CM_D void inelastic_one(const RunView<R>& v, int cur, int j, Sink& sink, StepCounts& sc) {
+  const SceneView<R>& s = v.s;
+  El<R> e = load(v.w[cur], v.q[Q_TAB][j]);
+  const Msm& m = s.msms[s.regions[e.region].msm];
+  const Mech& k = s.mechs[m.mech0 + aux_val(e.aux)];
+  Rng<R> g(e.key, e.step - 1, 1);
+  R sd[3], sE;
+  const bool made = tabulated_scatter(s, k, e.d, e.E, sd, sE, g);
+  if (!(e.E < (R)m.minE)) keep(v, cur ^ 1, e, sink);
+  if (made) push_secondary(v, e, sd, sE, sink, sc);
+}
+
+// barrier crossings, FittedInelSM, phonon, and steps that end without a mechanism
+template <typename R, typename Sink> CM_D void misc_one(const RunView<R>& v, int cur, int j, Sink& sink, StepCounts& sc) {
+  const SceneView<R>& s = v.s;
+  El<R> e = load(v.w[cur], v.q[Q_MISC][j]);
+  const Msm& m = s.msms[s.regions[e.region].msm];
+  const int kind = aux_kind(e.aux);
+  Rng<R> g(e.key, e.step - 1, 1);
+  if (kind == AUX_BARRIER) {
+    // MonteCarloSS::takeStep (:143-156): barrierScatter, a nudge along the new direction, region update
+    const double hn[3] = {(double)e.h[0], (double)e.h[1], (double)e.h[2]};
+    e.region = barrier_scatter(s, m, e.p, e.d, e.E, e.region, aux_val(e.aux), hn, g);
+    e.p[0] += kSmallDispNm * (double)e.d[0];
+    e.p[1] += kSmallDispNm * (double)e.d[1];
+    e.p[2] += kSmallDispNm * (double)e.d[2];
+    if (!shape_contains(s, s.regions[e.region].shape, e.p)) e.region = containing_subregion(s, s.chamber, e.p);
+    keep(v, cur ^ 1, e, sink);
+    return;
+  }
+  if (kind == AUX_MECH) {
+    const Mech& k = s.mechs[m.mech0 + aux_val(e.aux)];
+    if (k.kind == MECH_FITTED) {  // FittedInelSM::scatter (FittedInelSM.cu:13-18)
+      const R phi = R(2) * R(kPi) * g.next();
+      const R theta = iso_angle(g.next());
+      R sd[3];
+      dir_from_angles(sd, theta, phi);
+      push_secondary(v, e, sd, (R)(k.energySEgen + k.eFermi), sink, sc);
+    } else if (k.kind == MECH_PHONON) {
+      phonon_scatter(k, e.d, e.E, e.Ep, g);
+    }
+  }
+  if (!(e.E < (R)m.minE)) keep(v, cur ^ 1, e, sink);
+}
+
+// refill plan of the next wave: secondaries from the pool first; new primaries
+// only once the pool is empty, and at most W/32 per iteration so that the
+// cascades of one batch of primaries do not all peak together
+CM_D void refill_plan(const Counters* c, int nxt, int W, int poolCap, int& nn, int& take_se, int& take_p) {
+  nn = c->n[nxt];
+  const int room = W - nn > 0 ? W - nn : 0;
+  const int pool = c->pool < poolCap ? c->pool : poolCap;  // an overflowed pool holds poolCap valid entries
+  take_se = pool < room ? pool : room;
+  const unsigned long long rem = c->total_primaries - c->next_primary;
+  int left = pool > take_se ? 0 : room - take_se;
+  const int ramp = W / 32 > 1 ? W / 32 : 1;
+  if (left > ramp) left = ramp;
+  take_p = rem < (unsigned long long)left ? (int)rem : left;
+}
+
+// slot nn + j of the next wave: a secondary from the top of the pool or a new primary
+template <typename R> CM_D void spawn_one(const RunView<R>& v, int nxt, int j, int nn, int take_se, int poolTop,
+                                          unsigned long long first) {
+  if (j < take_se) {
+    store(v.w[nxt], nn + j, load(v.pool, poolTop - 1 - j));
+    return;
+  }
+  // GaussianBeam::createElectron (NISTMonte/GaussianBeam.cu:52-65) + initializeTrajectory (MonteCarloSS.cu:99-105)
+  const unsigned long long gi = first + (unsigned long long)(j - take_se);
+  int lo = 0, hi = v.npix;
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (v.prefix[mid] <= gi) lo = mid;
+    else hi = mid;
+  }
+  const int px = lo;
+  const unsigned long long k = gi - v.prefix[px];
+  El<R> e;
+  e.key = mix64(v.pkey[px] + mix64(k + 1));
+  Rng<R> g(e.key, 0xFFFFFFFFu, 0);
+  const double u1 = (double)g.next(), u2 = (double)g.next();
+  const double r = sqrt(-2. * log(u1)) * v.width;
+  const double th = 2.0 * kPi * u2;
+  e.p[0] = v.pc[3 * px] + r * cos(th);
+  e.p[1] = v.pc[3 * px + 1] + r * sin(th);
+  e.p[2] = v.pc[3 * px + 2];
+  e.d[0] = 0; e.d[1] = 0; e.d[2] = 1;
+  e.E = (R)v.pe0[px];
+  e.Ep = e.E;
+  e.region = containing_subregion(v.s, v.s.chamber, e.p);
+  e.pixel = px;
+  e.aux = 0;
+  e.step = 0;
+  e.h[0] = e.h[1] = e.h[2] = 0;
+  store(v.w[nxt], nn + j, e);
+}
+
+// end of an iteration: counters of the next wave, reset of this one
+CM_D void tail_update(Counters* c, int cur, int W, int poolCap) {
+  const int nxt = cur ^ 1;
+  int nn, take_se, take_p;
+  refill_plan(c, nxt, W, poolCap, nn, take_se, take_p);
+  if (c->pool > poolCap) c->pool = poolCap;
+  if (!c->done) {
+    c->units[0] += (unsigned long long)c->n[cur];
+    c->units[1] += (unsigned long long)c->q[0];
+    c->units[2] += (unsigned long long)c->q[1];
+    c->units[3] += (unsigned long long)c->q[2];
+    c->iterations += 1;
+  }
+  c->n[nxt] = nn + take_se + take_p;
+  c->pool -= take_se;
+  c->next_primary += (unsigned long long)take_p;
+  c->n[cur] = 0;
+  c->q[0] = c->q[1] = c->q[2] = 0;
+  c->done = (c->n[nxt] == 0 && c->pool == 0 && c->next_primary == c->total_primaries) ? 1 : 0;
+}
+
+}  // namespace cm

@@ -116,11 +116,26 @@ typedef struct {
   int hist_stride;             /* >= max(pixel_nbins) + 2 */
   int wave;                    /* electrons per wave; 0 = default */
   int max_iterations;          /* 0 = default */
+  const uint64_t* pixel_key;   /* [npix] random-stream key of each pixel, or NULL: derived from seed and index.
+                                  A pixel's result depends only on its key, its beam and primary count,
+                                  not on the other pixels of the run. */
+  int profile;                 /* nonzero: time each kernel with CUDA events inside the loop */
 } cm_run_desc;
+
+/* kernels of one wavefront iteration, in launch order */
+#define CM_K_FLIGHT 0
+#define CM_K_ELASTIC 1
+#define CM_K_INELASTIC 2
+#define CM_K_MISC 3
+#define CM_K_SPAWN 4
+#define CM_K_TAIL 5
 
 typedef struct {
   int64_t primaries, steps, scatter_events, barrier_events, escapes, secondaries, iterations;
   double device_ms;            /* time of the transport loop on the device */
+  double kernel_ms[6];         /* per kernel, summed over launches (profile != 0 only) */
+  int64_t kernel_launches[6];
+  int64_t units[4];            /* electrons handled by flight, elastic, inelastic, misc */
 } cm_run_stats;
 
 /* back/fwd: [npix * hist_stride] counts, index = histogram bin + 1 (0 = underflow,

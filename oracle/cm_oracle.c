@@ -1200,9 +1200,12 @@ static double pick_be(const mechanism* k, double Eq, double deltaE)
    return k->core[i - 1];
 }
 
+static double g_last_theta; /* the PE deflection sampled by the last tabulated_scatter (per-function checks) */
+
 /* TabulatedInelasticSM.cu:209-434.  Returns 1 and fills *se when a secondary is made. */
 static int tabulated_scatter(const cmo_scene* s, const mechanism* k, electron* pe, electron* se, cmo_rng* r)
 {
+   g_last_theta = 0.;
    int fixes = s->options & 1;
    double kE0 = pe->E;
    double kE = kE0 + k->energyOffset;
@@ -1221,6 +1224,7 @@ static int tabulated_scatter(const cmo_scene* s, const mechanism* k, electron* p
       else if (in[1] < 0.) in[1] = 0.;
       in[2] = randoms[1];
       theta = table_interp(&s->tables[k->tTheta], in, 3, fixes);
+      g_last_theta = theta;
       phi = 2. * PI * randoms[2];
       update_direction(&pe->theta, &pe->phi, theta, phi);
    }
@@ -1662,10 +1666,22 @@ void cmo_eval_table(cmo_scene* s, int table, int n, const double* x3, int order,
 
 void cmo_eval_tabulated(cmo_scene* s, int msm, int mech, int n, const double* in, double* out)
 {
+   cmo_eval_tabulated_stride(s, msm, mech, n, in, out, 9);
+}
+
+int cmo_table_window(cmo_scene* s, int table, double x0)
+{
+   int loc[2];
+   cmo_nu_locate(x0, s->tables[table].x[0], s->tables[table].n[0], 3, loc);
+   return loc[0];
+}
+
+void cmo_eval_tabulated_stride(cmo_scene* s, int msm, int mech, int n, const double* in, double* out, int stride)
+{
    const mechanism* k = &s->msms[msm].mech[mech];
    for (int i = 0; i < n; ++i) {
       const double* q = in + 9 * i;
-      double* o = out + 9 * i;
+      double* o = out + stride * i;
       electron e, se;
       memset(&e, 0, sizeof(e));
       e.E = e.Eprev = q[0];
@@ -1682,6 +1698,7 @@ void cmo_eval_tabulated(cmo_scene* s, int msm, int mech, int n, const double* in
       o[6] = made ? se.theta : 0;
       o[7] = made ? se.phi : 0;
       o[8] = r.used;
+      if (stride > 9) o[9] = g_last_theta;
    }
 }
 

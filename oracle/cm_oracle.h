@@ -73,6 +73,10 @@ void cmo_eval_nistmott(cmo_scene* s, int Z, int n, const double* E, const double
 void cmo_eval_table(cmo_scene* s, int table, int n, const double* x3, int order, double* out);
 void cmo_eval_tabulated(cmo_scene* s, int msm, int mech, int n, const double* in /* E th ph u0..u5 */,
                         double* out /* rate E th ph hasSE ESE thSE phSE ndev */);
+/* the same with stride >= 10 also writes the sampled PE deflection theta in column 9 */
+void cmo_eval_tabulated_stride(cmo_scene* s, int msm, int mech, int n, const double* in, double* out, int stride);
+/* first index of the 4-point window NULagrangeInterpolation::locate picks on a table's first axis */
+int cmo_table_window(cmo_scene* s, int table, double x0);
 void cmo_eval_elastic(cmo_scene* s, int msm, int mech, int n, const double* in /* E th ph u0..u3 */,
                       double* out /* rate th ph Z ndev */);
 void cmo_eval_pmma(cmo_scene* s, int msm, int n, const double* in /* E len */, double* out /* csd fittedRate polaronRate */);

@@ -1,0 +1,148 @@
+"""Whole-run parity of the CUDA engine with the reference and the oracle.
+
+Trajectories use different random streams on each side, so the comparison is
+statistical: yields per batch (a batch = one pixel of N primaries at the same
+landing point) give the standard errors, BSE and SE yields must agree within
+3 standard errors, and the back-scattered energy spectra must pass a
+two-sample chi-squared test (p > 1e-3).  FP32 must also sit within 1 % of FP64.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN
+
+pytestmark = pytest.mark.gpu
+
+FP64, FP32 = 0, 1
+
+
+def ref_runs():
+    runs = []
+    for line in open(os.path.join(GOLDEN, "run_halfspace_1keV.txt")):
+        w = line.split()
+        if w and w[0] == "back":
+            runs.append([int(x) for x in w[1:]])
+    return np.array(runs)
+
+
+def batch_yields(back, nprim, beam_eV, nbins):
+    from cudamonsel_b200 import scenes
+    return scenes.yields(back, nprim, beam_eV, nbins)
+
+
+@pytest.fixture(scope="module")
+def half(engine):
+    from cudamonsel_b200 import scenes
+    sc = scenes.halfspace()
+    return engine, scenes.build_engine(sc, engine)
+
+
+def run_half(engine, h, prec, npix, nprim, seed, energy_eV=1000.0):
+    from cudamonsel_b200 import scenes
+    centers = np.tile([0.0, 0.0, -20e-9], (npix, 1))
+    nb = int(energy_eV / 10)
+    back, fwd, st = engine.run(h["chamber"], centers, scenes.eV(energy_eV), nprim, nb, 0.0, seed, precision=prec)
+    return back, fwd, st
+
+
+def test_halfspace_fp64_matches_reference(half):
+    """1 keV pencil beam on flat Si (the reference's configs[0] path): engine FP64, 40 x 1000
+    primaries, vs the reference's 4 x 10 000."""
+    from cudamonsel_b200 import stats
+    e, h = half
+    back, fwd, st = run_half(e, h, FP64, 40, 1000, seed=5)
+    assert st.primaries == 40000
+    bse, se = batch_yields(back, 1000, 1000.0, 100)
+    ref = ref_runs()
+    rb, rs = batch_yields(ref, 10000, 1000.0, 100)
+    # reference batches are 10x larger: scale their spread to the engine's batch size
+    zb = (bse.mean() - rb.mean()) / np.sqrt(bse.var(ddof=1) / len(bse) * (1 + len(bse) / (len(rb) * 10)))
+    zs = (se.mean() - rs.mean()) / np.sqrt(se.var(ddof=1) / len(se) * (1 + len(se) / (len(rs) * 10)))
+    print("BSE engine %.4f ref %.4f z=%.2f | SE engine %.4f ref %.4f z=%.2f" % (bse.mean(), rb.mean(), zb, se.mean(),
+                                                                              rs.mean(), zs))
+    assert abs(zb) < 3 and abs(zs) < 3
+    chi, dof, p = stats.chi2_two_sample(back.sum(0), 40000, ref.sum(0), 40000)
+    print("spectrum chi2 %.1f dof %d p %.3g" % (chi, dof, p))
+    assert p > 1e-3
+
+
+def test_halfspace_fp32_within_1pct_of_fp64(half):
+    """FP32 transport (FP64 positions and plane solves) vs FP64 on 200 x 2000 primaries each."""
+    from cudamonsel_b200 import stats
+    e, h = half
+    b64, _, _ = run_half(e, h, FP64, 200, 2000, seed=11)
+    b32, _, _ = run_half(e, h, FP32, 200, 2000, seed=12)
+    y64 = batch_yields(b64, 2000, 1000.0, 100)
+    y32 = batch_yields(b32, 2000, 1000.0, 100)
+    for name, a, b in (("BSE", y32[0], y64[0]), ("SE", y32[1], y64[1])):
+        z = stats.z_score(a, b)
+        relerr = abs(a.mean() - b.mean()) / b.mean()
+        print("%s fp32 %.5f fp64 %.5f rel %.4f z %.2f" % (name, a.mean(), b.mean(), relerr, z))
+        assert abs(z) < 3
+        assert relerr < 0.01
+    chi, dof, p = stats.chi2_two_sample(b32.sum(0), 400000, b64.sum(0), 400000)
+    print("spectrum chi2 %.1f dof %d p %.3g" % (chi, dof, p))
+    assert p > 1e-3
+
+
+def test_lines_fp64_matches_oracle(engine):
+    """PMMA lines on Si, 500 eV, sigma 1 nm: 6 landing points (gap, sidewall foot, sidewall,
+    top) engine FP64 vs the oracle's whole trajectories."""
+    import pyoracle
+    from cudamonsel_b200 import scenes
+    sc = scenes.lines()
+    h = scenes.build_engine(sc, engine)
+    xs = np.array([-60.0, -22.0, -19.0, -12.0, 0.0, 100.0]) * 1e-9
+    centers = np.stack([xs, np.zeros(6), np.full(6, -120e-9)], axis=1)
+    npix_rep = 16
+    nprim = 500
+    back, fwd, st = engine.run(h["chamber"], np.repeat(centers, npix_rep, axis=0), scenes.eV(500.0), nprim, 50, 1e-9,
+                               seed=3, precision=FP64)
+    ob, of, tl = pyoracle.run_scene(sc, centers, 1e-9, scenes.eV(500.0), nprim * 4, 77, 50)
+    for i in range(6):
+        eb, es = batch_yields(back[i * npix_rep:(i + 1) * npix_rep], nprim, 500.0, 50)
+        rb, rs = batch_yields(ob[i:i + 1], nprim * 4, 500.0, 50)
+        se_b = eb.std(ddof=1) * np.sqrt(1.0 / npix_rep + 1.0 / 4)
+        se_s = es.std(ddof=1) * np.sqrt(1.0 / npix_rep + 1.0 / 4)
+        zb = (eb.mean() - rb[0]) / se_b
+        zs = (es.mean() - rs[0]) / se_s
+        print("x=%5.1f nm BSE %.4f/%.4f z=%.2f SE %.4f/%.4f z=%.2f" % (xs[i] * 1e9, eb.mean(), rb[0], zb, es.mean(),
+                                                                    rs[0], zs))
+        assert abs(zb) < 3.5 and abs(zs) < 3.5
+
+
+def test_deterministic_and_independent_of_batch(half):
+    """Same seed -> identical tallies; a pixel's tally is the same alone and inside a larger
+    batch of other pixels when it carries the same stream key (the serving guarantee)."""
+    from cudamonsel_b200 import scenes
+    e, h = half
+    c = np.array([[0.0, 0.0, -20e-9]])
+    k = np.array([12345], dtype=np.uint64)
+    a, _, _ = e.run(h["chamber"], c, scenes.eV(1000.0), 300, 100, 0.0, 1, precision=FP64, pixel_keys=k)
+    b, _, _ = e.run(h["chamber"], c, scenes.eV(1000.0), 300, 100, 0.0, 1, precision=FP64, pixel_keys=k)
+    assert (a == b).all()
+    many = np.tile(c, (50, 1))
+    keys = np.arange(1000, 1050, dtype=np.uint64)
+    keys[17] = 12345
+    m, _, _ = e.run(h["chamber"], many, scenes.eV(1000.0), 300, 100, 0.0, 9, precision=FP64, pixel_keys=keys)
+    assert (m[17] == a[0]).all()
+    assert not (m[16] == a[0]).all()
+    a32, _, _ = e.run(h["chamber"], c, scenes.eV(1000.0), 300, 100, 0.0, 1, precision=FP32, pixel_keys=k)
+    m32, _, _ = e.run(h["chamber"], many, scenes.eV(1000.0), 300, 100, 0.0, 9, precision=FP32, pixel_keys=keys)
+    assert (m32[17] == a32[0]).all()
+
+
+def test_edge_cases(half):
+    """Empty pixels, a single primary, nbins at both ends, energies below the tracking cut."""
+    from cudamonsel_b200 import scenes
+    e, h = half
+    c = np.tile([0.0, 0.0, -20e-9], (4, 1))
+    back, fwd, st = e.run(h["chamber"], c, scenes.eV(1000.0), [0, 1, 0, 5], [1, 100, 1024, 7], 0.0, 2)
+    assert back.shape == (4, 1026)
+    assert back[0].sum() == 0 and back[2].sum() == 0
+    assert st.primaries == 6
+    # a 2 eV beam: below Si's 3.75 eV barrier after entering? (it gains 3.75 eV entering) -> tracked
+    back, fwd, st = e.run(h["chamber"], c[:1], scenes.eV(2.0), 50, 1, 0.0, 3)
+    assert st.primaries == 50
