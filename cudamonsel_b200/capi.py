@@ -22,9 +22,9 @@ EXPORTS = (
     "cm_add_mott_element", "cm_add_table", "cm_add_material", "cm_add_msm", "cm_msm_add_nistmott",
     "cm_msm_add_tabulated", "cm_msm_add_fitted", "cm_msm_add_phonon", "cm_msm_add_polaron", "cm_msm_set_csd_jln",
     "cm_msm_set_min_e", "cm_msm_set_barrier", "cm_shape_sphere", "cm_shape_planes", "cm_shape_intersection",
-    "cm_shape_translate", "cm_shape_line", "cm_region_add", "cm_run", "cm_run_device", "cm_eval_nistmott",
-    "cm_eval_table", "cm_eval_tabulated", "cm_eval_elastic", "cm_eval_csd", "cm_eval_phonon", "cm_eval_shape",
-    "cm_eval_barrier", "cm_eval_freepath",
+    "cm_shape_translate", "cm_shape_line", "cm_region_add", "cm_run", "cm_run_device", "cm_run_noalloc",
+    "cm_eval_nistmott", "cm_eval_table", "cm_eval_tabulated", "cm_eval_elastic", "cm_eval_csd", "cm_eval_phonon",
+    "cm_eval_shape", "cm_eval_barrier", "cm_eval_freepath",
 )
 
 
@@ -93,6 +93,7 @@ def load(path=LIBPATH):
         "cm_region_add": [ctx, C.c_int, C.c_int, C.c_int, i],
         "cm_run": [ctx, C.POINTER(RunDesc), C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.POINTER(RunStats)],
         "cm_run_device": [ctx, C.POINTER(RunDesc), C.c_void_p, C.c_void_p, C.POINTER(RunStats), C.c_void_p],
+        "cm_run_noalloc": [ctx, C.POINTER(RunDesc), C.c_void_p, C.c_void_p, C.POINTER(RunStats), C.c_void_p],
         "cm_eval_nistmott": [ctx, C.c_int, C.c_int, d, d, d, d, C.c_int],
         "cm_eval_table": [ctx, C.c_int, C.c_int, d, C.c_int, d, C.c_int],
         "cm_eval_tabulated": [ctx, C.c_int, C.c_int, C.c_int, d, d, C.c_int],
@@ -251,6 +252,13 @@ class Engine:
         st = RunStats()
         self._check(self.L.cm_run_device(self.h, C.byref(desc), C.c_void_p(back_ptr), C.c_void_p(fwd_ptr),
                                          C.byref(st), C.c_void_p(stream_ptr) if stream_ptr else None))
+        return st
+
+    def run_noalloc(self, desc, back_ptr, fwd_ptr, stream_ptr=None):
+        """cm_run_device without device allocations (fixed scratch array; see the header)."""
+        st = RunStats()
+        self._check(self.L.cm_run_noalloc(self.h, C.byref(desc), C.c_void_p(back_ptr), C.c_void_p(fwd_ptr),
+                                          C.byref(st), C.c_void_p(stream_ptr) if stream_ptr else None))
         return st
 
     # ---- per-function entry points

@@ -26,6 +26,8 @@
 #include <cstring>
 #include <map>
 #include <memory>
+#include <mutex>
+#include <chrono>
 #include <string>
 #include <vector>
 
@@ -1549,3 +1551,247 @@ int cm_eval_freepath(cm_context* ctx, int msm, int n, const double* in, double* 
 }
 
 }  // extern "C"
+
+// ================================================================== allocation-free run
+// cm_run_noalloc: the transport run of cm_run_device for callers that cannot
+// allocate device memory when they run trajectories -- a service whose device
+// memory is owned and budgeted by another allocator (a caching pool, a fixed
+// reservation made at start-up), where a cudaMalloc would be refused, would
+// break that allocator's accounting or would stall the device.  Its scratch
+// (wave records, secondary pool, event queues, counters, per-pixel tables)
+// lives in one file-scope device array of fixed size, reserved on every GPU
+// that loads the library for as long as the process lives.  The caller passes
+// the pixel inputs and the tally outputs, as for cm_run_device.
+namespace cm {
+
+constexpr size_t kNoAllocScratchBytes = (size_t)32 << 20;  // 32 MiB
+constexpr int kNoAllocMaxPix = 65536;
+constexpr int kNoAllocMaxDevices = 64;
+constexpr double kFromSIeVc = 1.0 / 1.60217653e-19;  // FromSI::EV, as kFromSIeV
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+static std::mutex g_noalloc_mu;
+static void* g_noalloc_addr[kNoAllocMaxDevices];  // device address of g_noalloc_scratch, per device
+
+// The per-pixel tables prep_pixels builds on the host, built here on the
+// device from the caller's device arrays: centres in nm, energies in eV, the
+// exclusive prefix of primaries per pixel and the per-pixel stream keys.  One
+// block of 1024 threads.  A bad input sets *bad instead of running.
+__global__ void k_noalloc_pixels(int n, int stride, const double* center_m, const double* energy_j, const int* nprim,
+                                 const int* nbins, const uint64_t* keys, unsigned long long seedmix, double* pc,
+                                 double* pe0, unsigned long long* pkey, unsigned long long* prefix, Counters* c,
+                                 int* bad) {
+  __shared__ unsigned long long part[1024];
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    for (int k = 0; k < 3; ++k) pc[3 * i + k] = center_m[3 * i + k] * 1e9;
+    pe0[i] = energy_j[i] * kFromSIeVc;
+    pkey[i] = keys ? (unsigned long long)keys[i] : mix64(seedmix + (unsigned long long)i);
+    if (!(energy_j[i] > 0) || nprim[i] < 0 || nbins[i] < 1 || nbins[i] + 2 > stride) atomicExch(bad, 1);
+  }
+  const int chunk = (n + (int)blockDim.x - 1) / (int)blockDim.x;
+  const int lo = (int)threadIdx.x * chunk, hi = min(n, lo + chunk);
+  unsigned long long sum = 0;
+  for (int i = lo; i < hi; ++i) sum += (unsigned long long)max(nprim[i], 0);
+  part[threadIdx.x] = sum;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned long long acc = 0;
+    for (int t = 0; t < (int)blockDim.x; ++t) {
+      const unsigned long long x = part[t];
+      part[t] = acc;
+      acc += x;
+    }
+    prefix[n] = acc;
+    c->total_primaries = acc;
+  }
+  __syncthreads();
+  unsigned long long acc = part[threadIdx.x];
+  for (int i = lo; i < hi; ++i) {
+    prefix[i] = acc;
+    acc += (unsigned long long)max(nprim[i], 0);
+  }
+}
+
+// bump allocator over the scratch array; every piece starts on a 256-byte boundary
+struct Carve {
+  unsigned char* base;
+  size_t off = 0;
+  template <typename T> T* take(size_t count) {
+    T* p = (T*)(base + off);
+    off += (count * sizeof(T) + 255) & ~(size_t)255;
+    return p;
+  }
+};
+
+template <typename R> static void carve_wave(Carve& a, Wave<R>& w, int cap) {
+  w.px = a.take<double>(cap);
+  w.py = a.take<double>(cap);
+  w.pz = a.take<double>(cap);
+  w.dx = a.take<R>(cap);
+  w.dy = a.take<R>(cap);
+  w.dz = a.take<R>(cap);
+  w.E = a.take<R>(cap);
+  w.Ep = a.take<R>(cap);
+  w.region = a.take<int>(cap);
+  w.pixel = a.take<int>(cap);
+  w.aux = a.take<int>(cap);
+  w.step = a.take<uint32_t>(cap);
+  w.key = a.take<unsigned long long>(cap);
+  w.hx = a.take<R>(cap);
+  w.hy = a.take<R>(cap);
+  w.hz = a.take<R>(cap);
+}
+
+template <typename R>
+static int run_noalloc(cm_context* ctx, const cm_run_desc* d, uint32_t* back, uint32_t* fwd, cm_run_stats* st,
+                       cudaStream_t s, unsigned char* scratch) {
+  DevScene<R>& ds = scene_of<R>(ctx);
+  if (!ds.valid || ds.host)
+    return fail(CM_ESTATE, "cm_run_noalloc: the scene is not on the device for this precision; uploading it "
+                           "allocates, so make one cm_run, cm_run_device or cm_eval_* call with this precision "
+                           "after the last scene change first");
+  const int n = d->npix;
+  // layout: counters | bad flag | pixel tables | wave 0 | wave 1 | 3 queues | secondary pool (8 W)
+  Carve a{scratch};
+  Counters* c = a.take<Counters>(1);
+  int* bad = a.take<int>(1);
+  double* pc = a.take<double>(3 * (size_t)n);
+  double* pe0 = a.take<double>(n);
+  unsigned long long* pkey = a.take<unsigned long long>(n);
+  unsigned long long* prefix = a.take<unsigned long long>((size_t)n + 1);
+  // bytes per electron record: position (3 double), direction, pre-step
+  // direction (3 R each), E and Ep (R), region, pixel, aux, step (4 B each), key (8 B)
+  const size_t rec = 3 * 8 + 8 * sizeof(R) + 4 * 4 + 8;
+  const size_t pad = (3 * 16 + 3) * 256;  // worst-case rounding of the 51 pieces below
+  const size_t left = kNoAllocScratchBytes - a.off;
+  long long W = (long long)((left > pad ? left - pad : 0) / (10 * rec + 3 * 4));
+  if (d->wave > 0 && d->wave < W) W = d->wave;
+  if (W < 1024) return fail(CM_EINVAL, "cm_run_noalloc: no room for a wave of 1024 electrons");
+  const int poolCap = (int)(8 * W);
+  RunView<R> v;
+#ifdef CM_TRACE
+  v.trace = nullptr;
+  v.ntrace = nullptr;
+  v.tracecap = 0;
+#endif
+  v.s = ds.view;
+  v.s.chamber = d->chamber;
+  carve_wave(a, v.w[0], (int)W);
+  carve_wave(a, v.w[1], (int)W);
+  for (int k = 0; k < 3; ++k) v.q[k] = a.take<int>(W);
+  carve_wave(a, v.pool, poolCap);
+  if (a.off > kNoAllocScratchBytes) return fail(CM_EINVAL, "cm_run_noalloc: scratch layout does not fit");
+  v.c = c;
+  v.W = (int)W;
+  v.poolCap = poolCap;
+  v.pc = pc;
+  v.pe0 = pe0;
+  v.pe0ref = pe0;  // BackscatterStats: FromSI::eV(beam energy), the same value
+  v.pnbins = d->pixel_nbins;
+  v.prefix = prefix;
+  v.pkey = pkey;
+  v.npix = n;
+  v.width = d->beam_width * 1e9;  // m -> nm
+  v.back = back;
+  v.fwd = fwd;
+  v.stride = d->hist_stride;
+  // the array keeps the previous call's contents: the counters, the bad-input
+  // flag and the caller's tallies start at zero; waves, queues and pool are
+  // only read below the counts, so they need no clearing
+  const size_t hbytes = (size_t)n * d->hist_stride * sizeof(uint32_t);
+  CM_CUDA(cudaMemsetAsync(c, 0, sizeof(Counters), s));
+  CM_CUDA(cudaMemsetAsync(bad, 0, sizeof(int), s));
+  CM_CUDA(cudaMemsetAsync(back, 0, hbytes, s));
+  CM_CUDA(cudaMemsetAsync(fwd, 0, hbytes, s));
+  k_noalloc_pixels<<<1, 1024, 0, s>>>(n, d->hist_stride, d->pixel_center, d->pixel_energy, d->pixel_nprim,
+                                      d->pixel_nbins, d->pixel_key, mix64(d->seed ^ 0x243F6A8885A308D3ULL), pc, pe0,
+                                      pkey, prefix, c, bad);
+  CM_CUDA(cudaGetLastError());
+  int hbad = 0;
+  CM_CUDA(cudaMemcpyAsync(&hbad, bad, sizeof(int), cudaMemcpyDeviceToHost, s));
+  CM_CUDA(cudaStreamSynchronize(s));
+  if (hbad)
+    return fail(CM_EINVAL, "cm_run_noalloc: a pixel has a non-positive energy, a negative primary count or "
+                           "pixel_nbins out of range");
+  const int grid = ctx->nsm * 8;
+  const int maxIt = d->max_iterations > 0 ? d->max_iterations : 500000;
+  Counters hc;
+  memset(&hc, 0, sizeof(hc));
+  const auto t0 = std::chrono::steady_clock::now();
+  int it = 0, status = 0;
+  for (;;) {
+    for (int k = 0; k < 16; ++k, ++it) {
+      const int cur = it & 1;
+      k_flight<R><<<grid, 256, 0, s>>>(v, cur);
+      k_elastic<R><<<grid, 256, 0, s>>>(v, cur);
+      k_inelastic<R><<<grid, 256, 0, s>>>(v, cur);
+      k_misc<R><<<grid, 256, 0, s>>>(v, cur);
+      k_spawn<R><<<grid, 256, 0, s>>>(v, cur);
+      k_tail<R><<<1, 32, 0, s>>>(v, cur);
+    }
+    CM_CUDA(cudaGetLastError());
+    CM_CUDA(cudaMemcpyAsync(&hc, c, sizeof(Counters), cudaMemcpyDeviceToHost, s));
+    CM_CUDA(cudaStreamSynchronize(s));
+    if (hc.error) {
+      status = fail(CM_EOVERFLOW, "cm_run_noalloc: the secondary pool in the fixed scratch overflowed; pass "
+                                  "fewer primaries per call or use cm_run_device");
+      break;
+    }
+    if (hc.done) break;
+    if (it >= maxIt) {
+      status = fail(CM_ELIMIT, "cm_run_noalloc: iteration limit reached");
+      break;
+    }
+  }
+  const double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  if (st) {
+    memset(st, 0, sizeof(*st));
+    st->primaries = (int64_t)hc.next_primary;
+    st->steps = (int64_t)hc.steps;
+    st->scatter_events = (int64_t)hc.scatters;
+    st->barrier_events = (int64_t)hc.barriers;
+    st->escapes = (int64_t)hc.escapes;
+    st->secondaries = (int64_t)hc.secondaries;
+    st->iterations = (int64_t)hc.iterations;
+    st->device_ms = ms;
+    for (int k = 0; k < 6; ++k) st->kernel_launches[k] = it;
+    for (int k = 0; k < 4; ++k) st->units[k] = (int64_t)hc.units[k];
+  }
+  return status;
+}
+
+}  // namespace cm
+
+extern "C" int cm_run_noalloc(cm_context* ctx, const cm_run_desc* d, uint32_t* back, uint32_t* fwd,
+                              cm_run_stats* stats, void* stream) {
+  using namespace cm;
+  int rc = check_desc(ctx, d);
+  if (rc) return rc;
+  if (!d->pixel_center || !d->pixel_energy || !d->pixel_nprim || !d->pixel_nbins || !back || !fwd)
+    return fail(CM_EINVAL, "null array");
+  if (d->npix > kNoAllocMaxPix)
+    return fail(CM_EINVAL, "cm_run_noalloc: npix " + std::to_string(d->npix) + " exceeds its maximum of " +
+                               std::to_string(kNoAllocMaxPix));
+  if (ctx->device < 0 || ctx->device >= kNoAllocMaxDevices)
+    return fail(CM_EINVAL, "cm_run_noalloc: device index beyond " + std::to_string(kNoAllocMaxDevices));
+  CM_CUDA(cudaSetDevice(ctx->device));
+  void* scratch;
+  {
+    // set-up on the first call on each device, with that device current: the
+    // host-side name of the array is only a stand-in, the runtime gives its
+    // device address
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_addr[ctx->device]) {
+      void* ptr = nullptr;
+      const cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+      if (e != cudaSuccess || !ptr)
+        return fail(CM_ECUDA, std::string("cudaGetSymbolAddress(g_noalloc_scratch): ") + cudaGetErrorString(e));
+      g_noalloc_addr[ctx->device] = ptr;
+    }
+    scratch = g_noalloc_addr[ctx->device];
+  }
+  cudaStream_t s = (cudaStream_t)stream;
+  return d->precision == CM_PREC_FP64 ? run_noalloc<double>(ctx, d, back, fwd, stats, s, (unsigned char*)scratch)
+                                      : run_noalloc<float>(ctx, d, back, fwd, stats, s, (unsigned char*)scratch);
+}

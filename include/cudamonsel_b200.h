@@ -145,6 +145,26 @@ int cm_run(cm_context* ctx, const cm_run_desc* desc, uint32_t* back, uint32_t* f
 /* Same with inputs (pixel arrays) and outputs (back, fwd) already in device memory. */
 int cm_run_device(cm_context* ctx, const cm_run_desc* desc_device_arrays, uint32_t* back_device, uint32_t* fwd_device,
                   cm_run_stats* stats, void* stream);
+/* No counterpart in the reference.  cm_run_device for callers that cannot
+ * allocate device memory while they run: a service whose device memory belongs
+ * to another allocator (a caching pool, a reservation fixed at start-up), where
+ * a cudaMalloc would fail or upset that allocator's accounting.  This call
+ * allocates nothing: its scratch is one fixed 32 MiB device array that the
+ * library holds on every GPU that loads it until the process exits.  Same
+ * arguments, same tallies as cm_run_device (stream 0 = the legacy default
+ * stream; stats->kernel_ms stays zero).  Limits: npix <= 65536; the wave is
+ * capped by the scratch (about 41 k electrons in FP32, 29 k in FP64), so a run
+ * whose secondaries overflow the fixed pool returns CM_EOVERFLOW instead of
+ * growing it.  The scene must already be on the device for desc->precision
+ * (uploading it allocates): after the last scene change, make one cm_run,
+ * cm_run_device or cm_eval_* call with that precision first, else CM_ESTATE.
+ * The first call on a device looks up the array's device address; make that
+ * first call before any stream capture.  Every call, from any context on the
+ * device, shares the one array and clears what must start at zero (counters,
+ * tallies); calls whose work overlaps on the GPU race on it and must be
+ * ordered by the caller. */
+int cm_run_noalloc(cm_context* ctx, const cm_run_desc* desc_device_arrays, uint32_t* back_device,
+                   uint32_t* fwd_device, cm_run_stats* stats, void* stream);
 
 /* ---- per-function entry points (parity checks; host arrays, SI units) -------
  * Deviates are injected from u arrays so that each result can be compared
