@@ -168,6 +168,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-run", action="store_true",
+                    help="run one FP32 step of the workload and exit (the case for ncu captures)")
     a = ap.parse_args()
     a.warmup = max(a.warmup, 3) if a.impl == "ours" else a.warmup
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -210,6 +212,12 @@ def main():
         return eng.run_device(desc(prec, profile), t_back.data_ptr(), t_fwd.data_ptr(), stream.cuda_stream)
 
     prec = capi.PREC_FP32
+    if a.profile_run:
+        st = step(prec)
+        torch.cuda.synchronize()
+        print("profile run: %d primaries, %d electron-steps, %d iterations" % (st.primaries, st.steps, st.iterations))
+        eng.close()
+        return 0
     for _ in range(a.warmup):
         step(prec)
     torch.cuda.synchronize()

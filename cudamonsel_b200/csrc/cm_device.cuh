@@ -25,6 +25,14 @@ CM_D uint32_t umulhi32(uint32_t a, uint32_t b) {
 #endif
 }
 
+CM_D int popcount64(unsigned long long x) {
+#ifdef __CUDA_ARCH__
+  return __popcll(x);
+#else
+  return __builtin_popcountll(x);
+#endif
+}
+
 // ------------------------------------------------------------ counter-based RNG
 // Philox-4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11), keyed per electron.
 struct U4 { uint32_t x, y, z, w; };
@@ -443,27 +451,42 @@ template <> CM_D float nieminen_loss(float kE, float x) { return kE * expm1f(-(2
 template <typename R> CM_D R jln_compute(const Jln& c, R len, R kE) {
   if ((c.nce == 0) || (kE < (R)c.minE) || (kE <= R(0))) return 0;
   if (kE <= (R)c.breakE) return nieminen_loss(kE, R(1.5) * (R)c.gamma * len * kE * msqrt(kE));
-  // pending segments are len / 2^depth; keep only their depths
-  unsigned char stack[48];
-  int sp = 0;
-  stack[sp++] = 0;
+  // The reference halves the step recursively while the loss exceeds 10 % of
+  // the energy (JoyLuoNieminenCSD.cu:101-121).  The segments form a binary tree
+  // visited depth first, left half first; node (depth, idx) covers
+  // len / 2^depth.  Walking it with the index alone needs no stack: after a
+  // leaf, climb while idx is a right child, then step to the right sibling.
+  // Halves still pending = depth - popcount(idx), bounded like a 46-deep stack.
   R total = 0;
-  while (sp > 0) {
-    const int depth = stack[--sp];
+  int depth = 0;
+  unsigned long long idx = 0;
+  for (;;) {
     R l = len;
     for (int k = 0; k < depth; ++k) l = l / 2;
     const R e = kE + total;
-    if ((e < (R)c.minE) || (e <= R(0))) continue;
-    if (e <= (R)c.breakE) {
+    bool leaf = true;
+    if ((e < (R)c.minE) || (e <= R(0))) {
+    } else if (e <= (R)c.breakE) {
       total += nieminen_loss(e, R(1.5) * (R)c.gamma * l * e * msqrt(e));
+    } else {
+      R loss = 0;
+      for (int i = 0; i < c.nce; i++) loss += (R)c.coef[i] * mlog(((R)c.recipJ[i] * e) + (R)c.beta[i]);
+      loss *= l / e;
+      const int pending = depth - popcount64(idx);
+      if (loss <= (R(0.1) * e) || pending >= 46 || depth >= 62) total += -loss;
+      else leaf = false;
+    }
+    if (!leaf) {  // descend into the first half
+      ++depth;
+      idx <<= 1;
       continue;
     }
-    R loss = 0;
-    for (int i = 0; i < c.nce; i++) loss += (R)c.coef[i] * mlog(((R)c.recipJ[i] * e) + (R)c.beta[i]);
-    loss *= l / e;
-    if (loss <= (R(0.1) * e) || sp >= 46 || depth >= 120) { total += -loss; continue; }
-    stack[sp++] = (unsigned char)(depth + 1);  // second half, processed after the first
-    stack[sp++] = (unsigned char)(depth + 1);  // first half
+    while (depth > 0 && (idx & 1ULL)) {
+      idx >>= 1;
+      --depth;
+    }
+    if (depth == 0) break;
+    idx |= 1ULL;  // the second half of the same parent
   }
   return total;
 }
@@ -596,9 +619,23 @@ CM_D double sphere_first_intersection(const Shape& sh, const double* p0, const d
   return INFINITY;
 }
 
-template <typename R> CM_D bool shape_contains(const SceneView<R>& s, int id, const double* p) {
+// a leaf shape (plane set or sphere) holds p
+template <typename R> CM_D bool leaf_contains(const SceneView<R>& s, const Shape& sh, const double* p) {
+  if (sh.kind == SHAPE_PLANES) {
+    for (int i = 0; i < sh.np; ++i)
+      if (!plane_contains(s.planes[sh.plane0 + i], p)) return false;
+    return true;
+  }
+  return sphere_contains(sh, p);
+}
+
+// D bounds the intersection nesting of the scene's shapes; D = 0: leaf shapes
+// only (intersections of plane sets merged into one plane set when the scene
+// was built), so no tree walk is needed
+template <typename R, int D = kMaxShapeDepth> CM_D bool shape_contains(const SceneView<R>& s, int id, const double* p) {
+  if (D == 0) return leaf_contains(s, s.shapes[id], p);
   // shapes form a binary tree of intersections over plane sets; walk it with a small stack
-  int stack[2 * kMaxShapeDepth + 2];
+  int stack[2 * D + 2];
   int sp = 0;
   stack[sp++] = id;
   while (sp > 0) {
@@ -616,8 +653,13 @@ template <typename R> CM_D bool shape_contains(const SceneView<R>& s, int id, co
   return true;
 }
 
-template <typename R> CM_D bool shape_contains2(const SceneView<R>& s, int id, const double* p0, const double* p1) {
-  int stack[2 * kMaxShapeDepth + 2];
+template <typename R, int D = kMaxShapeDepth>
+CM_D bool shape_contains2(const SceneView<R>& s, int id, const double* p0, const double* p1) {
+  if (D == 0) {
+    const Shape& sh = s.shapes[id];
+    return sh.kind == SHAPE_PLANES ? planes_contains2(s.planes + sh.plane0, sh.np, p0, p1) : sphere_contains(sh, p0);
+  }
+  int stack[2 * D + 2];
   int sp = 0;
   stack[sp++] = id;
   while (sp > 0) {
@@ -726,19 +768,20 @@ template <typename R> struct FirstNormal<R, 0> {
   }
 };
 
-template <typename R> CM_D NV shape_first_normal(const SceneView<R>& s, int id, const double* p0, const double* p1) {
-  return FirstNormal<R, kMaxShapeDepth>::eval(s, id, p0, p1);
+template <typename R, int D = kMaxShapeDepth>
+CM_D NV shape_first_normal(const SceneView<R>& s, int id, const double* p0, const double* p1) {
+  return FirstNormal<R, D>::eval(s, id, p0, p1);
 }
 
 // RegionBase.cu:50-60, iterative: the first child whose shape holds p owns it
-template <typename R> CM_D int containing_subregion(const SceneView<R>& s, int reg, const double* p) {
-  if (!shape_contains(s, s.regions[reg].shape, p)) return -1;
+template <typename R, int D = kMaxShapeDepth> CM_D int containing_subregion(const SceneView<R>& s, int reg, const double* p) {
+  if (!shape_contains<R, D>(s, s.regions[reg].shape, p)) return -1;
   for (int depth = 0; depth < 64; ++depth) {
     const Region& r = s.regions[reg];
     int found = -1;
     for (int i = 0; i < r.nchild; ++i) {
       const int c = s.children[r.child0 + i];
-      if (shape_contains(s, s.regions[c].shape, p)) { found = c; break; }
+      if (shape_contains<R, D>(s, s.regions[c].shape, p)) { found = c; break; }
     }
     if (found < 0) return reg;
     reg = found;
@@ -758,16 +801,17 @@ template <typename R> CM_D bool is_containing_region(const SceneView<R>& s, int 
 
 // RegionBase.cu:74-119.  p1 is clipped to the boundary; returns the region just
 // over it (-1: outside the chamber) and the struck boundary's normal.
-template <typename R> CM_D int find_end_of_step(const SceneView<R>& s, int reg, const double* p0, double* p1, double* hitn) {
+template <typename R, int D = kMaxShapeDepth>
+CM_D int find_end_of_step(const SceneView<R>& s, int reg, const double* p0, double* p1, double* hitn) {
   const Region& r = s.regions[reg];
   int base = reg;
-  NV nv = shape_first_normal(s, r.shape, p0, p1);
+  NV nv = shape_first_normal<R, D>(s, r.shape, p0, p1);
   double t = nv.u;
   hitn[0] = nv.n[0]; hitn[1] = nv.n[1]; hitn[2] = nv.n[2];
   if ((t <= 1.0) && r.parent >= 0) base = r.parent;
   for (int i = 0; i < r.nchild; ++i) {
     const int c = s.children[r.child0 + i];
-    NV cn = shape_first_normal(s, s.regions[c].shape, p0, p1);
+    NV cn = shape_first_normal<R, D>(s, s.regions[c].shape, p0, p1);
     if ((cn.u <= 1.0) && (cn.u < t)) {
       t = cn.u;
       base = c;
@@ -783,7 +827,7 @@ template <typename R> CM_D int find_end_of_step(const SceneView<R>& s, int reg, 
     const double over[3] = {p1[0] + kSmallDispNm * (delta[0] / mag), p1[1] + kSmallDispNm * (delta[1] / mag),
                             p1[2] + kSmallDispNm * (delta[2] / mag)};
     for (int depth = 0; depth < 64 && base >= 0; ++depth) {
-      const int res = containing_subregion(s, base, over);
+      const int res = containing_subregion<R, D>(s, base, over);
       if (res >= 0) return res;
       base = s.regions[base].parent;
     }

@@ -408,6 +408,47 @@ static int build_scene(cm_context* ctx, DevScene<R>& ds) {
     }
     shapes.push_back(s);
   }
+  // The batched (FP32) form merges every intersection of plane sets into one
+  // plane set: an intersection of convex polytopes is the polytope bounded by
+  // all their planes, so the first crossing and its normal are the same up to
+  // rounding (and up to the reference's corner average when two children are
+  // struck at exactly the same u), and the kernels need no tree walk.  The
+  // plain (FP64) form keeps NormalIntersectionShape's march as written.
+  if (sizeof(R) == 4 && !(ctx->options & CM_OPT_EXACT_CSG)) {
+    for (size_t i = 0; i < shapes.size(); ++i) {
+      if (shapes[i].kind != SHAPE_INTERSECTION) continue;
+      std::vector<int> todo{(int)i}, leaves;
+      while (!todo.empty()) {  // leaves in depth-first order, child a before child b
+        const int id = todo.back();
+        todo.pop_back();
+        const HShape& hs = ctx->shapes[id];
+        if (hs.kind == SHAPE_INTERSECTION) {
+          todo.push_back(hs.b);
+          todo.push_back(hs.a);
+        } else {
+          leaves.push_back(id);
+        }
+      }
+      bool planar = true;
+      for (int l : leaves) planar = planar && shapes[l].kind == SHAPE_PLANES;
+      if (!planar) continue;
+      const int plane0 = (int)planes.size();
+      for (int l : leaves)
+        for (int k = 0; k < shapes[l].np; ++k) {
+          const Plane pl = planes[shapes[l].plane0 + k];
+          planes.push_back(pl);
+        }
+      shapes[i].kind = SHAPE_PLANES;
+      shapes[i].plane0 = plane0;
+      shapes[i].np = (int)planes.size() - plane0;
+    }
+  }
+  std::vector<int> sdepth(shapes.size(), 0);  // children come before their parents
+  int depth = 0;
+  for (size_t i = 0; i < shapes.size(); ++i) {
+    if (shapes[i].kind == SHAPE_INTERSECTION) sdepth[i] = 1 + std::max(sdepth[shapes[i].a], sdepth[shapes[i].b]);
+    depth = std::max(depth, sdepth[i]);
+  }
   std::vector<Region> regions;
   std::vector<int> children;
   for (auto& hr : ctx->regions) {
@@ -431,6 +472,7 @@ static int build_scene(cm_context* ctx, DevScene<R>& ds) {
     return rc;
   v.chamber = 0;
   v.options = ctx->options;
+  v.depth = depth;
   v.dl50 = log(0.050 * kToSIkeV * kFromSIeV);
   v.param = (log(20.0 * kToSIkeV) - log(0.050 * kToSIkeV)) / 60.0;
   v.maxMott = 20.0 * kToSIkeV * kFromSIeV;
@@ -486,12 +528,13 @@ __device__ __forceinline__ void flush_counts(Counters* c, StepCounts& sc) {
   }
 }
 
-template <typename R>
+template <typename R, int D>
 __global__ void __launch_bounds__(256) k_flight(RunView<R> v, int cur) {
   DeviceSink sink;
   StepCounts sc;
   const int n = v.c->n[cur];
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) flight_one(v, cur, i, sink, sc);
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    flight_one<R, D>(v, cur, i, sink, sc);
   flush_counts(v.c, sc);
 }
 
@@ -511,13 +554,27 @@ __global__ void __launch_bounds__(256) k_inelastic(RunView<R> v, int cur) {
   flush_counts(v.c, sc);
 }
 
-template <typename R>
+template <typename R, int D>
 __global__ void __launch_bounds__(256) k_misc(RunView<R> v, int cur) {
   DeviceSink sink;
   StepCounts sc;
   const int n = v.c->q[Q_MISC];
-  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) misc_one(v, cur, j, sink, sc);
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x)
+    misc_one<R, D>(v, cur, j, sink, sc);
   flush_counts(v.c, sc);
+}
+
+// the kernels are compiled for the intersection nestings 0 (leaf shapes only), 2 and 4
+template <typename R> static void launch_flight(const RunView<R>& v, int cur, int grid, cudaStream_t s) {
+  if (v.s.depth == 0) k_flight<R, 0><<<grid, 256, 0, s>>>(v, cur);
+  else if (v.s.depth <= 2) k_flight<R, 2><<<grid, 256, 0, s>>>(v, cur);
+  else k_flight<R, kMaxShapeDepth><<<grid, 256, 0, s>>>(v, cur);
+}
+
+template <typename R> static void launch_misc(const RunView<R>& v, int cur, int grid, cudaStream_t s) {
+  if (v.s.depth == 0) k_misc<R, 0><<<grid, 256, 0, s>>>(v, cur);
+  else if (v.s.depth <= 2) k_misc<R, 2><<<grid, 256, 0, s>>>(v, cur);
+  else k_misc<R, kMaxShapeDepth><<<grid, 256, 0, s>>>(v, cur);
 }
 
 template <typename R>
@@ -646,13 +703,13 @@ static int run_device_once(cm_context* ctx, const cm_run_desc* d, uint32_t* back
   for (int it = 0; it < 2 * K; ++it) {
     const int cur = it & 1;
     cudaEvent_t* ev = d->profile ? &pev[(size_t)it * 6 + 1] : nullptr;
-    k_flight<R><<<grid, 256, 0, stream>>>(v, cur);
+    launch_flight<R>(v, cur, grid, stream);
     if (ev) cudaEventRecordWithFlags(ev[0], stream, cudaEventRecordExternal);
     k_elastic<R><<<grid, 256, 0, stream>>>(v, cur);
     if (ev) cudaEventRecordWithFlags(ev[1], stream, cudaEventRecordExternal);
     k_inelastic<R><<<grid, 256, 0, stream>>>(v, cur);
     if (ev) cudaEventRecordWithFlags(ev[2], stream, cudaEventRecordExternal);
-    k_misc<R><<<grid, 256, 0, stream>>>(v, cur);
+    launch_misc<R>(v, cur, grid, stream);
     if (ev) cudaEventRecordWithFlags(ev[3], stream, cudaEventRecordExternal);
     k_spawn<R><<<grid, 256, 0, stream>>>(v, cur);
     if (ev) cudaEventRecordWithFlags(ev[4], stream, cudaEventRecordExternal);
@@ -1723,10 +1780,10 @@ static int run_noalloc(cm_context* ctx, const cm_run_desc* d, uint32_t* back, ui
   for (;;) {
     for (int k = 0; k < 16; ++k, ++it) {
       const int cur = it & 1;
-      k_flight<R><<<grid, 256, 0, s>>>(v, cur);
+      launch_flight<R>(v, cur, grid, s);
       k_elastic<R><<<grid, 256, 0, s>>>(v, cur);
       k_inelastic<R><<<grid, 256, 0, s>>>(v, cur);
-      k_misc<R><<<grid, 256, 0, s>>>(v, cur);
+      launch_misc<R>(v, cur, grid, s);
       k_spawn<R><<<grid, 256, 0, s>>>(v, cur);
       k_tail<R><<<1, 32, 0, s>>>(v, cur);
     }

@@ -116,7 +116,8 @@ struct SceneView {
   const Table* tables;
   const R* blob;             // table data in compute precision
   int chamber;
-  int options;               // bit 0: JMONSEL fixes
+  int options;               // bit 0: JMONSEL fixes, bit 1: exact CSG in FP32
+  int depth;                 // deepest intersection nesting; 0 = every shape is a leaf (plane set or sphere)
   double dl50, param;        // NISTMott log-energy grid (eV)
   double maxMott;            // NISTMottRS MAX_NISTMOTT in eV
 };

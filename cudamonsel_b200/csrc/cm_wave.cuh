@@ -156,12 +156,13 @@ template <typename R, typename Sink> CM_D void cm_trace(const RunView<R>& v, con
 // region check, MONSEL_MaterialScatterModel::randomMeanPathLength, the
 // candidate point, RegionBase::findEndOfStep, the slowing-down loss, the
 // tracking cut; the step's end is queued for its event kernel, escapes are tallied.
-template <typename R, typename Sink> CM_D void flight_one(const RunView<R>& v, int cur, int i, Sink& sink, StepCounts& sc) {
+template <typename R, int D, typename Sink>
+CM_D void flight_one(const RunView<R>& v, int cur, int i, Sink& sink, StepCounts& sc) {
   const SceneView<R>& s = v.s;
   const Wave<R>& W = v.w[cur];
   El<R> e = load(W, i);
   int reg = e.region;
-  if (reg < 0 || !shape_contains(s, s.regions[reg].shape, e.p)) reg = containing_subregion(s, s.chamber, e.p);
+  if (reg < 0 || !shape_contains<R, D>(s, s.regions[reg].shape, e.p)) reg = containing_subregion<R, D>(s, s.chamber, e.p);
   if (reg < 0) return;
   const Msm& m = s.msms[s.regions[reg].msm];
   Rng<R> g(e.key, e.step, 0);
@@ -182,7 +183,7 @@ template <typename R, typename Sink> CM_D void flight_one(const RunView<R>& v, i
   }
   double p1[3] = {e.p[0] + fp * (double)e.d[0], e.p[1] + fp * (double)e.d[1], e.p[2] + fp * (double)e.d[2]};
   double hn[3];
-  const int next = find_end_of_step(s, reg, e.p, p1, hn);
+  const int next = find_end_of_step<R, D>(s, reg, e.p, p1, hn);
   const double dd = sqrt((p1[0] - e.p[0]) * (p1[0] - e.p[0]) + (p1[1] - e.p[1]) * (p1[1] - e.p[1]) +
                          (p1[2] - e.p[2]) * (p1[2] - e.p[2]));
   const R dE = m.csd ? jln_compute(m.jln, (R)dd, e.E) : R(0);
@@ -286,7 +287,8 @@ template <typename R, typename Sink> CM_D void inelastic_one(const RunView<R>& v
 }
 
 // barrier crossings, FittedInelSM, phonon, and steps that end without a mechanism
-template <typename R, typename Sink> CM_D void misc_one(const RunView<R>& v, int cur, int j, Sink& sink, StepCounts& sc) {
+template <typename R, int D, typename Sink>
+CM_D void misc_one(const RunView<R>& v, int cur, int j, Sink& sink, StepCounts& sc) {
   const SceneView<R>& s = v.s;
   El<R> e = load(v.w[cur], v.q[Q_MISC][j]);
   const Msm& m = s.msms[s.regions[e.region].msm];
@@ -299,7 +301,7 @@ template <typename R, typename Sink> CM_D void misc_one(const RunView<R>& v, int
     e.p[0] += kSmallDispNm * (double)e.d[0];
     e.p[1] += kSmallDispNm * (double)e.d[1];
     e.p[2] += kSmallDispNm * (double)e.d[2];
-    if (!shape_contains(s, s.regions[e.region].shape, e.p)) e.region = containing_subregion(s, s.chamber, e.p);
+    if (!shape_contains<R, D>(s, s.regions[e.region].shape, e.p)) e.region = containing_subregion<R, D>(s, s.chamber, e.p);
     keep(v, cur ^ 1, e, sink);
     return;
   }

@@ -41,6 +41,8 @@ extern "C" {
 #define CM_PREC_FP32 1  /* batched form: float physics, double positions and plane solves */
 
 #define CM_OPT_JMONSEL_FIXES 1 /* refraction at barriers, d3 abscissae; default is the reference as written */
+#define CM_OPT_EXACT_CSG 2     /* FP32 too walks NormalIntersectionShape trees as the reference does; by default
+                                  FP32 merges intersections of plane sets into single plane sets */
 
 typedef struct cm_context cm_context;
 

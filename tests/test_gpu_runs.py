@@ -87,20 +87,35 @@ def test_halfspace_fp32_within_1pct_of_fp64(half):
     assert p > 1e-3
 
 
-def test_lines_fp64_matches_oracle(engine):
-    """PMMA lines on Si, 500 eV, sigma 1 nm: 6 landing points (gap, sidewall foot, sidewall,
-    top) engine FP64 vs the oracle's whole trajectories."""
+LINE_XS = np.array([-60.0, -22.0, -19.0, -12.0, 0.0, 100.0]) * 1e-9
+
+
+@pytest.fixture(scope="module")
+def lines_oracle_runs():
     import pyoracle
     from cudamonsel_b200 import scenes
     sc = scenes.lines()
-    h = scenes.build_engine(sc, engine)
-    xs = np.array([-60.0, -22.0, -19.0, -12.0, 0.0, 100.0]) * 1e-9
-    centers = np.stack([xs, np.zeros(6), np.full(6, -120e-9)], axis=1)
+    centers = np.stack([LINE_XS, np.zeros(6), np.full(6, -120e-9)], axis=1)
+    ob, of, tl = pyoracle.run_scene(sc, centers, 1e-9, scenes.eV(500.0), 2000, 77, 50)
+    return centers, ob
+
+
+@pytest.mark.parametrize("prec,options", [(FP64, 0), (FP32, 0), (FP32, 2)], ids=["fp64", "fp32", "fp32-exact-csg"])
+def test_lines_match_oracle(lines_oracle_runs, prec, options):
+    """PMMA lines on Si, 500 eV, sigma 1 nm: 6 landing points (gap, sidewall foot, sidewall,
+    top), engine vs the oracle's whole trajectories.  FP32 runs with the lines merged into
+    single plane sets (default) and with the reference's intersection march (CM_OPT_EXACT_CSG)."""
+    from cudamonsel_b200 import capi, scenes
+    centers, ob = lines_oracle_runs
+    e = capi.Engine(0)
+    e.set_options(options)
+    sc = scenes.lines()
+    h = scenes.build_engine(sc, e)
     npix_rep = 16
     nprim = 500
-    back, fwd, st = engine.run(h["chamber"], np.repeat(centers, npix_rep, axis=0), scenes.eV(500.0), nprim, 50, 1e-9,
-                               seed=3, precision=FP64)
-    ob, of, tl = pyoracle.run_scene(sc, centers, 1e-9, scenes.eV(500.0), nprim * 4, 77, 50)
+    back, fwd, st = e.run(h["chamber"], np.repeat(centers, npix_rep, axis=0), scenes.eV(500.0), nprim, 50, 1e-9,
+                          seed=3, precision=prec)
+    e.close()
     for i in range(6):
         eb, es = batch_yields(back[i * npix_rep:(i + 1) * npix_rep], nprim, 500.0, 50)
         rb, rs = batch_yields(ob[i:i + 1], nprim * 4, 500.0, 50)
@@ -108,8 +123,8 @@ def test_lines_fp64_matches_oracle(engine):
         se_s = es.std(ddof=1) * np.sqrt(1.0 / npix_rep + 1.0 / 4)
         zb = (eb.mean() - rb[0]) / se_b
         zs = (es.mean() - rs[0]) / se_s
-        print("x=%5.1f nm BSE %.4f/%.4f z=%.2f SE %.4f/%.4f z=%.2f" % (xs[i] * 1e9, eb.mean(), rb[0], zb, es.mean(),
-                                                                    rs[0], zs))
+        print("x=%5.1f nm BSE %.4f/%.4f z=%.2f SE %.4f/%.4f z=%.2f" % (LINE_XS[i] * 1e9, eb.mean(), rb[0], zb,
+                                                                    es.mean(), rs[0], zs))
         assert abs(zb) < 3.5 and abs(zs) < 3.5
 
 
