@@ -458,6 +458,7 @@ static int build_scene(cm_context* ctx, DevScene<R>& ds) {
     r.shape = hr.shape;
     r.child0 = (int)children.size();
     r.nchild = (int)hr.children.size();
+    r.cls = hr.msm < kClasses ? hr.msm : kClasses - 1;
     for (int c : hr.children) children.push_back(c);
     regions.push_back(r);
   }
@@ -533,8 +534,13 @@ __global__ void __launch_bounds__(256) k_flight(RunView<R> v, int cur) {
   DeviceSink sink;
   StepCounts sc;
   const int n = v.c->n[cur];
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-    flight_one<R, D>(v, cur, i, sink, sc);
+  int cnt[kClasses];
+  for (int k = 0; k < kClasses; ++k) cnt[k] = v.c->nc[cur][k];
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    int k = 0, j = i;  // i-th electron over the class segments in order
+    while (k < kClasses - 1 && j >= cnt[k]) j -= cnt[k++];
+    flight_one<R, D>(v, cur, k * v.W + j, sink, sc);
+  }
   flush_counts(v.c, sc);
 }
 
@@ -584,8 +590,9 @@ __global__ void __launch_bounds__(256) k_spawn(RunView<R> v, int cur) {
   refill_plan(v.c, nxt, v.W, v.poolCap, nn, take_se, take_p);
   const int poolTop = v.c->pool < v.poolCap ? v.c->pool : v.poolCap;
   const unsigned long long first = v.c->next_primary;
+  DeviceSink sink;
   for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < take_se + take_p; j += gridDim.x * blockDim.x)
-    spawn_one(v, nxt, j, nn, take_se, poolTop, first);
+    spawn_one(v, nxt, j, take_se, poolTop, first, sink);
 }
 
 template <typename R>
@@ -625,7 +632,7 @@ static int ensure_buffers(cm_context* ctx, int W, int poolCap) {
   if (rb.cap == W && rb.poolCap >= poolCap) return 0;
   rb.release();
   int rc;
-  if ((rc = alloc_wave(rb.allocs, rb.w[0], W)) || (rc = alloc_wave(rb.allocs, rb.w[1], W)) ||
+  if ((rc = alloc_wave(rb.allocs, rb.w[0], kClasses * W)) || (rc = alloc_wave(rb.allocs, rb.w[1], kClasses * W)) ||
       (rc = alloc_wave(rb.allocs, rb.pool, poolCap)))
     return rc;
   for (int k = 0; k < 3; ++k) {
@@ -1709,7 +1716,7 @@ static int run_noalloc(cm_context* ctx, const cm_run_desc* d, uint32_t* back, ui
                            "allocates, so make one cm_run, cm_run_device or cm_eval_* call with this precision "
                            "after the last scene change first");
   const int n = d->npix;
-  // layout: counters | bad flag | pixel tables | wave 0 | wave 1 | 3 queues | secondary pool (8 W)
+  // layout: counters | bad flag | pixel tables | wave 0 | wave 1 (kClasses W each) | 3 queues | pool (8 W)
   Carve a{scratch};
   Counters* c = a.take<Counters>(1);
   int* bad = a.take<int>(1);
@@ -1722,7 +1729,7 @@ static int run_noalloc(cm_context* ctx, const cm_run_desc* d, uint32_t* back, ui
   const size_t rec = 3 * 8 + 8 * sizeof(R) + 4 * 4 + 8;
   const size_t pad = (3 * 16 + 3) * 256;  // worst-case rounding of the 51 pieces below
   const size_t left = kNoAllocScratchBytes - a.off;
-  long long W = (long long)((left > pad ? left - pad : 0) / (10 * rec + 3 * 4));
+  long long W = (long long)((left > pad ? left - pad : 0) / ((2 * kClasses + 8) * rec + 3 * 4));
   if (d->wave > 0 && d->wave < W) W = d->wave;
   if (W < 1024) return fail(CM_EINVAL, "cm_run_noalloc: no room for a wave of 1024 electrons");
   const int poolCap = (int)(8 * W);
@@ -1734,8 +1741,8 @@ static int run_noalloc(cm_context* ctx, const cm_run_desc* d, uint32_t* back, ui
 #endif
   v.s = ds.view;
   v.s.chamber = d->chamber;
-  carve_wave(a, v.w[0], (int)W);
-  carve_wave(a, v.w[1], (int)W);
+  carve_wave(a, v.w[0], kClasses * (int)W);
+  carve_wave(a, v.w[1], kClasses * (int)W);
   for (int k = 0; k < 3; ++k) v.q[k] = a.take<int>(W);
   carve_wave(a, v.pool, poolCap);
   if (a.off > kNoAllocScratchBytes) return fail(CM_EINVAL, "cm_run_noalloc: scratch layout does not fit");

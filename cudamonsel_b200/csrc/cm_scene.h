@@ -37,7 +37,12 @@ struct Plane {
 struct Region {
   int parent, msm, shape;
   int child0, nchild;  // children indices in Scene::children
+  int cls;             // wave segment of electrons in this region (by material model)
 };
+
+// electrons are kept in one wave segment per material class, so that the
+// threads of a warp mostly run the same material's code
+constexpr int kClasses = 4;
 
 // JoyLuoNieminenCSD (JMONSEL/JoyLuoNieminenCSD.cu:42-121) in eV/nm units
 struct Jln {

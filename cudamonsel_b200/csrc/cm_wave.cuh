@@ -23,7 +23,9 @@ struct Wave {
 };
 
 struct Counters {
-  int n[2];
+  int n[2];              // electrons in each wave
+  int nc[2][kClasses];   // of which in each class segment (segment k holds slots [k W, k W + nc))
+  int ns[kClasses];      // electrons the refill appends after the survivors of each segment
   int pool;
   int q[3];
   int error;
@@ -232,10 +234,27 @@ CM_D void flight_one(const RunView<R>& v, int cur, int i, Sink& sink, StepCounts
   v.q[queue][slot] = i;
 }
 
-// append a surviving electron to the next wave
+// append a surviving electron to its class segment of the next wave
 template <typename R, typename Sink> CM_D void keep(const RunView<R>& v, int nxt, const El<R>& e, Sink& sink) {
-  const int slot = sink.append(&v.c->n[nxt]);
-  store(v.w[nxt], slot, e);
+  const int k = v.s.regions[e.region].cls;
+  const int slot = sink.append_q(v.c->nc[nxt], k);
+  store(v.w[nxt], k * v.W + slot, e);
+}
+
+// wave index of the i-th electron of a wave counted over its class segments in order
+CM_D int wave_index(const Counters* c, int cur, int W, int i) {
+  int k = 0;
+  while (k < kClasses - 1 && i >= c->nc[cur][k]) {
+    i -= c->nc[cur][k];
+    ++k;
+  }
+  return k * W + i;
+}
+
+CM_D int survivors(const Counters* c, int nxt) {
+  int n = 0;
+  for (int k = 0; k < kClasses; ++k) n += c->nc[nxt][k];
+  return n;
 }
 
 // push a secondary to the pool when MonteCarloSS::trackSecondaryElectron (:165-174) would track it
@@ -324,7 +343,7 @@ CM_D void misc_one(const RunView<R>& v, int cur, int j, Sink& sink, StepCounts& 
 // only once the pool is empty, and at most W/32 per iteration so that the
 // cascades of one batch of primaries do not all peak together
 CM_D void refill_plan(const Counters* c, int nxt, int W, int poolCap, int& nn, int& take_se, int& take_p) {
-  nn = c->n[nxt];
+  nn = survivors(c, nxt);
   const int room = W - nn > 0 ? W - nn : 0;
   const int pool = c->pool < poolCap ? c->pool : poolCap;  // an overflowed pool holds poolCap valid entries
   take_se = pool < room ? pool : room;
@@ -335,11 +354,15 @@ CM_D void refill_plan(const Counters* c, int nxt, int W, int poolCap, int& nn, i
   take_p = rem < (unsigned long long)left ? (int)rem : left;
 }
 
-// slot nn + j of the next wave: a secondary from the top of the pool or a new primary
-template <typename R> CM_D void spawn_one(const RunView<R>& v, int nxt, int j, int nn, int take_se, int poolTop,
-                                          unsigned long long first) {
+// the j-th electron the refill adds to the next wave: a secondary from the top
+// of the pool or a new primary, appended after the survivors of its segment
+template <typename R, typename Sink>
+CM_D void spawn_one(const RunView<R>& v, int nxt, int j, int take_se, int poolTop, unsigned long long first,
+                    Sink& sink) {
   if (j < take_se) {
-    store(v.w[nxt], nn + j, load(v.pool, poolTop - 1 - j));
+    const El<R> se = load(v.pool, poolTop - 1 - j);
+    const int seg = v.s.regions[se.region].cls;
+    store(v.w[nxt], seg * v.W + v.c->nc[nxt][seg] + sink.append_q(v.c->ns, seg), se);
     return;
   }
   // GaussianBeam::createElectron (NISTMonte/GaussianBeam.cu:52-65) + initializeTrajectory (MonteCarloSS.cu:99-105)
@@ -369,7 +392,8 @@ template <typename R> CM_D void spawn_one(const RunView<R>& v, int nxt, int j, i
   e.aux = 0;
   e.step = 0;
   e.h[0] = e.h[1] = e.h[2] = 0;
-  store(v.w[nxt], nn + j, e);
+  const int seg = e.region >= 0 ? v.s.regions[e.region].cls : 0;
+  store(v.w[nxt], seg * v.W + v.c->nc[nxt][seg] + sink.append_q(v.c->ns, seg), e);
 }
 
 // end of an iteration: counters of the next wave, reset of this one
@@ -386,6 +410,11 @@ CM_D void tail_update(Counters* c, int cur, int W, int poolCap) {
     c->iterations += 1;
   }
   c->n[nxt] = nn + take_se + take_p;
+  for (int k = 0; k < kClasses; ++k) {
+    c->nc[nxt][k] += c->ns[k];
+    c->ns[k] = 0;
+    c->nc[cur][k] = 0;
+  }
   c->pool -= take_se;
   c->next_primary += (unsigned long long)take_p;
   c->n[cur] = 0;
