@@ -22,7 +22,7 @@ EXPORTS = (
     "cm_add_mott_element", "cm_add_table", "cm_add_material", "cm_add_msm", "cm_msm_add_nistmott",
     "cm_msm_add_tabulated", "cm_msm_add_fitted", "cm_msm_add_phonon", "cm_msm_add_polaron", "cm_msm_set_csd_jln",
     "cm_msm_set_min_e", "cm_msm_set_barrier", "cm_shape_sphere", "cm_shape_planes", "cm_shape_intersection",
-    "cm_shape_translate", "cm_shape_line", "cm_region_add", "cm_run", "cm_run_device", "cm_run_noalloc",
+    "cm_shape_union", "cm_shape_cylinder", "cm_shape_translate", "cm_shape_line", "cm_region_add", "cm_run", "cm_run_device", "cm_run_noalloc",
     "cm_eval_nistmott", "cm_eval_table", "cm_eval_tabulated", "cm_eval_elastic", "cm_eval_csd", "cm_eval_phonon",
     "cm_eval_shape", "cm_eval_barrier", "cm_eval_freepath",
 )
@@ -89,7 +89,9 @@ def load(path=LIBPATH):
         "cm_shape_planes": [ctx, C.c_int, d, d, i],
         "cm_shape_intersection": [ctx, C.c_int, C.c_int, i],
         "cm_shape_translate": [ctx, C.c_int, d],
-        "cm_shape_line": [ctx, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double, i],
+        "cm_shape_union": [ctx, C.c_int, C.c_int, i],
+        "cm_shape_cylinder": [ctx, d, d, C.c_double, i],
+        "cm_shape_line": [ctx] + [C.c_double] * 7 + [i],
         "cm_region_add": [ctx, C.c_int, C.c_int, C.c_int, i],
         "cm_run": [ctx, C.POINTER(RunDesc), C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.POINTER(RunStats)],
         "cm_run_device": [ctx, C.POINTER(RunDesc), C.c_void_p, C.c_void_p, C.POINTER(RunStats), C.c_void_p],
@@ -220,8 +222,16 @@ class Engine:
         a, pa = _d(d)
         self._check(self.L.cm_shape_translate(self.h, shape, pa))
 
-    def line(self, topz, width, length, thetal, thetar):
-        return self._out(self.L.cm_shape_line, topz, width, length, thetal, thetar)
+    def union(self, a, b):
+        return self._out(self.L.cm_shape_union, a, b)
+
+    def cylinder(self, end0, end1, radius):
+        a, pa = _d(end0)
+        b, pb = _d(end1)
+        return self._out(self.L.cm_shape_cylinder, pa, pb, radius)
+
+    def line(self, topz, width, length, thetal, thetar, radl=0.0, radr=0.0):
+        return self._out(self.L.cm_shape_line, topz, width, length, thetal, thetar, radl, radr)
 
     def region(self, parent, msm, shape):
         return self._out(self.L.cm_region_add, parent, msm, shape)
@@ -300,7 +310,7 @@ class Engine:
         return self._eval(self.L.cm_eval_phonon, (msm, mech), inp, 6, precision)
 
     def eval_shape(self, shape, p01):
-        return self._eval(self.L.cm_eval_shape, (shape,), p01, 5)
+        return self._eval(self.L.cm_eval_shape, (shape,), p01, 6)
 
     def eval_barrier(self, frm, to, inp, precision=PREC_FP64):
         return self._eval(self.L.cm_eval_barrier, (frm, to), inp, 8, precision)

@@ -619,35 +619,203 @@ CM_D double sphere_first_intersection(const Shape& sh, const double* p0, const d
   return INFINITY;
 }
 
-// a leaf shape (plane set or sphere) holds p
+// CylindricalShape::contains (NISTMonte/CylindricalShape.cu:31-48)
+CM_D bool cylinder_contains(const Shape& sh, const double* p) {
+  const double u = (sh.ax[0] * (p[0] - sh.e0[0]) + sh.ax[1] * (p[1] - sh.e0[1]) + sh.ax[2] * (p[2] - sh.e0[2])) / sh.len2;
+  const double a = p[0] - (sh.e0[0] + u * sh.ax[0]), b = p[1] - (sh.e0[1] + u * sh.ax[1]),
+               c = p[2] - (sh.e0[2] + u * sh.ax[2]);
+  return (u >= 0) && (u <= 1.0) && ((a * a + b * b + c * c) <= sh.rad2);
+}
+
+// NormalCylindricalShape::contains(pos0, pos1) (NormalCylindricalShape.cu:24-98)
+CM_D bool cylinder_contains2(const Shape& sh, const double* pos0, const double* pos1) {
+  const double* na = sh.nax;
+  const double p0c[3] = {pos0[0] - sh.e0[0], pos0[1] - sh.e0[1], pos0[2] - sh.e0[2]};
+  const double p0cdotn = (p0c[0] * na[0]) + (p0c[1] * na[1]) + (p0c[2] * na[2]);
+  const double p0cSquared = (p0c[0] * p0c[0]) + (p0c[1] * p0c[1]) + (p0c[2] * p0c[2]);
+  const double r2 = p0cSquared - (p0cdotn * p0cdotn);
+  const bool on_end0 = (p0cdotn == 0) && (r2 <= sh.rad2);
+  const bool on_end1 = (p0cdotn == sh.len) && (r2 <= sh.rad2);
+  const bool on_cylinder = (r2 == sh.rad2) && (p0cdotn >= 0) && (p0cdotn <= sh.len);
+  const double delta[3] = {pos1[0] - pos0[0], pos1[1] - pos0[1], pos1[2] - pos0[2]};
+  if (on_end0 || on_end1) {
+    const double dd = (delta[0] * na[0]) + (delta[1] * na[1]) + (delta[2] * na[2]);
+    if (dd == 0) {
+      if (na[0] == 0) return na[1] == 0 ? na[2] > 0 : na[1] > 0;
+      return na[0] > 0;
+    }
+    return on_end0 ? dd > 0 : dd < 0;
+  }
+  if (on_cylinder) {
+    const double nv[3] = {p0c[0] - (p0cdotn * na[0]), p0c[1] - (p0cdotn * na[1]), p0c[2] - (p0cdotn * na[2])};
+    return ((nv[0] * delta[0]) + (nv[1] * delta[1]) + (nv[2] * delta[2])) < 0;
+  }
+  return (r2 < sh.rad2) && (p0cdotn > 0) && (p0cdotn < sh.len);
+}
+
+// NormalCylindricalShape::getFirstNormal (NormalCylindricalShape.cu:111-322): the end caps,
+// then the wall's quadratic; the first crossing in (0, 1] with its outward normal
+CM_D NV cylinder_first_normal(const Shape& sh, const double* pos0, const double* pos1) {
+  NV nv = nv_none();
+  const double* na = sh.nax;
+  const double radius2 = sh.rad2, mLen = sh.len, mLen2 = sh.len2;
+  const double p0c[3] = {pos0[0] - sh.e0[0], pos0[1] - sh.e0[1], pos0[2] - sh.e0[2]};
+  const double p0cSquared = (p0c[0] * p0c[0]) + (p0c[1] * p0c[1]) + (p0c[2] * p0c[2]);
+  const double delta[3] = {pos1[0] - pos0[0], pos1[1] - pos0[1], pos1[2] - pos0[2]};
+  const double p0cdotn = (p0c[0] * na[0]) + (p0c[1] * na[1]) + (p0c[2] * na[2]);
+  const double deltadotn = (delta[0] * na[0]) + (delta[1] * na[1]) + (delta[2] * na[2]);
+  const double deltadotnSquared = deltadotn * deltadotn;
+  const double p0cdotdelta = (delta[0] * p0c[0]) + (delta[1] * p0c[1]) + (delta[2] * p0c[2]);
+  const double deltaSquared = (delta[0] * delta[0]) + (delta[1] * delta[1]) + (delta[2] * delta[2]);
+  int which = 0;
+  double u1 = 0., u2 = 0., saved = 0.;
+  if (deltadotn != 0.) {
+    u1 = -p0cdotn / deltadotn;
+    if ((u1 > 0.) && (u1 <= 1.) && ((p0cSquared + (2 * u1 * p0cdotdelta) + (u1 * u1 * deltaSquared)) <= radius2)) {
+      nv.u = u1;
+      which = 1;
+    }
+    u2 = u1 + (mLen / deltadotn);
+    if ((u2 > 0.) && (u2 <= 1.) && (u2 < nv.u) &&
+        (((p0cSquared + (2 * u2 * p0cdotdelta) + (u2 * u2 * deltaSquared) + mLen2) -
+          (2 * mLen * (p0cdotn + (u2 * deltadotn)))) <= radius2)) {
+      nv.u = u2;
+      which = 2;
+    }
+  }
+  if (!(((u1 < 0) && (u2 < 0)) || ((u1 > 1) && (u2 > 1)))) {
+    const double r0Squared = p0cSquared - (p0cdotn * p0cdotn);
+    const double r1Squared = (r0Squared + (2. * (p0cdotdelta - (p0cdotn * deltadotn))) + deltaSquared) - deltadotnSquared;
+    if ((r0Squared > radius2) || (r1Squared > radius2)) {
+      const double a = deltaSquared - deltadotnSquared;
+      const double minusbover2 = (p0cdotn * deltadotn) - p0cdotdelta;
+      double term = (minusbover2 * minusbover2) - (a * (r0Squared - radius2));
+      if (term >= 0) {
+        term = sqrt(term);
+        for (int root = 0; root < 2; ++root) {
+          const double u = (minusbover2 + (root == 0 ? term : -term)) / a;
+          if ((u > 0) && (u <= 1) && (u < nv.u)) {
+            const double projection = p0cdotn + (u * deltadotn);
+            if ((projection >= 0) && (projection <= mLen)) {
+              nv.u = u;
+              which = 3;
+              saved = projection;
+            }
+          }
+        }
+      }
+    }
+  }
+  if (which == 1 || which == 2) {
+    const double sg = which == 1 ? -1.0 : 1.0;
+    nv.n[0] = sg * na[0];
+    nv.n[1] = sg * na[1];
+    nv.n[2] = sg * na[2];
+  } else if (which == 3) {
+    const double v[3] = {(p0c[0] + (nv.u * delta[0])) - (saved * na[0]), (p0c[1] + (nv.u * delta[1])) - (saved * na[1]),
+                         (p0c[2] + (nv.u * delta[2])) - (saved * na[2])};
+    const double mag = sqrt((v[0] * v[0]) + (v[1] * v[1]) + (v[2] * v[2]));
+    nv.n[0] = v[0] / mag;
+    nv.n[1] = v[1] / mag;
+    nv.n[2] = v[2] / mag;
+  }
+  return nv;
+}
+
+// out-of-line copies for the shape-tree walks, which would otherwise inline the
+// cylinder at every level of the tree (the leaf-only kernels inline it)
+__host__ __device__ __noinline__ bool cylinder_contains2_call(const Shape& sh, const double* pos0, const double* pos1) {
+  return cylinder_contains2(sh, pos0, pos1);
+}
+__host__ __device__ __noinline__ NV cylinder_first_normal_call(const Shape& sh, const double* pos0, const double* pos1) {
+  return cylinder_first_normal(sh, pos0, pos1);
+}
+
+// a leaf shape (plane set, sphere or cylinder) holds p
 template <typename R> CM_D bool leaf_contains(const SceneView<R>& s, const Shape& sh, const double* p) {
   if (sh.kind == SHAPE_PLANES) {
     for (int i = 0; i < sh.np; ++i)
       if (!plane_contains(s.planes[sh.plane0 + i], p)) return false;
     return true;
   }
+  if (sh.kind == SHAPE_CYLINDER) return cylinder_contains(sh, p);
   return sphere_contains(sh, p);
 }
 
-// D bounds the intersection nesting of the scene's shapes; D = 0: leaf shapes
-// only (intersections of plane sets merged into one plane set when the scene
-// was built), so no tree walk is needed
+template <typename R, bool INL = true>
+CM_D bool leaf_contains2(const SceneView<R>& s, const Shape& sh, const double* p0, const double* p1) {
+  if (sh.kind == SHAPE_PLANES) return planes_contains2(s.planes + sh.plane0, sh.np, p0, p1);
+  if (sh.kind == SHAPE_CYLINDER) return INL ? cylinder_contains2(sh, p0, p1) : cylinder_contains2_call(sh, p0, p1);
+  return sphere_contains(sh, p0);
+}
+
+// D bounds the intersection/union nesting of the scene's shapes; D = 0: leaf
+// shapes only (intersections of plane sets merged into one plane set when the
+// scene was built), so no tree walk is compiled in.
+// NormalIntersectionShape::contains = A && B, NormalUnionShape (SumShape) = A || B.
+template <typename R, int D> struct Contains {
+  static __host__ __device__ __noinline__ bool eval(const SceneView<R>& s, int id, const double* p) {
+    const Shape& sh = s.shapes[id];
+    if (sh.kind == SHAPE_INTERSECTION)
+      return Contains<R, D - 1>::eval(s, sh.a, p) && Contains<R, D - 1>::eval(s, sh.b, p);
+    if (sh.kind == SHAPE_UNION) return Contains<R, D - 1>::eval(s, sh.a, p) || Contains<R, D - 1>::eval(s, sh.b, p);
+    return leaf_contains(s, sh, p);
+  }
+  static __host__ __device__ __noinline__ bool eval2(const SceneView<R>& s, int id, const double* p0, const double* p1) {
+    const Shape& sh = s.shapes[id];
+    if (sh.kind == SHAPE_INTERSECTION)
+      return Contains<R, D - 1>::eval2(s, sh.a, p0, p1) && Contains<R, D - 1>::eval2(s, sh.b, p0, p1);
+    if (sh.kind == SHAPE_UNION)
+      return Contains<R, D - 1>::eval2(s, sh.a, p0, p1) || Contains<R, D - 1>::eval2(s, sh.b, p0, p1);
+    return leaf_contains2<R, false>(s, sh, p0, p1);
+  }
+};
+
+template <typename R> struct Contains<R, 0> {
+  static CM_D bool eval(const SceneView<R>& s, int id, const double* p) { return leaf_contains(s, s.shapes[id], p); }
+  static CM_D bool eval2(const SceneView<R>& s, int id, const double* p0, const double* p1) {
+    return leaf_contains2<R, false>(s, s.shapes[id], p0, p1);
+  }
+};
+
+// Leaves are tested inline; a tree of intersections only is the AND of its
+// leaves, walked with a small stack; trees holding a union recurse out of line.
 template <typename R, int D = kMaxShapeDepth> CM_D bool shape_contains(const SceneView<R>& s, int id, const double* p) {
-  if (D == 0) return leaf_contains(s, s.shapes[id], p);
-  // shapes form a binary tree of intersections over plane sets; walk it with a small stack
-  int stack[2 * D + 2];
+  const Shape& top = s.shapes[id];
+  if (D == 0 || (top.kind != SHAPE_INTERSECTION && top.kind != SHAPE_UNION)) return leaf_contains(s, top, p);
+  if (top.anyunion) return Contains<R, D>::eval(s, id, p);
+  int stack[D + 2];
   int sp = 0;
   stack[sp++] = id;
   while (sp > 0) {
     const Shape& sh = s.shapes[stack[--sp]];
-    if (sh.kind == SHAPE_PLANES) {
-      for (int i = 0; i < sh.np; ++i)
-        if (!plane_contains(s.planes[sh.plane0 + i], p)) return false;
-    } else if (sh.kind == SHAPE_INTERSECTION) {
+    if (sh.kind == SHAPE_INTERSECTION) {
+      if (sp + 2 > D + 2) return Contains<R, D>::eval(s, id, p);
       stack[sp++] = sh.b;
       stack[sp++] = sh.a;
-    } else if (sh.kind == SHAPE_SPHERE) {
-      if (!sphere_contains(sh, p)) return false;
+    } else if (!leaf_contains(s, sh, p)) {
+      return false;
+    }
+  }
+  return true;
+}
+
+// NormalShape::contains(p0, p1) inside the tree walks (cylinders out of line)
+template <typename R, int D> CM_D bool tree_contains2(const SceneView<R>& s, int id, const double* p0, const double* p1) {
+  const Shape& top = s.shapes[id];
+  if (D == 0 || (top.kind != SHAPE_INTERSECTION && top.kind != SHAPE_UNION)) return leaf_contains2<R, false>(s, top, p0, p1);
+  if (top.anyunion) return Contains<R, D>::eval2(s, id, p0, p1);
+  int stack[D + 2];
+  int sp = 0;
+  stack[sp++] = id;
+  while (sp > 0) {
+    const Shape& sh = s.shapes[stack[--sp]];
+    if (sh.kind == SHAPE_INTERSECTION) {
+      if (sp + 2 > D + 2) return Contains<R, D>::eval2(s, id, p0, p1);
+      stack[sp++] = sh.b;
+      stack[sp++] = sh.a;
+    } else if (!leaf_contains2<R, false>(s, sh, p0, p1)) {
+      return false;
     }
   }
   return true;
@@ -655,25 +823,8 @@ template <typename R, int D = kMaxShapeDepth> CM_D bool shape_contains(const Sce
 
 template <typename R, int D = kMaxShapeDepth>
 CM_D bool shape_contains2(const SceneView<R>& s, int id, const double* p0, const double* p1) {
-  if (D == 0) {
-    const Shape& sh = s.shapes[id];
-    return sh.kind == SHAPE_PLANES ? planes_contains2(s.planes + sh.plane0, sh.np, p0, p1) : sphere_contains(sh, p0);
-  }
-  int stack[2 * D + 2];
-  int sp = 0;
-  stack[sp++] = id;
-  while (sp > 0) {
-    const Shape& sh = s.shapes[stack[--sp]];
-    if (sh.kind == SHAPE_PLANES) {
-      if (!planes_contains2(s.planes + sh.plane0, sh.np, p0, p1)) return false;
-    } else if (sh.kind == SHAPE_INTERSECTION) {
-      stack[sp++] = sh.b;
-      stack[sp++] = sh.a;
-    } else if (sh.kind == SHAPE_SPHERE) {
-      if (!sphere_contains(sh, p0)) return false;
-    }
-  }
-  return true;
+  if (D == 0) return leaf_contains2<R, true>(s, s.shapes[id], p0, p1);
+  return tree_contains2<R, D>(s, id, p0, p1);
 }
 
 template <typename R, int D> struct FirstNormal;
@@ -688,13 +839,13 @@ template <typename R, int D> __host__ __device__ __noinline__ NV inter_first_nor
   NV nva = FirstNormal<R, D - 1>::eval(s, sh.a, pos0, pos1);
   if (nva.u <= 1.) adepth = ((delta[0] * nva.n[0]) + (delta[1] * nva.n[1]) + (delta[2] * nva.n[2])) > 0 ? 1 : 0;
   else {
-    if (!shape_contains2(s, sh.a, pos0, pos1)) return none;
+    if (!tree_contains2<R, D - 1>(s, sh.a, pos0, pos1)) return none;
     adepth = 1;
   }
   NV nvb = FirstNormal<R, D - 1>::eval(s, sh.b, pos0, pos1);
   if (nvb.u <= 1.) bdepth = ((delta[0] * nvb.n[0]) + (delta[1] * nvb.n[1]) + (delta[2] * nvb.n[2])) > 0 ? 1 : 0;
   else {
-    if (!shape_contains2(s, sh.b, pos0, pos1)) return none;
+    if (!tree_contains2<R, D - 1>(s, sh.b, pos0, pos1)) return none;
     if (adepth == 1) return nva;
     bdepth = 1;
   }
@@ -747,29 +898,103 @@ template <typename R, int D> __host__ __device__ __noinline__ NV inter_first_nor
   return none;
 }
 
+// NormalUnionShape.cu:40-269: the crossings of A and B in order along the step,
+// tracking the depth (number of shapes the point is inside); a crossing where the
+// union's depth changes to or from 0 is the union's boundary
+template <typename R, int D> __host__ __device__ __noinline__ NV union_first_normal(const SceneView<R>& s, const Shape& sh,
+                                                                           const double* pos0, const double* pos1) {
+  const NV none = nv_none();
+  int adepth, bdepth;
+  double u;
+  const double delta[3] = {pos1[0] - pos0[0], pos1[1] - pos0[1], pos1[2] - pos0[2]};
+  NV nva = FirstNormal<R, D - 1>::eval(s, sh.a, pos0, pos1);
+  if (nva.u <= 1.) adepth = ((delta[0] * nva.n[0]) + (delta[1] * nva.n[1]) + (delta[2] * nva.n[2])) > 0 ? 1 : 0;
+  else {
+    if (tree_contains2<R, D - 1>(s, sh.a, pos0, pos1)) return none;
+    adepth = 0;
+  }
+  NV nvb = FirstNormal<R, D - 1>::eval(s, sh.b, pos0, pos1);
+  if (nvb.u <= 1.) bdepth = ((delta[0] * nvb.n[0]) + (delta[1] * nvb.n[1]) + (delta[2] * nvb.n[2])) > 0 ? 1 : 0;
+  else {
+    if (tree_contains2<R, D - 1>(s, sh.b, pos0, pos1)) return none;
+    return nva;
+  }
+  int cdepth = adepth + bdepth;
+  const double EXTRAU = 1.e-10;
+  for (int guard = 0; guard < 4096; ++guard) {
+    if (nva.u < nvb.u) {
+      if (adepth == cdepth) return nva;
+      cdepth = cdepth == 1 ? 2 : 1;
+      u = nva.u + EXTRAU;
+      const double tmp[3] = {pos0[0] + (u * delta[0]), pos0[1] + (u * delta[1]), pos0[2] + (u * delta[2])};
+      nva = FirstNormal<R, D - 1>::eval(s, sh.a, tmp, pos1);
+      if (nva.u < INFINITY) nva.u = (nva.u * (1. - u)) + u;
+      if (nva.u > 1) return cdepth == bdepth ? nvb : none;
+      adepth ^= 1;
+    } else if (nva.u > nvb.u) {
+      if (bdepth == cdepth) return nvb;
+      cdepth = cdepth == 1 ? 2 : 1;
+      u = nvb.u + EXTRAU;
+      const double tmp[3] = {pos0[0] + (u * delta[0]), pos0[1] + (u * delta[1]), pos0[2] + (u * delta[2])};
+      nvb = FirstNormal<R, D - 1>::eval(s, sh.b, tmp, pos1);
+      if (nvb.u < INFINITY) nvb.u = (nvb.u * (1. - u)) + u;
+      if (nvb.u > 1) return cdepth == adepth ? nva : none;
+      bdepth ^= 1;
+    } else {
+      const int depthchange = (((adepth ^ 1) - adepth) + (bdepth ^ 1)) - bdepth;
+      if (depthchange == 0) {
+        u = nva.u + EXTRAU;
+        const double t1[3] = {pos0[0] + (u * delta[0]), pos0[1] + (u * delta[1]), pos0[2] + (u * delta[2])};
+        nva = FirstNormal<R, D - 1>::eval(s, sh.a, t1, pos1);
+        if (nva.u < INFINITY) nva.u = (nva.u * (1. - u)) + u;
+        u = nvb.u + EXTRAU;
+        const double t2[3] = {pos0[0] + (u * delta[0]), pos0[1] + (u * delta[1]), pos0[2] + (u * delta[2])};
+        nvb = FirstNormal<R, D - 1>::eval(s, sh.b, t2, pos1);
+        if (nvb.u < INFINITY) nvb.u = (nvb.u * (1. - u)) + u;
+        if (nva.u > 1) return cdepth != bdepth ? nvb : none;
+        if (nvb.u > 1) return cdepth != adepth ? nva : none;
+        adepth ^= 1;
+        bdepth ^= 1;
+      } else {
+        NV r;
+        r.n[0] = (nva.n[0] + nvb.n[0]) / 2.;
+        r.n[1] = (nva.n[1] + nvb.n[1]) / 2.;
+        r.n[2] = (nva.n[2] + nvb.n[2]) / 2.;
+        r.u = nva.u;
+        return r;
+      }
+    }
+  }
+  return none;
+}
+
+template <typename R, bool INL = true>
+CM_D NV leaf_first_normal(const SceneView<R>& s, const Shape& sh, const double* p0, const double* p1) {
+  if (sh.kind == SHAPE_PLANES) return planes_first_normal(s.planes + sh.plane0, sh.np, p0, p1);
+  if (sh.kind == SHAPE_CYLINDER) return INL ? cylinder_first_normal(sh, p0, p1) : cylinder_first_normal_call(sh, p0, p1);
+  NV r = nv_none();
+  if (sh.kind == SHAPE_SPHERE) r.u = sphere_first_intersection(sh, p0, p1);
+  return r;
+}
+
 template <typename R, int D> struct FirstNormal {
   static CM_D NV eval(const SceneView<R>& s, int id, const double* p0, const double* p1) {
     const Shape& sh = s.shapes[id];
-    if (sh.kind == SHAPE_PLANES) return planes_first_normal(s.planes + sh.plane0, sh.np, p0, p1);
     if (sh.kind == SHAPE_INTERSECTION) return inter_first_normal<R, D>(s, sh, p0, p1);
-    NV r = nv_none();
-    if (sh.kind == SHAPE_SPHERE) r.u = sphere_first_intersection(sh, p0, p1);
-    return r;
+    if (sh.kind == SHAPE_UNION) return union_first_normal<R, D>(s, sh, p0, p1);
+    return leaf_first_normal<R, false>(s, sh, p0, p1);
   }
 };
 
 template <typename R> struct FirstNormal<R, 0> {
   static CM_D NV eval(const SceneView<R>& s, int id, const double* p0, const double* p1) {
-    const Shape& sh = s.shapes[id];
-    if (sh.kind == SHAPE_PLANES) return planes_first_normal(s.planes + sh.plane0, sh.np, p0, p1);
-    NV r = nv_none();
-    if (sh.kind == SHAPE_SPHERE) r.u = sphere_first_intersection(sh, p0, p1);
-    return r;
+    return leaf_first_normal<R, false>(s, s.shapes[id], p0, p1);
   }
 };
 
 template <typename R, int D = kMaxShapeDepth>
 CM_D NV shape_first_normal(const SceneView<R>& s, int id, const double* p0, const double* p1) {
+  if (D == 0) return leaf_first_normal<R, true>(s, s.shapes[id], p0, p1);
   return FirstNormal<R, D>::eval(s, id, p0, p1);
 }
 

@@ -104,6 +104,7 @@ struct HShape {
   double c[3], r;
   std::vector<double> n, p;  // planes
   int a, b;
+  double e0[3], ax[3], nax[3], radius;  // cylinder (SI); nax as NormalCylindricalShape computed it
 };
 
 struct HRegion {
@@ -394,6 +395,16 @@ static int build_scene(cm_context* ctx, DevScene<R>& ds) {
     s.b = hs.b;
     for (int k = 0; k < 3; ++k) s.c[k] = hs.c[k] * 1e9;
     s.r = hs.r * 1e9;
+    if (hs.kind == SHAPE_CYLINDER) {
+      for (int k = 0; k < 3; ++k) {
+        s.e0[k] = hs.e0[k] * 1e9;
+        s.ax[k] = hs.ax[k] * 1e9;
+        s.nax[k] = hs.nax[k];
+      }
+      s.rad2 = (hs.radius * 1e9) * (hs.radius * 1e9);
+      s.len2 = (s.ax[0] * s.ax[0]) + (s.ax[1] * s.ax[1]) + (s.ax[2] * s.ax[2]);
+      s.len = sqrt(s.len2);
+    }
     if (hs.kind == SHAPE_PLANES) {
       s.plane0 = (int)planes.size();
       s.np = (int)hs.n.size() / 3;
@@ -446,7 +457,12 @@ static int build_scene(cm_context* ctx, DevScene<R>& ds) {
   std::vector<int> sdepth(shapes.size(), 0);  // children come before their parents
   int depth = 0;
   for (size_t i = 0; i < shapes.size(); ++i) {
-    if (shapes[i].kind == SHAPE_INTERSECTION) sdepth[i] = 1 + std::max(sdepth[shapes[i].a], sdepth[shapes[i].b]);
+    Shape& sh = shapes[i];
+    sh.anyunion = sh.kind == SHAPE_UNION;
+    if (sh.kind == SHAPE_INTERSECTION || sh.kind == SHAPE_UNION) {
+      sdepth[i] = 1 + std::max(sdepth[sh.a], sdepth[sh.b]);
+      sh.anyunion = sh.anyunion || shapes[sh.a].anyunion || shapes[sh.b].anyunion;
+    }
     depth = std::max(depth, sdepth[i]);
   }
   std::vector<Region> regions;
@@ -583,7 +599,7 @@ template <typename R> static void launch_misc(const RunView<R>& v, int cur, int 
   else k_misc<R, kMaxShapeDepth><<<grid, 256, 0, s>>>(v, cur);
 }
 
-template <typename R>
+template <typename R, int D>
 __global__ void __launch_bounds__(256) k_spawn(RunView<R> v, int cur) {
   const int nxt = cur ^ 1;
   int nn, take_se, take_p;
@@ -592,7 +608,13 @@ __global__ void __launch_bounds__(256) k_spawn(RunView<R> v, int cur) {
   const unsigned long long first = v.c->next_primary;
   DeviceSink sink;
   for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < take_se + take_p; j += gridDim.x * blockDim.x)
-    spawn_one(v, nxt, j, take_se, poolTop, first, sink);
+    spawn_one<R, D>(v, nxt, j, take_se, poolTop, first, sink);
+}
+
+template <typename R> static void launch_spawn(const RunView<R>& v, int cur, int grid, cudaStream_t s) {
+  if (v.s.depth == 0) k_spawn<R, 0><<<grid, 256, 0, s>>>(v, cur);
+  else if (v.s.depth <= 2) k_spawn<R, 2><<<grid, 256, 0, s>>>(v, cur);
+  else k_spawn<R, kMaxShapeDepth><<<grid, 256, 0, s>>>(v, cur);
 }
 
 template <typename R>
@@ -718,7 +740,7 @@ static int run_device_once(cm_context* ctx, const cm_run_desc* d, uint32_t* back
     if (ev) cudaEventRecordWithFlags(ev[2], stream, cudaEventRecordExternal);
     launch_misc<R>(v, cur, grid, stream);
     if (ev) cudaEventRecordWithFlags(ev[3], stream, cudaEventRecordExternal);
-    k_spawn<R><<<grid, 256, 0, stream>>>(v, cur);
+    launch_spawn<R>(v, cur, grid, stream);
     if (ev) cudaEventRecordWithFlags(ev[4], stream, cudaEventRecordExternal);
     k_tail<R><<<1, 32, 0, stream>>>(v, cur);
     if (ev) cudaEventRecordWithFlags(ev[5], stream, cudaEventRecordExternal);
@@ -924,11 +946,12 @@ __global__ void k_eval_shape(SceneView<double> s, int shape, int n, const double
   const double p0[3] = {p01[6 * i] * 1e9, p01[6 * i + 1] * 1e9, p01[6 * i + 2] * 1e9};
   const double p1[3] = {p01[6 * i + 3] * 1e9, p01[6 * i + 4] * 1e9, p01[6 * i + 5] * 1e9};
   NV r = shape_first_normal(s, shape, p0, p1);
-  out[5 * i] = r.n[0];
-  out[5 * i + 1] = r.n[1];
-  out[5 * i + 2] = r.n[2];
-  out[5 * i + 3] = r.u;
-  out[5 * i + 4] = shape_contains(s, shape, p0) ? 1. : 0.;
+  out[6 * i] = r.n[0];
+  out[6 * i + 1] = r.n[1];
+  out[6 * i + 2] = r.n[2];
+  out[6 * i + 3] = r.u;
+  out[6 * i + 4] = shape_contains(s, shape, p0) ? 1. : 0.;
+  out[6 * i + 5] = shape_contains2(s, shape, p0, p1) ? 1. : 0.;
 }
 
 template <typename R> __global__ void k_eval_barrier(SceneView<R> s, int from, int to, int n, const double* in, double* out) {
@@ -1225,8 +1248,58 @@ int cm_shape_planes(cm_context* ctx, int n, const double* normals, const double*
 
 static int shape_depth(cm_context* ctx, int id) {
   const HShape& s = ctx->shapes[id];
-  if (s.kind != SHAPE_INTERSECTION) return 0;
+  if (s.kind != SHAPE_INTERSECTION && s.kind != SHAPE_UNION) return 0;
   return 1 + std::max(shape_depth(ctx, s.a), shape_depth(ctx, s.b));
+}
+
+// NormalCylindricalShape(end0, end1, radius) (JMONSEL/NormalCylindricalShape.cu:8-17).
+// Its members are initialised in declaration order (NormalCylindricalShape.cuh:29-35),
+// so the reference divides the axis by a length it has not set yet (read as 0):
+// the normalised axis is infinite (NaN where a component is 0) and the cylinder is
+// never struck by getFirstNormal nor holds a step by contains(p0, p1).  That is
+// reproduced unless CM_OPT_JMONSEL_FIXES is set when the cylinder is created.
+int cm_shape_cylinder(cm_context* ctx, const double end0[3], const double end1[3], double radius, int* out) {
+  if (!ctx || !end0 || !end1 || !out || !(radius > 0)) return fail(CM_EINVAL, "bad cylinder");
+  HShape s;
+  s.kind = SHAPE_CYLINDER;
+  s.a = s.b = -1;
+  s.r = 0;
+  s.c[0] = s.c[1] = s.c[2] = 0;
+  for (int k = 0; k < 3; ++k) {
+    s.e0[k] = end0[k];
+    s.ax[k] = end1[k] - end0[k];
+  }
+  const double len2 = (s.ax[0] * s.ax[0]) + (s.ax[1] * s.ax[1]) + (s.ax[2] * s.ax[2]);
+  if (!(len2 > 0)) return fail(CM_EINVAL, "cylinder of zero length");
+  const double len = (ctx->options & CM_OPT_JMONSEL_FIXES) ? sqrt(len2) : 0.0;
+  for (int k = 0; k < 3; ++k) s.nax[k] = s.ax[k] / len;
+  s.radius = radius;
+  *out = (int)ctx->shapes.size();
+  ctx->shapes.push_back(s);
+  ctx->dirty();
+  return 0;
+}
+
+// NormalUnionShape(a, b) (JMONSEL/NormalUnionShape.cu:8-11)
+int cm_shape_union(cm_context* ctx, int a, int b, int* out) {
+  if (!ctx || !out || a < 0 || b < 0 || a >= (int)ctx->shapes.size() || b >= (int)ctx->shapes.size())
+    return fail(CM_EINVAL, "bad shape handle");
+  if (ctx->shapes[a].kind == SHAPE_SPHERE || ctx->shapes[b].kind == SHAPE_SPHERE)
+    return fail(CM_EINVAL, "a Sphere is not a NormalShape");
+  HShape s;
+  s.kind = SHAPE_UNION;
+  s.a = a;
+  s.b = b;
+  s.r = 0;
+  s.c[0] = s.c[1] = s.c[2] = 0;
+  *out = (int)ctx->shapes.size();
+  ctx->shapes.push_back(s);
+  if (shape_depth(ctx, *out) > kMaxShapeDepth) {
+    ctx->shapes.pop_back();
+    return fail(CM_EINVAL, "shape nesting deeper than 4");
+  }
+  ctx->dirty();
+  return 0;
 }
 
 int cm_shape_intersection(cm_context* ctx, int a, int b, int* out) {
@@ -1244,7 +1317,7 @@ int cm_shape_intersection(cm_context* ctx, int a, int b, int* out) {
   ctx->shapes.push_back(s);
   if (shape_depth(ctx, *out) > kMaxShapeDepth) {
     ctx->shapes.pop_back();
-    return fail(CM_EINVAL, "intersection nesting deeper than 4");
+    return fail(CM_EINVAL, "shape nesting deeper than 4");
   }
   ctx->dirty();
   return 0;
@@ -1254,9 +1327,11 @@ static void translate_rec(cm_context* ctx, int id, const double* d) {
   HShape& s = ctx->shapes[id];
   if (s.kind == SHAPE_PLANES) {
     for (size_t i = 0; i < s.p.size(); ++i) s.p[i] += d[i % 3];  // Plane::translate (MultiPlaneShape.cu:59-64)
-  } else if (s.kind == SHAPE_INTERSECTION) {
+  } else if (s.kind == SHAPE_INTERSECTION || s.kind == SHAPE_UNION) {
     translate_rec(ctx, s.a, d);
     translate_rec(ctx, s.b, d);
+  } else if (s.kind == SHAPE_CYLINDER) {
+    for (int k = 0; k < 3; ++k) s.e0[k] += d[k];  // NormalCylindricalShape.cu:321-328
   } else {
     for (int k = 0; k < 3; ++k) s.c[k] += d[k];
   }
@@ -1269,20 +1344,59 @@ int cm_shape_translate(cm_context* ctx, int shape, const double d[3]) {
   return 0;
 }
 
-int cm_shape_line(cm_context* ctx, double topz, double width, double length, double thetal, double thetar, int* out) {
+// NShapes::createLine (JMONSEL/NShapes.cu:55-149).  A corner radius turns a
+// sidewall into the union of the sidewall (plus a clipping plane) and a cylinder
+// along y; the reference builds the left union from the RIGHT sidewall's plane
+// set (NShapes.cu:140), reproduced unless CM_OPT_JMONSEL_FIXES is set.
+int cm_shape_line(cm_context* ctx, double topz, double width, double length, double thetal, double thetar,
+                  double radl, double radr, int* out) {
   if (!ctx || !out) return fail(CM_EINVAL, "null argument");
-  // NShapes::createLine (JMONSEL/NShapes.cu:55-149) with zero corner radii
+  if (radr < 0.) radr = 0.;
+  if (radl < 0.) radl = 0.;
   double signz = !topz ? 0 : (topz > 0 ? 1 : -1);
   if (signz == 0.) signz = 1.;
   const double en[12] = {0., 0., signz, 0., 0., -signz, 0., 1., 0., 0., -1., 0.};
   const double ep[12] = {0., 0., topz, 0., 0., 0., 0., length / 2., 0., 0., -length / 2., 0.};
-  int enclosure, right, left, nts, rc;
+  const double root2 = sqrt(2.), absz = signz * topz;
+  int enclosure, rightNMPS, leftNMPS, rightSide, leftSide, nts, cyl, rc;
   if ((rc = cm_shape_planes(ctx, 4, en, ep, &enclosure))) return rc;
-  const double rn[3] = {cos(thetar), 0., signz * sin(thetar)}, rp[3] = {width / 2, 0., 0.};
-  if ((rc = cm_shape_planes(ctx, 1, rn, rp, &right))) return rc;
-  const double ln[3] = {-cos(thetal), 0., signz * sin(thetal)}, lp[3] = {-width / 2, 0., 0.};
-  if ((rc = cm_shape_planes(ctx, 1, ln, lp, &left))) return rc;
-  if ((rc = cm_shape_intersection(ctx, left, right, &nts))) return rc;
+  const double costhetar = cos(thetar), sinthetar = sin(thetar);
+  double rn[6] = {costhetar, 0., signz * sinthetar, 0, 0, 0}, rp[6] = {width / 2, 0., 0., 0, 0, 0};
+  if (radr > 0) {
+    const double rad = sqrt(1 - sinthetar);
+    rn[3] = rad / root2;
+    rn[5] = (signz * costhetar) / root2 / rad;
+    rp[3] = ((width / 2.) - (radr / costhetar)) + (((radr - absz) * sinthetar) / costhetar);
+    rp[5] = topz;
+  }
+  if ((rc = cm_shape_planes(ctx, radr > 0 ? 2 : 1, rn, rp, &rightNMPS))) return rc;
+  rightSide = rightNMPS;
+  if (radr > 0) {
+    const double xc = ((width / 2.) - (radr / cos(thetar))) + ((radr - absz) * tan(thetar));
+    const double zc = topz - (signz * radr);
+    const double e0[3] = {xc, -length / 2., zc}, e1[3] = {xc, length / 2., zc};
+    if ((rc = cm_shape_cylinder(ctx, e0, e1, radr, &cyl)) || (rc = cm_shape_union(ctx, rightNMPS, cyl, &rightSide)))
+      return rc;
+  }
+  const double costhetal = cos(thetal), sinthetal = sin(thetal);
+  double ln[6] = {-costhetal, 0., signz * sinthetal, 0, 0, 0}, lp[6] = {-width / 2, 0., 0., 0, 0, 0};
+  if (radl > 0.) {
+    const double rad = sqrt(1 - sinthetal);
+    ln[3] = -rad / root2;
+    ln[5] = (signz * costhetal) / root2 / rad;
+    lp[3] = ((-width / 2.) + (radl / costhetal)) - (((radl - absz) * sinthetal) / costhetal);
+    lp[5] = topz;
+  }
+  if ((rc = cm_shape_planes(ctx, radl > 0 ? 2 : 1, ln, lp, &leftNMPS))) return rc;
+  leftSide = leftNMPS;
+  if (radl > 0.) {
+    const double xc = ((width / 2.) - (radl / cos(thetal))) + ((radl - absz) * tan(thetal));
+    const double zc = topz - (signz * radl);
+    const double e0[3] = {-xc, -length / 2., zc}, e1[3] = {-xc, length / 2., zc};
+    const int side = (ctx->options & CM_OPT_JMONSEL_FIXES) ? leftNMPS : rightNMPS;
+    if ((rc = cm_shape_cylinder(ctx, e0, e1, radl, &cyl)) || (rc = cm_shape_union(ctx, side, cyl, &leftSide))) return rc;
+  }
+  if ((rc = cm_shape_intersection(ctx, leftSide, rightSide, &nts))) return rc;
   return cm_shape_intersection(ctx, nts, enclosure, out);
 }
 
@@ -1588,7 +1702,7 @@ int cm_eval_shape(cm_context* ctx, int shape, int n, const double* p01, double* 
   int rc = scene_for(ctx, CM_PREC_FP64);
   if (rc) return rc;
   if (shape < 0 || shape >= (int)ctx->shapes.size()) return fail(CM_EINVAL, "bad shape handle");
-  return eval_launch(ctx, n, p01, 6, out, 5, [&](double* din, double* dout, int g) {
+  return eval_launch(ctx, n, p01, 6, out, 6, [&](double* din, double* dout, int g) {
     k_eval_shape<<<g, 128>>>(ctx->d64.view, shape, n, din, dout);
   });
 }
@@ -1791,7 +1905,7 @@ static int run_noalloc(cm_context* ctx, const cm_run_desc* d, uint32_t* back, ui
       k_elastic<R><<<grid, 256, 0, s>>>(v, cur);
       k_inelastic<R><<<grid, 256, 0, s>>>(v, cur);
       launch_misc<R>(v, cur, grid, s);
-      k_spawn<R><<<grid, 256, 0, s>>>(v, cur);
+      launch_spawn<R>(v, cur, grid, s);
       k_tail<R><<<1, 32, 0, s>>>(v, cur);
     }
     CM_CUDA(cudaGetLastError());

@@ -19,14 +19,18 @@ constexpr double kChamberRadiusNm = 0.1e9;
 constexpr double kSmallDispNm = 1.0e-6;
 constexpr double kPi = 3.14159265358979323846;
 
-enum ShapeKind : int { SHAPE_SPHERE = 1, SHAPE_PLANES = 2, SHAPE_INTERSECTION = 3 };
+enum ShapeKind : int { SHAPE_SPHERE = 1, SHAPE_PLANES = 2, SHAPE_INTERSECTION = 3, SHAPE_CYLINDER = 4, SHAPE_UNION = 5 };
 enum MechKind : int { MECH_NISTMOTT = 1, MECH_TABULATED = 2, MECH_FITTED = 3, MECH_PHONON = 4, MECH_POLARON = 5 };
 
 struct Shape {
   int kind;
-  int a, b;          // intersection children
+  int anyunion;      // a union below (or at) this node
+  int a, b;          // intersection / union children
   int plane0, np;    // planes [plane0, plane0+np)
   double c[3], r;    // sphere (nm)
+  // NormalCylindricalShape (nm): end0, axis = end1 - end0, axis / |axis| as the
+  // reference computed it, radius^2, |axis|^2, |axis|
+  double e0[3], ax[3], nax[3], rad2, len2, len;
 };
 
 struct Plane {

@@ -356,7 +356,7 @@ CM_D void refill_plan(const Counters* c, int nxt, int W, int poolCap, int& nn, i
 
 // the j-th electron the refill adds to the next wave: a secondary from the top
 // of the pool or a new primary, appended after the survivors of its segment
-template <typename R, typename Sink>
+template <typename R, int D, typename Sink>
 CM_D void spawn_one(const RunView<R>& v, int nxt, int j, int take_se, int poolTop, unsigned long long first,
                     Sink& sink) {
   if (j < take_se) {
@@ -387,7 +387,7 @@ CM_D void spawn_one(const RunView<R>& v, int nxt, int j, int take_se, int poolTo
   e.d[0] = 0; e.d[1] = 0; e.d[2] = 1;
   e.E = (R)v.pe0[px];
   e.Ep = e.E;
-  e.region = containing_subregion(v.s, v.s.chamber, e.p);
+  e.region = containing_subregion<R, D>(v.s, v.s.chamber, e.p);
   e.pixel = px;
   e.aux = 0;
   e.step = 0;

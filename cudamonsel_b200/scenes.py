@@ -89,8 +89,14 @@ class SceneSpec:
     def translate(self, shape, d):
         return self._op("translate", shape, list(d))
 
-    def line(self, topz, width, length, thetal, thetar):
-        return self._op("line", topz, width, length, thetal, thetar)
+    def cylinder(self, end0, end1, radius):
+        return self._op("cylinder", list(end0), list(end1), radius)
+
+    def union(self, a, b):
+        return self._op("union", a, b)
+
+    def line(self, topz, width, length, thetal, thetar, radl=0.0, radr=0.0):
+        return self._op("line", topz, width, length, thetal, thetar, radl, radr)
 
     def region(self, parent, msm, shape):
         return self._op("region", -1 if parent is None else parent, msm, shape)
@@ -218,6 +224,41 @@ def lines(nlines=3, pitch=200e-9, height=100e-9, width=40e-9, length=1e-6, angle
         s.translate(ln, [(i - (nlines - 1) / 2.0) * pitch, 0.0, 0.0])
         line_regions.append(s.region(chamber, pm, ln))
     return Scene(s, chamber, vac=vac, si=si, pmma=pm, si_region=sireg, lines=line_regions)
+
+
+def features(options=1, tables=None):
+    """Si substrate carrying a PMMA cylinder lying along y (radius 30 nm, axis at x = -60 nm, z = -30 nm), a
+    rounded PMMA line (NShapes::createLine, corner radii 10 nm, centred at x = +60 nm) and a Si block.
+
+    options = 1 (CM_OPT_JMONSEL_FIXES) builds cylinders whose axis is normalised: the reference as
+    compiled never strikes a cylinder (its normalised axis is computed before the axis length is set)."""
+    s = SceneSpec()
+    s.options = options
+    vac = vacuum(s)
+    si = silicon(s, tables)
+    pm = pmma(s)
+    sphere = s.sphere([0.0, 0.0, 0.0], 0.1)
+    chamber = s.region(None, vac, sphere)
+    surf = s.planes([0.0, 0.0, -1.0], [0.0, 0.0, 0.0])
+    sireg = s.region(chamber, si, surf)
+    cyl = s.cylinder([-60e-9, -500e-9, -30e-9], [-60e-9, 500e-9, -30e-9], 30e-9)
+    creg = s.region(chamber, pm, cyl)
+    th = 5.0 * math.pi / 180.0
+    ln = s.line(-80e-9, 50e-9, 1e-6, th, th, 10e-9, 10e-9)
+    s.translate(ln, [60e-9, 0.0, 0.0])
+    lreg = s.region(chamber, pm, ln)
+    n, p = [], []
+    for a, (c, hw) in enumerate(zip((0.0, 150e-9, -20e-9), (20e-9, 20e-9, 20e-9))):
+        for sg in (-1.0, 1.0):
+            nn = [0.0, 0.0, 0.0]
+            pp = [0.0, 150e-9, -20e-9]
+            nn[a] = sg
+            pp[a] = c + sg * hw
+            n += nn
+            p += pp
+    block = s.planes(n, p)
+    breg = s.region(chamber, si, block)
+    return Scene(s, chamber, vac=vac, si=si, pmma=pm, si_region=sireg, cylinder=creg, line=lreg, block=breg)
 
 
 def build_engine(scene, engine):

@@ -94,9 +94,18 @@ int cm_shape_sphere(cm_context* ctx, const double center[3], double radius, int*
 /* NormalMultiPlaneShape with n planes (normal, point) (JMONSEL/NormalMultiPlaneShape.cu) */
 int cm_shape_planes(cm_context* ctx, int n, const double* normals, const double* points, int* out_shape);
 int cm_shape_intersection(cm_context* ctx, int a, int b, int* out_shape); /* JMONSEL/NormalIntersectionShape.cu */
+/* NormalUnionShape(a, b) (JMONSEL/NormalUnionShape.cu) */
+int cm_shape_union(cm_context* ctx, int a, int b, int* out_shape);
+/* NormalCylindricalShape(end0, end1, radius) (JMONSEL/NormalCylindricalShape.cu).  As compiled, the
+ * reference normalises the axis by a length it has not initialised yet (read as 0), so the cylinder is
+ * never struck by a step; that is reproduced unless CM_OPT_JMONSEL_FIXES is set when it is created. */
+int cm_shape_cylinder(cm_context* ctx, const double end0[3], const double end1[3], double radius, int* out_shape);
 int cm_shape_translate(cm_context* ctx, int shape, const double distance[3]);
-/* NShapes::createLine(topz, width, length, thetal, thetar, 0, 0) (JMONSEL/NShapes.cu:55-149), zero corner radii */
-int cm_shape_line(cm_context* ctx, double topz, double width, double length, double thetal, double thetar, int* out_shape);
+/* NShapes::createLine(topz, width, length, thetal, thetar, radl, radr) (JMONSEL/NShapes.cu:55-149); a corner
+ * radius adds a clipping plane and a cylinder joined by a union.  The reference's left corner uses the right
+ * sidewall (NShapes.cu:140); CM_OPT_JMONSEL_FIXES set when the line is created uses the left one. */
+int cm_shape_line(cm_context* ctx, double topz, double width, double length, double thetal, double thetar, double radl,
+                  double radr, int* out_shape);
 /* Region(parent, msm, shape) (NISTMonte/RegionBase.cu:193-200); parent -1 makes the chamber */
 int cm_region_add(cm_context* ctx, int parent, int msm, int shape, int* out_region);
 
@@ -188,7 +197,8 @@ int cm_eval_csd(cm_context* ctx, int msm, int n, const double* in, double* out, 
 /* GanachaudMokraniPhononInelasticSM (JMONSEL/GanachaudMokraniPhononInelasticSM.cu:19-72);
  * in[5n] = E theta phi u0 u1, out[6n] = rate E' dx dy dz Eprev */
 int cm_eval_phonon(cm_context* ctx, int msm, int mech, int n, const double* in, double* out, int precision);
-/* NormalShape::getFirstNormal + Shape::contains (double precision); p01[6n], out[5n] = nx ny nz u inside */
+/* NormalShape::getFirstNormal, Shape::contains(p0) and NormalShape::contains(p0, p1) (double precision);
+ * p01[6n], out[6n] = nx ny nz u contains(p0) contains(p0,p1) */
 int cm_eval_shape(cm_context* ctx, int shape, int n, const double* p01, double* out);
 /* ExpQMBarrierSM::barrierScatter + the nudge of MonteCarloSS::takeStep
  * (JMONSEL/ExpQMBarrierSM.cu:50-219); in[6n] = E theta phi x y z, out[7n] = E' dx dy dz x y z ... see implementation */

@@ -413,7 +413,7 @@ typedef struct {
    double lambda, lambdaFactor, u0;
 } msm_t;
 
-enum { S_SPHERE = 1, S_PLANES, S_INTERSECTION };
+enum { S_SPHERE = 1, S_PLANES, S_INTERSECTION, S_CYLINDER, S_UNION };
 
 typedef struct {
    int kind;
@@ -421,6 +421,8 @@ typedef struct {
    int np;
    double n[MAXPLANES][3], p[MAXPLANES][3];
    int a, b;
+   /* NormalCylindricalShape: end0, axis = end1 - end0, radius^2, |axis|^2, |axis|, axis / |axis| */
+   double e0[3], ax[3], rad2, len2, len, nax[3];
 } shape_t;
 
 typedef struct {
@@ -739,8 +741,47 @@ int cmo_shape_intersection(cmo_scene* s, int a, int b)
    return s->nshapes++;
 }
 
+/* NormalCylindricalShape(end0, end1, radius) (JMONSEL/NormalCylindricalShape.cu:8-17,
+ * NISTMonte/CylindricalShape.cu:11-20).  The members are initialised in their
+ * declaration order (NormalCylindricalShape.cuh:29-35), so normalizedaxis is
+ * computed from mLen before mLen is set; the compiled reference reads it as 0
+ * and gets an axis of infinities (NaN where the axis component is 0), which
+ * makes getFirstNormal and contains(p0, p1) never see the cylinder (pinned by
+ * the golden vectors).  That is reproduced unless the fixes option is set when
+ * the cylinder is created. */
+int cmo_shape_cylinder(cmo_scene* s, const double end0[3], const double end1[3], double radius)
+{
+   GROW(s->shapes, s->nshapes);
+   shape_t* sh = &s->shapes[s->nshapes];
+   memset(sh, 0, sizeof(*sh));
+   sh->kind = S_CYLINDER;
+   for (int k = 0; k < 3; ++k) {
+      sh->e0[k] = end0[k];
+      sh->ax[k] = end1[k] - end0[k];
+   }
+   sh->rad2 = radius * radius;
+   sh->len2 = (sh->ax[0] * sh->ax[0]) + (sh->ax[1] * sh->ax[1]) + (sh->ax[2] * sh->ax[2]);
+   sh->len = sqrt(sh->len2);
+   const double mlen = (s->options & 1) ? sh->len : 0.0;
+   for (int k = 0; k < 3; ++k) sh->nax[k] = sh->ax[k] / mlen;
+   return s->nshapes++;
+}
+
+/* NormalUnionShape(a, b) (JMONSEL/NormalUnionShape.cu:8-11) */
+int cmo_shape_union(cmo_scene* s, int a, int b)
+{
+   GROW(s->shapes, s->nshapes);
+   shape_t* sh = &s->shapes[s->nshapes];
+   memset(sh, 0, sizeof(*sh));
+   sh->kind = S_UNION;
+   sh->a = a;
+   sh->b = b;
+   return s->nshapes++;
+}
+
 /* Plane::translate (NISTMonte/MultiPlaneShape.cu:59-64) applied to every plane;
- * an intersection translates both children. */
+ * an intersection or union translates both children, a cylinder its end0
+ * (NormalCylindricalShape.cu:321-328). */
 int cmo_shape_translate(cmo_scene* s, int shape, const double d[3])
 {
    shape_t* sh = &s->shapes[shape];
@@ -748,9 +789,12 @@ int cmo_shape_translate(cmo_scene* s, int shape, const double d[3])
       for (int i = 0; i < sh->np; ++i)
          for (int k = 0; k < 3; ++k) sh->p[i][k] += d[k];
    }
-   else if (sh->kind == S_INTERSECTION) {
+   else if (sh->kind == S_INTERSECTION || sh->kind == S_UNION) {
       cmo_shape_translate(s, sh->a, d);
       cmo_shape_translate(s, sh->b, d);
+   }
+   else if (sh->kind == S_CYLINDER) {
+      for (int k = 0; k < 3; ++k) sh->e0[k] += d[k];
    }
    else if (sh->kind == S_SPHERE) {
       for (int k = 0; k < 3; ++k) sh->c[k] += d[k];
@@ -758,21 +802,68 @@ int cmo_shape_translate(cmo_scene* s, int shape, const double d[3])
    return 0;
 }
 
-/* JMONSEL/NShapes.cu:55-149 with zero corner radii */
-int cmo_shape_line(cmo_scene* s, double topz, double width, double length, double thetal, double thetar)
+/* JMONSEL/NShapes.cu:55-149.  With a corner radius the sidewall becomes the
+ * union of the sidewall (plus a clipping plane) and a cylinder along y.  The
+ * reference builds the left union from the RIGHT sidewall's plane set
+ * (NShapes.cu:140); that is reproduced unless the fixes option is set when the
+ * line is created. */
+int cmo_shape_line(cmo_scene* s, double topz, double width, double length, double thetal, double thetar, double radl,
+                   double radr)
 {
+   if (radr < 0.) radr = 0.;
+   if (radl < 0.) radl = 0.;
    double signz = !topz ? 0 : (topz > 0 ? 1 : -1);
    if (signz == 0.) signz = 1.;
    double en[12] = { 0., 0., signz, 0., 0., -signz, 0., 1., 0., 0., -1., 0. };
    double ep[12] = { 0., 0., topz, 0., 0., 0., 0., length / 2., 0., 0., -length / 2., 0. };
    int enclosure = cmo_shape_planes(s, 4, en, ep);
+   const double root2 = sqrt(2.);
+   const double absz = signz * topz;
    double costhetar = cos(thetar), sinthetar = sin(thetar);
-   double rn[3] = { costhetar, 0., signz * sinthetar }, rp[3] = { width / 2, 0., 0. };
-   int right = cmo_shape_planes(s, 1, rn, rp);
+   double rn[6] = { costhetar, 0., signz * sinthetar }, rp[6] = { width / 2, 0., 0. };
+   int nright = 1;
+   if (radr > 0) {
+      double rad = sqrt(1 - sinthetar);
+      rn[3] = rad / root2;
+      rn[4] = 0.;
+      rn[5] = (signz * costhetar) / root2 / rad;
+      rp[3] = ((width / 2.) - (radr / costhetar)) + (((radr - absz) * sinthetar) / costhetar);
+      rp[4] = 0.;
+      rp[5] = topz;
+      nright = 2;
+   }
+   int rightNMPS = cmo_shape_planes(s, nright, rn, rp);
+   int rightSide = rightNMPS;
+   if (radr > 0) {
+      double xc = ((width / 2.) - (radr / cos(thetar))) + ((radr - absz) * tan(thetar));
+      double zc = topz - (signz * radr);
+      double e0[3] = { xc, -length / 2., zc }, e1[3] = { xc, length / 2., zc };
+      int cyl = cmo_shape_cylinder(s, e0, e1, radr);
+      rightSide = cmo_shape_union(s, rightNMPS, cyl);
+   }
    double costhetal = cos(thetal), sinthetal = sin(thetal);
-   double ln[3] = { -costhetal, 0., signz * sinthetal }, lp[3] = { -width / 2, 0., 0. };
-   int left = cmo_shape_planes(s, 1, ln, lp);
-   int nts = cmo_shape_intersection(s, left, right);
+   double ln[6] = { -costhetal, 0., signz * sinthetal }, lp[6] = { -width / 2, 0., 0. };
+   int nleft = 1;
+   if (radl > 0.) {
+      double rad = sqrt(1 - sinthetal);
+      ln[3] = -rad / root2;
+      ln[4] = 0.;
+      ln[5] = (signz * costhetal) / root2 / rad;
+      lp[3] = ((-width / 2.) + (radl / costhetal)) - (((radl - absz) * sinthetal) / costhetal);
+      lp[4] = 0.;
+      lp[5] = topz;
+      nleft = 2;
+   }
+   int leftNMPS = cmo_shape_planes(s, nleft, ln, lp);
+   int leftSide = leftNMPS;
+   if (radl > 0.) {
+      double xc = ((width / 2.) - (radl / cos(thetal))) + ((radl - absz) * tan(thetal));
+      double zc = topz - (signz * radl);
+      double e0[3] = { -xc, -length / 2., zc }, e1[3] = { -xc, length / 2., zc };
+      int cyl = cmo_shape_cylinder(s, e0, e1, radl);
+      leftSide = cmo_shape_union(s, (s->options & 1) ? leftNMPS : rightNMPS, cyl);
+   }
+   int nts = cmo_shape_intersection(s, leftSide, rightSide);
    return cmo_shape_intersection(s, nts, enclosure);
 }
 
@@ -904,8 +995,44 @@ static int shape_contains(const cmo_scene* s, int id, const double* p)
       return 1;
    case S_INTERSECTION:
       return shape_contains(s, sh->a, p) && shape_contains(s, sh->b, p);
+   case S_UNION: /* SumShape::contains (NISTMonte/SumShape.cu:38-44) */
+      return shape_contains(s, sh->a, p) || shape_contains(s, sh->b, p);
+   case S_CYLINDER: { /* CylindricalShape::contains (NISTMonte/CylindricalShape.cu:31-48) */
+      const double u = (sh->ax[0] * (p[0] - sh->e0[0]) + sh->ax[1] * (p[1] - sh->e0[1]) + sh->ax[2] * (p[2] - sh->e0[2])) /
+                       sh->len2;
+      const double a = p[0] - (sh->e0[0] + u * sh->ax[0]), b = p[1] - (sh->e0[1] + u * sh->ax[1]),
+                   c = p[2] - (sh->e0[2] + u * sh->ax[2]);
+      return (u >= 0) && (u <= 1.0) && ((a * a + b * b + c * c) <= sh->rad2);
+   }
    }
    return 0;
+}
+
+/* NormalCylindricalShape::contains(pos0, pos1) (NormalCylindricalShape.cu:24-98) */
+static int cylinder_contains2(const shape_t* sh, const double* pos0, const double* pos1)
+{
+   const double* na = sh->nax;
+   const double p0c[] = { pos0[0] - sh->e0[0], pos0[1] - sh->e0[1], pos0[2] - sh->e0[2] };
+   const double p0cdotn = (p0c[0] * na[0]) + (p0c[1] * na[1]) + (p0c[2] * na[2]);
+   const double p0cSquared = (p0c[0] * p0c[0]) + (p0c[1] * p0c[1]) + (p0c[2] * p0c[2]);
+   const double r2 = p0cSquared - (p0cdotn * p0cdotn);
+   const int on_end0 = (p0cdotn == 0) && (r2 <= sh->rad2);
+   const int on_end1 = (p0cdotn == sh->len) && (r2 <= sh->rad2);
+   const int on_cylinder = (r2 == sh->rad2) && (p0cdotn >= 0) && (p0cdotn <= sh->len);
+   const double delta[] = { pos1[0] - pos0[0], pos1[1] - pos0[1], pos1[2] - pos0[2] };
+   if (on_end0 || on_end1) {
+      const double dd = (delta[0] * na[0]) + (delta[1] * na[1]) + (delta[2] * na[2]);
+      if (dd == 0) {
+         if (na[0] == 0) return na[1] == 0 ? na[2] > 0 : na[1] > 0;
+         return na[0] > 0;
+      }
+      return on_end0 ? dd > 0 : dd < 0;
+   }
+   if (on_cylinder) {
+      const double nv[] = { p0c[0] - (p0cdotn * na[0]), p0c[1] - (p0cdotn * na[1]), p0c[2] - (p0cdotn * na[2]) };
+      return ((nv[0] * delta[0]) + (nv[1] * delta[1]) + (nv[2] * delta[2])) < 0;
+   }
+   return (r2 < sh->rad2) && (p0cdotn > 0) && (p0cdotn < sh->len);
 }
 
 static int shape_contains2(const cmo_scene* s, int id, const double* p0, const double* p1)
@@ -913,6 +1040,8 @@ static int shape_contains2(const cmo_scene* s, int id, const double* p0, const d
    const shape_t* sh = &s->shapes[id];
    if (sh->kind == S_PLANES) return planes_contains2(sh, p0, p1);
    if (sh->kind == S_INTERSECTION) return shape_contains2(s, sh->a, p0, p1) && shape_contains2(s, sh->b, p0, p1);
+   if (sh->kind == S_UNION) return shape_contains2(s, sh->a, p0, p1) || shape_contains2(s, sh->b, p0, p1);
+   if (sh->kind == S_CYLINDER) return cylinder_contains2(sh, p0, p1);
    return shape_contains(s, id, p0);
 }
 
@@ -998,6 +1127,161 @@ static nvec inter_first_normal(const cmo_scene* s, const shape_t* sh, const doub
    return nointersection;
 }
 
+/* NormalUnionShape.cu:40-269: the crossings of A and B in order along the step,
+ * tracking the depth (number of shapes the point is inside); a crossing where the
+ * union's depth changes to or from 0 is the union's boundary. */
+static nvec union_first_normal(const cmo_scene* s, const shape_t* sh, const double* pos0, const double* pos1)
+{
+   nvec nointersection = { { 0., 0., 0., INFINITY } };
+   int adepth, bdepth;
+   double u;
+   const double delta[] = { pos1[0] - pos0[0], pos1[1] - pos0[1], pos1[2] - pos0[2] };
+   nvec nva = shape_first_normal(s, sh->a, pos0, pos1);
+   if (nva.v[3] <= 1.) adepth = ((delta[0] * nva.v[0]) + (delta[1] * nva.v[1]) + (delta[2] * nva.v[2])) > 0 ? 1 : 0;
+   else {
+      if (shape_contains2(s, sh->a, pos0, pos1)) return nointersection;
+      adepth = 0;
+   }
+   nvec nvb = shape_first_normal(s, sh->b, pos0, pos1);
+   if (nvb.v[3] <= 1.) bdepth = ((delta[0] * nvb.v[0]) + (delta[1] * nvb.v[1]) + (delta[2] * nvb.v[2])) > 0 ? 1 : 0;
+   else {
+      if (shape_contains2(s, sh->b, pos0, pos1)) return nointersection;
+      return nva;
+   }
+   int cdepth = adepth + bdepth;
+   const double EXTRAU = 1.e-10;
+   for (int guard = 0; guard < 100000; ++guard) {
+      if (nva.v[3] < nvb.v[3]) {
+         if (adepth == cdepth) return nva;
+         cdepth = (cdepth == 1 ? 2 : 1);
+         u = nva.v[3] + EXTRAU;
+         double tmp[] = { pos0[0] + (u * delta[0]), pos0[1] + (u * delta[1]), pos0[2] + (u * delta[2]) };
+         nva = shape_first_normal(s, sh->a, tmp, pos1);
+         if (nva.v[3] < INFINITY) nva.v[3] = (nva.v[3] * (1. - u)) + u;
+         if (nva.v[3] > 1) return cdepth == bdepth ? nvb : nointersection;
+         adepth = adepth ^ 1;
+      }
+      else if (nva.v[3] > nvb.v[3]) {
+         if (bdepth == cdepth) return nvb;
+         cdepth = (cdepth == 1 ? 2 : 1);
+         u = nvb.v[3] + EXTRAU;
+         double tmp[] = { pos0[0] + (u * delta[0]), pos0[1] + (u * delta[1]), pos0[2] + (u * delta[2]) };
+         nvb = shape_first_normal(s, sh->b, tmp, pos1);
+         if (nvb.v[3] < INFINITY) nvb.v[3] = (nvb.v[3] * (1. - u)) + u;
+         if (nvb.v[3] > 1) return cdepth == adepth ? nva : nointersection;
+         bdepth = bdepth ^ 1;
+      }
+      else {
+         int depthchange = (((adepth ^ 1) - adepth) + (bdepth ^ 1)) - bdepth;
+         if (depthchange == 0) {
+            u = nva.v[3] + EXTRAU;
+            double tmp0[] = { pos0[0] + (u * delta[0]), pos0[1] + (u * delta[1]), pos0[2] + (u * delta[2]) };
+            nva = shape_first_normal(s, sh->a, tmp0, pos1);
+            if (nva.v[3] < INFINITY) nva.v[3] = (nva.v[3] * (1. - u)) + u;
+            u = nvb.v[3] + EXTRAU;
+            double tmp1[] = { pos0[0] + (u * delta[0]), pos0[1] + (u * delta[1]), pos0[2] + (u * delta[2]) };
+            nvb = shape_first_normal(s, sh->b, tmp1, pos1);
+            if (nvb.v[3] < INFINITY) nvb.v[3] = (nvb.v[3] * (1. - u)) + u;
+            if (nva.v[3] > 1) return cdepth != bdepth ? nvb : nointersection;
+            if (nvb.v[3] > 1) return cdepth != adepth ? nva : nointersection;
+            adepth = adepth ^ 1;
+            bdepth = bdepth ^ 1;
+         }
+         else {
+            nvec r = { { (nva.v[0] + nvb.v[0]) / 2., (nva.v[1] + nvb.v[1]) / 2., (nva.v[2] + nvb.v[2]) / 2., nva.v[3] } };
+            return r;
+         }
+      }
+   }
+   return nointersection;
+}
+
+/* NormalCylindricalShape::getFirstNormal (NormalCylindricalShape.cu:111-322) */
+static nvec cylinder_first_normal(const shape_t* sh, const double* pos0, const double* pos1)
+{
+   nvec nv = { { 0., 0., 0., INFINITY } };
+   const double* na = sh->nax;
+   const double radius2 = sh->rad2, mLen = sh->len, mLen2 = sh->len2;
+   const double p0c[] = { pos0[0] - sh->e0[0], pos0[1] - sh->e0[1], pos0[2] - sh->e0[2] };
+   const double p0cSquared = (p0c[0] * p0c[0]) + (p0c[1] * p0c[1]) + (p0c[2] * p0c[2]);
+   const double delta[] = { pos1[0] - pos0[0], pos1[1] - pos0[1], pos1[2] - pos0[2] };
+   const double p0cdotn = (p0c[0] * na[0]) + (p0c[1] * na[1]) + (p0c[2] * na[2]);
+   const double deltadotn = (delta[0] * na[0]) + (delta[1] * na[1]) + (delta[2] * na[2]);
+   const double deltadotnSquared = deltadotn * deltadotn;
+   const double p0cdotdelta = (delta[0] * p0c[0]) + (delta[1] * p0c[1]) + (delta[2] * p0c[2]);
+   const double deltaSquared = (delta[0] * delta[0]) + (delta[1] * delta[1]) + (delta[2] * delta[2]);
+   int intersectionnumber = 0;
+   double u = 0., u1 = 0., u2 = 0., projection = 0., savedprojection = 0.;
+   if (deltadotn != 0.) {
+      u1 = -p0cdotn / deltadotn;
+      if ((u1 > 0.) && (u1 <= 1.) && ((p0cSquared + (2 * u1 * p0cdotdelta) + (u1 * u1 * deltaSquared)) <= radius2)) {
+         nv.v[3] = u1;
+         intersectionnumber = 1;
+      }
+      u2 = u1 + (mLen / deltadotn);
+      if ((u2 > 0.) && (u2 <= 1.) && (u2 < nv.v[3]) &&
+          (((p0cSquared + (2 * u2 * p0cdotdelta) + (u2 * u2 * deltaSquared) + mLen2) -
+            (2 * mLen * (p0cdotn + (u2 * deltadotn)))) <= radius2)) {
+         nv.v[3] = u2;
+         intersectionnumber = 2;
+      }
+   }
+   if (!(((u1 < 0) && (u2 < 0)) || ((u1 > 1) && (u2 > 1)))) {
+      const double r0Squared = p0cSquared - (p0cdotn * p0cdotn);
+      const double r1Squared = (r0Squared + (2. * (p0cdotdelta - (p0cdotn * deltadotn))) + deltaSquared) - deltadotnSquared;
+      if ((r0Squared > radius2) || (r1Squared > radius2)) {
+         const double a = deltaSquared - deltadotnSquared;
+         const double minusbover2 = (p0cdotn * deltadotn) - p0cdotdelta;
+         double term = (minusbover2 * minusbover2) - (a * (r0Squared - radius2));
+         if (term >= 0) {
+            term = sqrt(term);
+            u = (minusbover2 + term) / a;
+            if ((u > 0) && (u <= 1) && (u < nv.v[3])) {
+               projection = p0cdotn + (u * deltadotn);
+               if ((projection >= 0) && (projection <= mLen)) {
+                  nv.v[3] = u;
+                  intersectionnumber = 3;
+                  savedprojection = projection;
+               }
+            }
+            u = (minusbover2 - term) / a;
+            if ((u > 0) && (u <= 1) && (u < nv.v[3])) {
+               projection = p0cdotn + (u * deltadotn);
+               if ((projection >= 0) && (projection <= mLen)) {
+                  nv.v[3] = u;
+                  intersectionnumber = 4;
+                  savedprojection = projection;
+               }
+            }
+         }
+      }
+   }
+   switch (intersectionnumber) {
+   case 1:
+      nv.v[0] = -na[0];
+      nv.v[1] = -na[1];
+      nv.v[2] = -na[2];
+      return nv;
+   case 2:
+      nv.v[0] = na[0];
+      nv.v[1] = na[1];
+      nv.v[2] = na[2];
+      return nv;
+   case 3:
+   case 4: {
+      const double normalv[] = { (p0c[0] + (nv.v[3] * delta[0])) - (savedprojection * na[0]),
+                                 (p0c[1] + (nv.v[3] * delta[1])) - (savedprojection * na[1]),
+                                 (p0c[2] + (nv.v[3] * delta[2])) - (savedprojection * na[2]) };
+      const double normalvmag = sqrt((normalv[0] * normalv[0]) + (normalv[1] * normalv[1]) + (normalv[2] * normalv[2]));
+      nv.v[0] = normalv[0] / normalvmag;
+      nv.v[1] = normalv[1] / normalvmag;
+      nv.v[2] = normalv[2] / normalvmag;
+      return nv;
+   }
+   }
+   return nv;
+}
+
 /* NISTMonte/Sphere.cu:21-45 (the normal is not defined for a sphere; returned as 0) */
 static double sphere_first_intersection(const shape_t* sh, const double* pos0, const double* pos1)
 {
@@ -1022,6 +1306,8 @@ static nvec shape_first_normal(const cmo_scene* s, int id, const double* pos0, c
    const shape_t* sh = &s->shapes[id];
    if (sh->kind == S_PLANES) return planes_first_normal(sh, pos0, pos1);
    if (sh->kind == S_INTERSECTION) return inter_first_normal(s, sh, pos0, pos1);
+   if (sh->kind == S_UNION) return union_first_normal(s, sh, pos0, pos1);
+   if (sh->kind == S_CYLINDER) return cylinder_first_normal(sh, pos0, pos1);
    nvec r = { { 0., 0., 0., sphere_first_intersection(sh, pos0, pos1) } };
    return r;
 }
@@ -1772,8 +2058,9 @@ void cmo_eval_shape(cmo_scene* s, int shape, int n, const double* p01, double* o
       const double* p0 = p01 + 6 * i;
       const double* p1 = p0 + 3;
       nvec v = shape_first_normal(s, shape, p0, p1);
-      for (int k = 0; k < 4; ++k) out[5 * i + k] = v.v[k];
-      out[5 * i + 4] = shape_contains(s, shape, p0);
+      for (int k = 0; k < 4; ++k) out[6 * i + k] = v.v[k];
+      out[6 * i + 4] = shape_contains(s, shape, p0);
+      out[6 * i + 5] = shape_contains2(s, shape, p0, p1);
    }
 }
 

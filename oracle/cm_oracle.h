@@ -63,8 +63,11 @@ int cmo_msm_set_barrier(cmo_scene* s, int msm, int classical, double lambda);
 int cmo_shape_sphere(cmo_scene* s, const double center[3], double radius);
 int cmo_shape_planes(cmo_scene* s, int n, const double* normals, const double* points);
 int cmo_shape_intersection(cmo_scene* s, int a, int b);
+int cmo_shape_cylinder(cmo_scene* s, const double end0[3], const double end1[3], double radius);
+int cmo_shape_union(cmo_scene* s, int a, int b);
 int cmo_shape_translate(cmo_scene* s, int shape, const double d[3]);
-int cmo_shape_line(cmo_scene* s, double topz, double width, double length, double thetal, double thetar);
+int cmo_shape_line(cmo_scene* s, double topz, double width, double length, double thetal, double thetar, double radl,
+                   double radr);
 int cmo_region(cmo_scene* s, int parent, int msm, int shape);
 
 /* ---- per-function evaluation on arrays, deviates injected (u arrays are row-major) */
@@ -82,7 +85,8 @@ void cmo_eval_elastic(cmo_scene* s, int msm, int mech, int n, const double* in /
 void cmo_eval_pmma(cmo_scene* s, int msm, int n, const double* in /* E len */, double* out /* csd fittedRate polaronRate */);
 void cmo_eval_phonon(cmo_scene* s, int msm, int mech, int n, const double* in /* E th ph u0 u1 */,
                      double* out /* rate E th ph Eprev ndev */);
-void cmo_eval_shape(cmo_scene* s, int shape, int n, const double* p01, double* out /* nx ny nz u inside */);
+void cmo_eval_shape(cmo_scene* s, int shape, int n, const double* p01,
+                    double* out /* nx ny nz u contains(p0) contains(p0,p1) */);
 void cmo_eval_barrier(cmo_scene* s, int from_region, int to_region, int struck_shape, int n,
                       const double* in /* E th ph x y z */, double* out /* E th ph x y z region */);
 void cmo_eval_freepath(cmo_scene* s, int msm, int n, const double* in /* E u */, double* out);

@@ -54,7 +54,9 @@ def lib():
         L.cmo_shape_planes.argtypes = [C.c_void_p, C.c_int, d, d]
         L.cmo_shape_intersection.argtypes = [C.c_void_p, C.c_int, C.c_int]
         L.cmo_shape_translate.argtypes = [C.c_void_p, C.c_int, d]
-        L.cmo_shape_line.argtypes = [C.c_void_p] + [C.c_double] * 5
+        L.cmo_shape_line.argtypes = [C.c_void_p] + [C.c_double] * 7
+        L.cmo_shape_cylinder.argtypes = [C.c_void_p, d, d, C.c_double]
+        L.cmo_shape_union.argtypes = [C.c_void_p, C.c_int, C.c_int]
         L.cmo_region.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int]
         L.cmo_eval_nistmott.argtypes = [C.c_void_p, C.c_int, C.c_int, d, d, d, d, i]
         L.cmo_eval_table.argtypes = [C.c_void_p, C.c_int, C.c_int, d, C.c_int, d]
@@ -197,8 +199,14 @@ class OracleBackend:
         d = np.array(d, dtype=np.float64)
         return self.L.cmo_shape_translate(self.h, shape, dp(d))
 
-    def line(self, *a):
-        return self._chk(self.L.cmo_shape_line(self.h, *a))
+    def line(self, topz, width, length, thetal, thetar, radl=0.0, radr=0.0):
+        return self._chk(self.L.cmo_shape_line(self.h, topz, width, length, thetal, thetar, radl, radr))
+
+    def cylinder(self, end0, end1, radius):
+        return self._chk(self.L.cmo_shape_cylinder(self.h, dp(list(end0)), dp(list(end1)), radius))
+
+    def union(self, a, b):
+        return self._chk(self.L.cmo_shape_union(self.h, a, b))
 
     def region(self, parent, msm, shape):
         return self._chk(self.L.cmo_region(self.h, parent, msm, shape))

@@ -52,6 +52,8 @@
 #include "gov/nist/nanoscalemetrology/JMONSEL/NormalMultiPlaneShape.cuh"
 #include "gov/nist/nanoscalemetrology/JMONSEL/NormalIntersectionShape.cuh"
 #include "gov/nist/nanoscalemetrology/JMONSEL/NShapes.cuh"
+#include "gov/nist/nanoscalemetrology/JMONSEL/NormalCylindricalShape.cuh"
+#include "gov/nist/nanoscalemetrology/JMONSEL/NormalUnionShape.cuh"
 
 // ---------------------------------------------------------------- deviate hook
 static std::deque<double> g_queue;
@@ -404,6 +406,86 @@ static void golden_shapes(const std::string& out)
    fclose(f);
 }
 
+// NormalCylindricalShape, NormalUnionShape and createLine with rounded corners
+static void golden_shapes2(const std::string& out)
+{
+   FILE* f = openw(out, "shapes2.txt");
+   fprintf(f, "# shape(0 oblique cylinder,1 cylinder along y,2 union(block, oblique cylinder),3 createLine radl 5 nm radr 8 nm,"
+              "4 the oblique cylinder translated by (30, 0, -10) nm, 5-7 shapes 0-2 with the cylinder axis normalised) "
+              "p0(3) p1(3) | nx ny nz u contains(p0) contains(p0,p1)\n");
+   double e0[] = { -20e-9, -10e-9, 30e-9 }, e1[] = { 25e-9, 15e-9, 50e-9 };
+   NormalCylindricalShapeT* cyl = new NormalCylindricalShapeT(e0, e1, 12e-9);
+   double f0[] = { 10e-9, -500e-9, -30e-9 }, f1[] = { 10e-9, 500e-9, -30e-9 };
+   NormalCylindricalShapeT* cyly = new NormalCylindricalShapeT(f0, f1, 8e-9);
+   NormalMultiPlaneShapeT* block = new NormalMultiPlaneShapeT();
+   double c[] = { 5e-9, -3e-9, 12e-9 }, h[] = { 15e-9, 10e-9, 5e-9 };
+   for (int a = 0; a < 3; ++a)
+      for (int sg = -1; sg <= 1; sg += 2) {
+         double n[] = { 0, 0, 0 }, p[] = { c[0], c[1], c[2] };
+         n[a] = sg;
+         p[a] += sg * h[a];
+         block->addPlane(*new PlaneT(n, 3, p, 3));
+      }
+   double e0b[] = { -20e-9, -10e-9, 30e-9 }, e1b[] = { 25e-9, 15e-9, 50e-9 };
+   NormalCylindricalShapeT* cylb = new NormalCylindricalShapeT(e0b, e1b, 12e-9);
+   NormalUnionShapeT* uni = new NormalUnionShapeT(*block, *cylb);
+   const double th = 3 * Math2::PI / 180;
+   NormalShapeT* rline = NShapes::createLine(-100e-9, 40e-9, 1e-6, th, th, 5e-9, 8e-9);
+   // (translating composites is unsafe in the reference: its casts between the
+   // ITransform and Shape bases; a cylinder translates itself)
+   double e0t[] = { -20e-9, -10e-9, 30e-9 }, e1t[] = { 25e-9, 15e-9, 50e-9 };
+   NormalCylindricalShapeT* cylt = new NormalCylindricalShapeT(e0t, e1t, 12e-9);
+   double d[] = { 30e-9, 0., -10e-9 };
+   cylt->translate(d);
+   // the same cylinders with their axis normalised: an identity rotation about the
+   // origin recomputes normalizedaxis from the (by then initialised) length
+   const double zero[] = { 0., 0., 0. };
+   NormalCylindricalShapeT* wcyl = new NormalCylindricalShapeT(e0, e1, 12e-9);
+   wcyl->rotate(zero, 0., 0., 0.);
+   NormalCylindricalShapeT* wcyly = new NormalCylindricalShapeT(f0, f1, 8e-9);
+   wcyly->rotate(zero, 0., 0., 0.);
+   NormalCylindricalShapeT* wcylb = new NormalCylindricalShapeT(e0b, e1b, 12e-9);
+   wcylb->rotate(zero, 0., 0., 0.);
+   NormalMultiPlaneShapeT* block2 = new NormalMultiPlaneShapeT();
+   for (int a = 0; a < 3; ++a)
+      for (int sg = -1; sg <= 1; sg += 2) {
+         double n[] = { 0, 0, 0 }, p[] = { c[0], c[1], c[2] };
+         n[a] = sg;
+         p[a] += sg * h[a];
+         block2->addPlane(*new PlaneT(n, 3, p, 3));
+      }
+   NormalUnionShapeT* wuni = new NormalUnionShapeT(*block2, *wcylb);
+   NormalShapeT* shapes[] = { cyl, cyly, uni, rline, cylt, wcyl, wcyly, wuni };
+   for (int s = 0; s < 8; ++s) {
+      for (int i = 0; i < 4000; ++i) {
+         double p0[3], p1[3];
+         for (int k = 0; k < 3; ++k) p0[k] = (uin() * 120 - 60) * 1e-9;
+         if (s >= 5) {  // start near the cylinders so that many steps cross them
+            const double* a0 = s == 6 ? f0 : e0;
+            const double* a1 = s == 6 ? f1 : e1;
+            const double t = s == 6 ? 0.45 + 0.1 * uin() : uin();
+            for (int k = 0; k < 3; ++k) p0[k] = a0[k] + t * (a1[k] - a0[k]) + (uin() * 40 - 20) * 1e-9;
+         }
+         if (s == 3) {
+            p0[0] = (uin() * 100 - 50) * 1e-9;
+            p0[2] = (uin() * 130 - 120) * 1e-9;
+         }
+         if (s == 4) p0[0] += 30e-9;
+         double len = ::exp(::log(0.05e-9) + (::log(200e-9) - ::log(0.05e-9)) * uin());
+         double th2 = Math2::PI * uin(), ph = 2 * Math2::PI * uin();
+         p1[0] = p0[0] + len * ::sin(th2) * ::cos(ph);
+         p1[1] = p0[1] + len * ::sin(th2) * ::sin(ph);
+         p1[2] = p0[2] + len * ::cos(th2);
+         VectorXd r = shapes[s]->getFirstNormal(p0, p1);
+         int inside = ((ShapeT*)shapes[s])->contains(p0) ? 1 : 0;
+         int inside2 = shapes[s]->contains(p0, p1) ? 1 : 0;
+         fprintf(f, "%d " G " " G " " G " " G " " G " " G " " G " " G " " G " " G " %d %d\n", s, p0[0], p0[1], p0[2], p1[0], p1[1],
+                 p1[2], r[0], r[1], r[2], r[3], inside, inside2);
+      }
+   }
+   fclose(f);
+}
+
 static void golden_misc(const std::string& out, SiModel& si)
 {
    FILE* f = openw(out, "misc.txt");
@@ -592,6 +674,7 @@ int main(int argc, char** argv)
       golden_shapes(out);
       golden_misc(out, si);
       golden_barrier(out, si);
+      golden_shapes2(out);
       return 0;
    }
    if (mode == "run1" && argc >= 5) {

@@ -51,3 +51,31 @@ def engine():
     e = capi.Engine(0)
     yield e
     e.close()
+
+
+def shapes2_scene(fixes=0):
+    """The shapes of the second shapes fixture: NormalCylindricalShape, NormalUnionShape and
+    NShapes::createLine with rounded corners."""
+    from cudamonsel_b200 import scenes
+    s = scenes.SceneSpec()
+    s.options = fixes
+    cyl = s.cylinder([-20e-9, -10e-9, 30e-9], [25e-9, 15e-9, 50e-9], 12e-9)
+    cyly = s.cylinder([10e-9, -500e-9, -30e-9], [10e-9, 500e-9, -30e-9], 8e-9)
+    c, hh = (5e-9, -3e-9, 12e-9), (15e-9, 10e-9, 5e-9)
+    n, p = [], []
+    for a in range(3):
+        for sg in (-1, 1):
+            nn = [0.0, 0.0, 0.0]
+            pp = list(c)
+            nn[a] = float(sg)
+            pp[a] += sg * hh[a]
+            n += nn
+            p += pp
+    block = s.planes(n, p)
+    cylb = s.cylinder([-20e-9, -10e-9, 30e-9], [25e-9, 15e-9, 50e-9], 12e-9)
+    uni = s.union(block, cylb)
+    th = 3 * 3.14159265358979323846 / 180
+    rline = s.line(-100e-9, 40e-9, 1e-6, th, th, 5e-9, 8e-9)
+    cylt = s.cylinder([-20e-9, -10e-9, 30e-9], [25e-9, 15e-9, 50e-9], 12e-9)
+    s.translate(cylt, [30e-9, 0.0, -10e-9])
+    return s, [cyl, cyly, uni, rline, cylt]

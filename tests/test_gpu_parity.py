@@ -331,6 +331,39 @@ def test_shapes(engine):
         assert (out[:, 4] == rows[:, 11]).mean() > 0.9999
 
 
+@pytest.mark.parametrize("fixes", [0, 1])
+def test_shapes2(fixes):
+    """NormalCylindricalShape, NormalUnionShape and the rounded createLine against the reference's
+    own results (cases 0-4: cylinders as the reference builds them; 5-7: axis normalised, built
+    here with CM_OPT_JMONSEL_FIXES).  The engine works in nm, the reference in m: u within 1e-9
+    relative and normals within 1e-9 where both report a crossing, crossing/containment decisions
+    identical except within rounding of a tangency (< 0.1 %)."""
+    from conftest import shapes2_scene
+    from cudamonsel_b200 import capi, scenes
+    s, shapes = shapes2_scene(fixes)
+    e = capi.Engine(0)
+    res = scenes.replay(s, scenes.EngineBackend(e))
+    g = golden("shapes2")
+    cases = range(5) if fixes == 0 else range(5, 8)
+    for k in cases:
+        sh = res[shapes[k if fixes == 0 else k - 5].idx]
+        rows = g[g[:, 0] == k]
+        out = e.eval_shape(sh, np.ascontiguousarray(rows[:, 1:7]))
+        fin = np.isfinite(rows[:, 10])
+        both = fin & np.isfinite(out[:, 3])
+        agree = (np.isfinite(out[:, 3]) == fin).mean()
+        r = rel(out[both, 3], rows[both, 10])
+        nerr = np.abs(out[both, 0:3] - rows[both, 7:10]).max(axis=1) if both.any() else np.zeros(1)
+        print("case %d crossings %d agree %.5f u max rel %.3g normal max err %.3g" % (
+            k, fin.sum(), agree, r.max() if both.any() else 0, nerr.max()))
+        assert agree > 0.999
+        if both.any():
+            assert np.quantile(r, 0.999) < 1e-9 and np.quantile(nerr, 0.999) < 1e-9
+        assert (out[:, 4] == rows[:, 11]).mean() > 0.999
+        assert (out[:, 5] == rows[:, 12]).mean() > 0.999
+    e.close()
+
+
 @pytest.mark.parametrize("prec", [FP64, FP32])
 def test_barrier(engine, prec):
     """ExpQMBarrierSM (classical) both ways across the vacuum/Si surface."""

@@ -128,6 +128,44 @@ def test_lines_match_oracle(lines_oracle_runs, prec, options):
         assert abs(zb) < 3.5 and abs(zs) < 3.5
 
 
+FEATURE_XS = np.array([-60.0, -35.0, 40.0, 60.0, 82.0]) * 1e-9
+
+
+@pytest.fixture(scope="module")
+def features_oracle_runs():
+    import pyoracle
+    from cudamonsel_b200 import scenes
+    sc = scenes.features()
+    centers = np.stack([FEATURE_XS, np.zeros(5), np.full(5, -120e-9)], axis=1)
+    ob, of, tl = pyoracle.run_scene(sc, centers, 1e-9, scenes.eV(800.0), 2000, 91, 80)
+    return centers, ob
+
+
+@pytest.mark.parametrize("prec", [FP64, FP32], ids=["fp64", "fp32"])
+def test_features_match_oracle(features_oracle_runs, prec):
+    """NormalCylindricalShape, the rounded createLine (NormalUnionShape of plane sets and cylinders)
+    and a block on Si at 800 eV: engine vs the oracle's whole trajectories at 5 landing points."""
+    from cudamonsel_b200 import capi, scenes
+    centers, ob = features_oracle_runs
+    e = capi.Engine(0)
+    sc = scenes.features()
+    h = scenes.build_engine(sc, e)
+    npix_rep, nprim = 16, 500
+    back, fwd, st = e.run(h["chamber"], np.repeat(centers, npix_rep, axis=0), scenes.eV(800.0), nprim, 80, 1e-9,
+                          seed=5, precision=prec)
+    e.close()
+    for i in range(5):
+        eb, es = batch_yields(back[i * npix_rep:(i + 1) * npix_rep], nprim, 800.0, 80)
+        rb, rs = batch_yields(ob[i:i + 1], nprim * 4, 800.0, 80)
+        se_b = eb.std(ddof=1) * np.sqrt(1.0 / npix_rep + 1.0 / 4)
+        se_s = es.std(ddof=1) * np.sqrt(1.0 / npix_rep + 1.0 / 4)
+        zb = (eb.mean() - rb[0]) / se_b
+        zs = (es.mean() - rs[0]) / se_s
+        print("x=%5.1f nm BSE %.4f/%.4f z=%.2f SE %.4f/%.4f z=%.2f" % (FEATURE_XS[i] * 1e9, eb.mean(), rb[0], zb,
+                                                                    es.mean(), rs[0], zs))
+        assert abs(zb) < 3.5 and abs(zs) < 3.5
+
+
 def test_deterministic_and_independent_of_batch(half):
     """Same seed -> identical tallies; a pixel's tally is the same alone and inside a larger
     batch of other pixels when it carries the same stream key (the serving guarantee)."""

@@ -160,12 +160,38 @@ def test_shapes():
     for k, sh in enumerate(handles):
         rows = g[g[:, 0] == k]
         p01 = np.ascontiguousarray(rows[:, 1:7])
-        out = np.zeros((len(rows), 5))
+        out = np.zeros((len(rows), 6))
         b.L.cmo_eval_shape(b.h, sh, len(rows), po.dp(p01), D(out))
         for j in range(5):
             ok, bad = exact(out[:, j], rows[:, 7 + j])
             assert ok, (k, j, bad)
         assert np.isfinite(rows[:, 10]).sum() > 10  # crossings exist
+
+
+@pytest.mark.parametrize("fixes", [0, 1])
+def test_shapes2(fixes):
+    """NormalCylindricalShape (oblique, along y, translated), NormalUnionShape(block, cylinder) and
+    the rounded createLine: first normal, u, contains(p0), contains(p0, p1).  The reference's
+    cylinder normalises its axis by a length not yet initialised (read as 0): pinned by cases
+    0-4; cases 5-7 are the reference's cylinders with the axis normalised, which the oracle
+    builds with the fixes option."""
+    import pyoracle as po
+    from cudamonsel_b200 import scenes
+    from conftest import shapes2_scene
+    s, shapes = shapes2_scene(fixes)
+    b = po.OracleBackend()
+    res = scenes.replay(s, b)
+    g = golden("shapes2")
+    cases = range(5) if fixes == 0 else range(5, 8)
+    for k in cases:
+        sh = shapes[k if fixes == 0 else k - 5]
+        rows = g[g[:, 0] == k]
+        p01 = np.ascontiguousarray(rows[:, 1:7])
+        out = np.zeros((len(rows), 6))
+        b.L.cmo_eval_shape(b.h, res[sh.idx], len(rows), po.dp(p01), D(out))
+        for j in range(6):
+            ok, bad = exact(out[:, j], rows[:, 7 + j])
+            assert ok, (k, j, bad)
 
 
 def test_barrier(oracle_halfspace):
