@@ -13,7 +13,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libcudamonsel_b200.so")
 SOURCES = ["cm_engine.cu"]
-DEPS = ["cm_engine.cu", "cm_device.cuh", "cm_physics.cuh", "cm_scene.h", "cm_wave.cuh"]
+DEPS = ["cm_engine.cu", "cm_device.cuh", "cm_physics.cuh", "cm_scene.h", "cm_wave.cuh", "cm_server.cuh"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
 FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC",

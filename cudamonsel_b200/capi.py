@@ -18,14 +18,17 @@ OPT_JMONSEL_FIXES = 1
 
 # every symbol include/cudamonsel_b200.h declares
 EXPORTS = (
-    "cm_context_create", "cm_context_destroy", "cm_last_error", "cm_set_options", "cm_version",
+    "cm_context_create", "cm_context_destroy", "cm_context_reset", "cm_last_error", "cm_set_options", "cm_version",
     "cm_add_mott_element", "cm_add_table", "cm_add_material", "cm_add_msm", "cm_msm_add_nistmott",
     "cm_msm_add_tabulated", "cm_msm_add_fitted", "cm_msm_add_phonon", "cm_msm_add_polaron", "cm_msm_set_csd_jln",
     "cm_msm_set_min_e", "cm_msm_set_barrier", "cm_shape_sphere", "cm_shape_planes", "cm_shape_intersection",
     "cm_shape_union", "cm_shape_cylinder", "cm_shape_translate", "cm_shape_line", "cm_region_add", "cm_run", "cm_run_device", "cm_run_noalloc",
     "cm_eval_nistmott", "cm_eval_table", "cm_eval_tabulated", "cm_eval_elastic", "cm_eval_csd", "cm_eval_phonon",
-    "cm_eval_shape", "cm_eval_barrier", "cm_eval_freepath",
+    "cm_eval_shape", "cm_eval_barrier", "cm_eval_freepath", "cm_server_create", "cm_server_destroy", "cm_job_submit",
+    "cm_job_poll", "cm_job_wait", "cm_job_cancel", "cm_job_result",
 )
+
+JOB_QUEUED, JOB_RUNNING, JOB_DONE, JOB_FAILED, JOB_CANCELLED = 0, 1, 2, 3, 4
 
 
 class RunDesc(C.Structure):
@@ -34,6 +37,11 @@ class RunDesc(C.Structure):
                 ("pixel_nprim", C.POINTER(C.c_int)), ("pixel_nbins", C.POINTER(C.c_int)), ("seed", C.c_uint64),
                 ("hist_stride", C.c_int), ("wave", C.c_int), ("max_iterations", C.c_int),
                 ("pixel_key", C.POINTER(C.c_uint64)), ("profile", C.c_int)]
+
+
+class JobInfo(C.Structure):
+    _fields_ = [("state", C.c_int), ("error", C.c_int), ("submit_s", C.c_double), ("start_s", C.c_double),
+                ("end_s", C.c_double), ("primaries", C.c_int64), ("steps", C.c_int64)]
 
 
 class RunStats(C.Structure):
@@ -72,6 +80,7 @@ def load(path=LIBPATH):
     sig = {
         "cm_context_create": [C.c_int, C.POINTER(C.c_void_p)],
         "cm_context_destroy": [ctx],
+        "cm_context_reset": [ctx],
         "cm_set_options": [ctx, C.c_int],
         "cm_add_mott_element": [ctx, C.c_int, d, d],
         "cm_add_table": [ctx, C.c_int, i, d, d, i],
@@ -96,6 +105,13 @@ def load(path=LIBPATH):
         "cm_run": [ctx, C.POINTER(RunDesc), C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.POINTER(RunStats)],
         "cm_run_device": [ctx, C.POINTER(RunDesc), C.c_void_p, C.c_void_p, C.POINTER(RunStats), C.c_void_p],
         "cm_run_noalloc": [ctx, C.POINTER(RunDesc), C.c_void_p, C.c_void_p, C.POINTER(RunStats), C.c_void_p],
+        "cm_server_create": [C.c_int, C.c_int, C.c_double, C.POINTER(C.c_void_p)],
+        "cm_server_destroy": [C.c_void_p],
+        "cm_job_submit": [C.c_void_p, ctx, C.POINTER(RunDesc), i],
+        "cm_job_poll": [C.c_void_p, C.c_int, C.POINTER(JobInfo)],
+        "cm_job_wait": [C.c_void_p, C.c_int, C.c_double, C.POINTER(JobInfo)],
+        "cm_job_cancel": [C.c_void_p, C.c_int],
+        "cm_job_result": [C.c_void_p, C.c_int, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.POINTER(RunStats)],
         "cm_eval_nistmott": [ctx, C.c_int, C.c_int, d, d, d, d, C.c_int],
         "cm_eval_table": [ctx, C.c_int, C.c_int, d, C.c_int, d, C.c_int],
         "cm_eval_tabulated": [ctx, C.c_int, C.c_int, C.c_int, d, d, C.c_int],
@@ -140,6 +156,10 @@ class Engine:
         if getattr(self, "h", None):
             self.L.cm_context_destroy(self.h)
             self.h = None
+
+    def reset(self):
+        """Forget the scene so this context can describe another (cm_context_reset)."""
+        self._check(self.L.cm_context_reset(self.h))
 
     def __del__(self):
         try:
@@ -317,3 +337,80 @@ class Engine:
 
     def eval_freepath(self, msm, inp, precision=PREC_FP64):
         return self._eval(self.L.cm_eval_freepath, (msm,), inp, 1, precision)[:, 0]
+
+
+def _run_desc(chamber, centers, energies, nprim, nbins, beam_width, seed, precision, pixel_keys=None, wave=0,
+              max_iterations=0, profile=0):
+    """A RunDesc over host arrays, and the arrays it points at (keep them alive while it is used)."""
+    centers = np.ascontiguousarray(centers, dtype=np.float64).reshape(-1, 3)
+    npix = len(centers)
+    e, pe = _d(np.broadcast_to(np.asarray(energies, dtype=np.float64), (npix,)).copy())
+    c, pc = _d(centers.ravel())
+    n, pn = _i(np.broadcast_to(np.asarray(nprim), (npix,)).copy())
+    b, pb = _i(np.broadcast_to(np.asarray(nbins), (npix,)).copy())
+    stride = int(b.max()) + 2
+    keys = None if pixel_keys is None else np.ascontiguousarray(pixel_keys, dtype=np.uint64)
+    desc = RunDesc(chamber, precision, npix, beam_width, pc, pe, pn, pb, seed, stride, wave, max_iterations,
+                   keys.ctypes.data_as(C.POINTER(C.c_uint64)) if keys is not None else None, profile)
+    return desc, (c, e, n, b, keys), npix, stride
+
+
+class Server:
+    """cm_server: a job server with `slots` resident engine contexts on one GPU."""
+
+    def __init__(self, device=0, slots=4, budget_gb=16.0):
+        self.L = load()
+        h = C.c_void_p()
+        rc = self.L.cm_server_create(device, slots, budget_gb, C.byref(h))
+        if rc:
+            raise CMError("cudamonsel_b200 error %d: %s" % (rc, self.L.cm_last_error().decode()))
+        self.h = h
+        self.shape = {}
+
+    def _check(self, rc):
+        if rc != 0:
+            raise CMError("cudamonsel_b200 error %d: %s" % (rc, self.L.cm_last_error().decode()))
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.cm_server_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def submit(self, engine, chamber, centers, energies, nprim, nbins, beam_width, seed, precision=PREC_FP32,
+               pixel_keys=None):
+        """Queue a job: the scene held by `engine` (copied now) and host pixel arrays (copied now)."""
+        desc, keep, npix, stride = _run_desc(chamber, centers, energies, nprim, nbins, beam_width, seed, precision,
+                                             pixel_keys)
+        job = C.c_int(-1)
+        self._check(self.L.cm_job_submit(self.h, engine.h, C.byref(desc), C.byref(job)))
+        self.shape[job.value] = (npix, stride)
+        return job.value
+
+    def poll(self, job):
+        info = JobInfo()
+        self._check(self.L.cm_job_poll(self.h, job, C.byref(info)))
+        return info
+
+    def wait(self, job, timeout=-1.0):
+        info = JobInfo()
+        self._check(self.L.cm_job_wait(self.h, job, timeout, C.byref(info)))
+        return info
+
+    def cancel(self, job):
+        self._check(self.L.cm_job_cancel(self.h, job))
+
+    def result(self, job):
+        """Tallies (back, fwd as [npix, stride]) and RunStats of a finished job; the server then forgets it."""
+        npix, stride = self.shape.pop(job)
+        back = np.zeros((npix, stride), dtype=np.uint32)
+        fwd = np.zeros((npix, stride), dtype=np.uint32)
+        st = RunStats()
+        self._check(self.L.cm_job_result(self.h, job, back.ctypes.data_as(C.POINTER(C.c_uint32)),
+                                         fwd.ctypes.data_as(C.POINTER(C.c_uint32)), C.byref(st)))
+        return back, fwd, st

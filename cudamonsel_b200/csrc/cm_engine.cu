@@ -21,6 +21,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -163,6 +164,7 @@ struct cm_context {
   Counters* counters = nullptr;
   Counters* counters_host = nullptr;
   cudaStream_t stream = nullptr;
+  const std::atomic<int>* cancel = nullptr;  // set by a job server: checked between graph launches
   void dirty() {
     d64.release();
     d32.release();
@@ -768,6 +770,10 @@ static int run_device_once(cm_context* ctx, const cm_run_desc* d, uint32_t* back
       break;
     }
     if (ctx->counters_host->done) break;
+    if (ctx->cancel && ctx->cancel->load()) {
+      status = fail(CM_ECANCELED, "cancelled");
+      break;
+    }
     if (iters >= maxIt) {
       const Counters& hc = *ctx->counters_host;
       char msg[256];
@@ -1010,11 +1016,28 @@ int cm_context_create(int device, cm_context** out) {
   c->device = device;
   c->nsm = prop.multiProcessorCount;
   // the flight kernel's call tree through nested NormalIntersectionShapes needs a few KB of local stack
-  CM_CUDA(cudaDeviceSetLimit(cudaLimitStackSize, 8192));
+  // (raised only once per device: changing the limit waits for the device to idle)
+  size_t stack = 0;
+  CM_CUDA(cudaDeviceGetLimit(&stack, cudaLimitStackSize));
+  if (stack < 8192) CM_CUDA(cudaDeviceSetLimit(cudaLimitStackSize, 8192));
   CM_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
   CM_CUDA(cudaMalloc(&c->counters, sizeof(Counters)));
   CM_CUDA(cudaMallocHost(&c->counters_host, sizeof(Counters)));
   *out = c.release();
+  return 0;
+}
+
+int cm_context_reset(cm_context* ctx) {
+  if (!ctx) return fail(CM_EINVAL, "null context");
+  cudaSetDevice(ctx->device);
+  ctx->dirty();
+  ctx->options = 0;
+  ctx->mott.clear();
+  ctx->tables.clear();
+  ctx->mats.clear();
+  ctx->msms.clear();
+  ctx->shapes.clear();
+  ctx->regions.clear();
   return 0;
 }
 
@@ -1973,3 +1996,5 @@ extern "C" int cm_run_noalloc(cm_context* ctx, const cm_run_desc* d, uint32_t* b
   return d->precision == CM_PREC_FP64 ? run_noalloc<double>(ctx, d, back, fwd, stats, s, (unsigned char*)scratch)
                                       : run_noalloc<float>(ctx, d, back, fwd, stats, s, (unsigned char*)scratch);
 }
+
+#include "cm_server.cuh"

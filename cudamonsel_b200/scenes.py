@@ -46,6 +46,10 @@ class SceneSpec:
         self.ops.append((name, args))
         return H(len(self.ops) - 1)
 
+    def set_options(self, options):
+        """Switch the option bits mid-scene: shapes read them when they are created (cylinders, rounded lines)."""
+        return self._op("set_options", options)
+
     def table(self, path):
         return self._op("table", path)
 

@@ -36,6 +36,7 @@ extern "C" {
 #define CM_ESTATE -4    /* scene incomplete or inconsistent */
 #define CM_EOVERFLOW -5 /* a device queue overflowed (secondary pool too small) */
 #define CM_ELIMIT -6    /* iteration limit reached before all trajectories ended */
+#define CM_ECANCELED -7 /* the job was cancelled */
 
 #define CM_PREC_FP64 0  /* plain form: all transport arithmetic in double */
 #define CM_PREC_FP32 1  /* batched form: float physics, double positions and plane solves */
@@ -49,6 +50,8 @@ typedef struct cm_context cm_context;
 /* ---- context -------------------------------------------------------------- */
 int cm_context_create(int device, cm_context** out);
 int cm_context_destroy(cm_context* ctx);
+/* forgets the scene (materials, models, tables, shapes, regions, options) so the context can describe another */
+int cm_context_reset(cm_context* ctx);
 const char* cm_last_error(void);
 int cm_set_options(cm_context* ctx, int options);
 int cm_version(void);
@@ -176,6 +179,45 @@ int cm_run_device(cm_context* ctx, const cm_run_desc* desc_device_arrays, uint32
  * ordered by the caller. */
 int cm_run_noalloc(cm_context* ctx, const cm_run_desc* desc_device_arrays, uint32_t* back_device,
                    uint32_t* fwd_device, cm_run_stats* stats, void* stream);
+
+/* ---- job server: streams of scan jobs --------------------------------------
+ * The reference runs one LinesOnLayers scan at a time on one thread
+ * (JMONSELTests/LinesOnLayers.cu:327-398).  A server keeps `slots` engine
+ * contexts resident on one GPU (own stream, scene, waves and pixel buffers) and
+ * starts queued jobs first in, first out as soon as a slot is free and the
+ * job's pixel and tally buffers fit in `budget_gb` beside the running jobs';
+ * slots run concurrently, so jobs that arrive while others are on the GPU
+ * overlap with them.  A job is a scene (copied from `scene` at submission, which
+ * the caller may then reuse) and a run description with HOST arrays (copied).
+ * Its tallies depend only on its scene, pixels and stream keys: the same alone
+ * and in any mix. */
+typedef struct cm_server cm_server;
+
+#define CM_JOB_QUEUED 0
+#define CM_JOB_RUNNING 1
+#define CM_JOB_DONE 2
+#define CM_JOB_FAILED 3
+#define CM_JOB_CANCELLED 4
+
+typedef struct {
+  int state;                       /* CM_JOB_* */
+  int error;                       /* status of a failed or cancelled job */
+  double submit_s, start_s, end_s; /* seconds on the server's clock */
+  int64_t primaries, steps;        /* of a finished job */
+} cm_job_info;
+
+int cm_server_create(int device, int slots, double budget_gb, cm_server** out);
+/* cancels running jobs at their next graph boundary, waits for the slots, frees everything */
+int cm_server_destroy(cm_server* server);
+int cm_job_submit(cm_server* server, const cm_context* scene, const cm_run_desc* desc, int* out_job);
+int cm_job_poll(cm_server* server, int job, cm_job_info* info);
+/* waits until the job has ended or timeout_s passed (timeout_s < 0: no limit) */
+int cm_job_wait(cm_server* server, int job, double timeout_s, cm_job_info* info);
+/* a queued job is dropped; a running one stops at its next graph boundary */
+int cm_job_cancel(cm_server* server, int job);
+/* copies a finished job's tallies ([npix * hist_stride] each, may be NULL) and stats, then forgets the job;
+ * a failed or cancelled job returns its error */
+int cm_job_result(cm_server* server, int job, uint32_t* back, uint32_t* fwd, cm_run_stats* stats);
 
 /* ---- per-function entry points (parity checks; host arrays, SI units) -------
  * Deviates are injected from u arrays so that each result can be compared

@@ -148,6 +148,9 @@ class OracleBackend:
             spwem, x1 = data.read_mott(Z)
             self.s.mott(Z, spwem, x1)
 
+    def set_options(self, options):
+        self.L.cmo_scene_set_options(self.h, options)
+
     def _chk(self, v):
         assert v >= 0, "oracle scene call failed (%d)" % v
         return v
