@@ -30,6 +30,8 @@ NPIX, NPRIM, BEAM_EV, NBINS = 256, 2000, 500.0, 50
 METRIC = "primary electrons/s at <=1% BSE/SE yield error vs FP64"
 WORKLOAD = ("linescan: 3 PMMA lines (h 100 nm, bottom w 40 nm, 3 deg, pitch 200 nm) on Si, 500 eV Gaussian "
             "sigma 1 nm, 256 px x 1 nm, 2000 primaries/px (512k primaries)")
+# served stream (latency line): jobs, mean arrival rate (1/s), server slots and budget, size scale
+SERVE_JOBS, SERVE_RATE, SERVE_SLOTS, SERVE_BUDGET_GB, SERVE_SCALE = 64, 8.0, 4, 16.0, 1 / 8
 BYTES_PER_STEP = 128  # algorithmic bytes per electron-step: a 64 B SoA record read and written
 
 
@@ -168,6 +170,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-serving", action="store_true", help="skip the served-stream latency measurement")
+    ap.add_argument("--no-image", action="store_true", help="skip the rough-line image (FP32 vs FP64)")
     ap.add_argument("--profile-run", action="store_true",
                     help="run one FP32 step of the workload and exit (the case for ncu captures)")
     a = ap.parse_args()
@@ -299,6 +303,54 @@ def main():
     if os.path.exists(tf):
         traffic = json.load(open(tf)).get(names[dom])
 
+    # batched image: rough lines (3 x 128 segments), 256 x 256 pixels at 2 nm, Poisson(300) primaries per
+    # pixel, energy per row from {300, 500, 1000} eV; FP32 batched form against the FP64 plain form
+    image_line = None
+    if not a.no_image:
+        img = scenes.rough_lines(seed=0)
+        eimg = capi.Engine(local)
+        hi = scenes.build_engine(img, eimg)
+        ic, ie, inp, inb = scenes.rough_image(seed=rank)
+        ikeys = np.arange(len(ic), dtype=np.uint64) + np.uint64(7_000_003 * (rank + 1))
+        runs = {}
+        for name, pr in (("fp32", capi.PREC_FP32), ("fp64", capi.PREC_FP64)):
+            t0 = time.perf_counter()
+            ib, _, ist = eimg.run(hi["chamber"], ic, ie, inp, inb, 1e-9, 0, precision=pr, pixel_keys=ikeys)
+            runs[name] = (ib, ist, time.perf_counter() - t0)
+        eimg.close()
+        ntot = int(inp.sum())
+        e_eV = ie / scenes.EV
+        y = {k: scenes.yields(v[0].astype(np.int64), np.maximum(inp, 1), e_eV, inb) for k, v in runs.items()}
+        err = {}
+        for j, nm in ((0, "bse"), (1, "se")):
+            a32, a64 = (y["fp32"][j] * inp).sum() / ntot, (y["fp64"][j] * inp).sum() / ntot
+            err[nm + "_fp32"], err[nm + "_fp64"], err[nm + "_rel_err"] = a32, a64, abs(a32 - a64) / a64
+        image_line = {"workload": "rough lines 3 x 128 segments (sidewall offsets N(0, 1.5 nm)), 256 x 256 px at "
+                                  "2 nm, Poisson(300)/px, E per row in {300, 500, 1000} eV",
+                      "primaries": ntot,
+                      "fp32_primaries_per_s": ntot / (runs["fp32"][1].device_ms / 1e3),
+                      "fp64_primaries_per_s": ntot / (runs["fp64"][1].device_ms / 1e3),
+                      "fp32_over_fp64": runs["fp64"][1].device_ms / runs["fp32"][1].device_ms,
+                      "fp32_e2e_s": runs["fp32"][2], "fp64_e2e_s": runs["fp64"][2],
+                      "electron_steps_fp32": int(runs["fp32"][1].steps),
+                      "yield_error_vs_fp64": err}
+
+    # served stream: random scan jobs (1-8 lines/cylinders on Si, 200-5000 eV, images or linescans) at
+    # Poisson arrivals through the job server, sizes scaled by SERVE_SCALE; p50/p99 of submit-to-done latency
+    serving_line = None
+    if not a.no_serving:
+        from cudamonsel_b200 import serving
+        js = serving.make_jobs(SERVE_JOBS, seed=100 + rank, scale=SERVE_SCALE)
+        out = serving.serve(js, rate_per_s=SERVE_RATE, slots=SERVE_SLOTS, budget_gb=SERVE_BUDGET_GB, seed=200 + rank,
+                            device=local)
+        lat = out["latency"]
+        serving_line = {"jobs": SERVE_JOBS, "rate_per_s": SERVE_RATE, "slots": SERVE_SLOTS,
+                        "budget_gb": SERVE_BUDGET_GB, "size_scale": SERVE_SCALE,
+                        "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
+                        "makespan_s": out["makespan"], "primaries": out["primaries"],
+                        "primaries_per_s": out["primaries"] / out["makespan"],
+                        "electron_steps_per_s": out["steps"] / out["makespan"]}
+
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         nproc = os.cpu_count() or 1
@@ -324,7 +376,7 @@ def main():
                 "clocks": clk, "gpu_launches": launches,
                 "e2e": {"value": e2e_value, "unit": "primaries/s", "h2d_bytes_per_step": h2d,
                         "d2h_bytes_per_step": d2h},
-                "cpu_baseline": cpu}
+                "cpu_baseline": cpu, "serving": serving_line, "image": image_line}
         print(json.dumps(line), flush=True)
     eng.close()
     if world > 1:

@@ -998,6 +998,35 @@ CM_D NV shape_first_normal(const SceneView<R>& s, int id, const double* p0, cons
   return FirstNormal<R, D>::eval(s, id, p0, p1);
 }
 
+// Region boxes (built on the host, padded against rounding) let a step skip the
+// children it cannot reach; the children that remain are tested in the same
+// order as before, so the region found and its tie-breaks are unchanged.
+CM_D bool point_in_box(const double* bb, const double* p) {
+  return p[0] >= bb[0] && p[1] >= bb[1] && p[2] >= bb[2] && p[0] <= bb[3] && p[1] <= bb[4] && p[2] <= bb[5];
+}
+
+// the segment p0 -> p1 meets the box (slab test over u in [0, 1])
+CM_D bool segment_meets_box(const double* bb, const double* p0, const double* p1) {
+  double lo = 0.0, hi = 1.0;
+  for (int a = 0; a < 3; ++a) {
+    const double d = p1[a] - p0[a];
+    if (d == 0.0) {
+      if (p0[a] < bb[a] || p0[a] > bb[3 + a]) return false;
+      continue;
+    }
+    double t0 = (bb[a] - p0[a]) / d, t1 = (bb[3 + a] - p0[a]) / d;
+    if (t0 > t1) {
+      const double t = t0;
+      t0 = t1;
+      t1 = t;
+    }
+    lo = t0 > lo ? t0 : lo;
+    hi = t1 < hi ? t1 : hi;
+    if (lo > hi) return false;
+  }
+  return true;
+}
+
 // RegionBase.cu:50-60, iterative: the first child whose shape holds p owns it
 template <typename R, int D = kMaxShapeDepth> CM_D int containing_subregion(const SceneView<R>& s, int reg, const double* p) {
   if (!shape_contains<R, D>(s, s.regions[reg].shape, p)) return -1;
@@ -1006,7 +1035,7 @@ template <typename R, int D = kMaxShapeDepth> CM_D int containing_subregion(cons
     int found = -1;
     for (int i = 0; i < r.nchild; ++i) {
       const int c = s.children[r.child0 + i];
-      if (shape_contains<R, D>(s, s.regions[c].shape, p)) { found = c; break; }
+      if (point_in_box(s.regions[c].bb, p) && shape_contains<R, D>(s, s.regions[c].shape, p)) { found = c; break; }
     }
     if (found < 0) return reg;
     reg = found;
@@ -1027,7 +1056,8 @@ template <typename R> CM_D bool is_containing_region(const SceneView<R>& s, int 
 // RegionBase.cu:74-119.  p1 is clipped to the boundary; returns the region just
 // over it (-1: outside the chamber) and the struck boundary's normal.
 template <typename R, int D = kMaxShapeDepth>
-CM_D int find_end_of_step(const SceneView<R>& s, int reg, const double* p0, double* p1, double* hitn) {
+CM_D int find_end_of_step(const SceneView<R>& s, int reg, const double* p0, double* p1, double* hitn,
+                          bool* clipped = nullptr) {
   const Region& r = s.regions[reg];
   int base = reg;
   NV nv = shape_first_normal<R, D>(s, r.shape, p0, p1);
@@ -1036,6 +1066,7 @@ CM_D int find_end_of_step(const SceneView<R>& s, int reg, const double* p0, doub
   if ((t <= 1.0) && r.parent >= 0) base = r.parent;
   for (int i = 0; i < r.nchild; ++i) {
     const int c = s.children[r.child0 + i];
+    if (!segment_meets_box(s.regions[c].bb, p0, p1)) continue;
     NV cn = shape_first_normal<R, D>(s, s.regions[c].shape, p0, p1);
     if ((cn.u <= 1.0) && (cn.u < t)) {
       t = cn.u;
@@ -1043,6 +1074,7 @@ CM_D int find_end_of_step(const SceneView<R>& s, int reg, const double* p0, doub
       hitn[0] = cn.n[0]; hitn[1] = cn.n[1]; hitn[2] = cn.n[2];
     }
   }
+  if (clipped) *clipped = t <= 1.0;
   if (t <= 1.0) {
     const double delta[3] = {p1[0] - p0[0], p1[1] - p0[1], p1[2] - p0[2]};
     p1[0] = p0[0] + (t * delta[0]);

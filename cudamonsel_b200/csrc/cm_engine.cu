@@ -21,6 +21,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <atomic>
 #include <cmath>
 #include <cstdio>
@@ -266,6 +267,92 @@ static void mott_constants(int Z, const HMott& hm, Mott& m) {
   m.rutherfordAlpha = 5.44968e-19 * pow(Z, 2.0 / 3.0) * kFromSIeV;
 }
 
+// ---- bounding boxes (SI), used only to skip shapes a step cannot reach
+struct Box {
+  double lo[3], hi[3];
+};
+
+static const double kBoxWorld = 1.0;  // m: steps never leave |x| < 0.3 m (0.1 m chamber + a 0.2 m step)
+
+static Box box_world() { return Box{{-kBoxWorld, -kBoxWorld, -kBoxWorld}, {kBoxWorld, kBoxWorld, kBoxWorld}}; }
+
+// vertices of {x : n_i . (x - p_i) <= 0} clipped to the world box, by intersecting plane triples
+static Box planes_box(const HShape& s) {
+  std::vector<std::array<double, 6>> pl;  // n, p
+  for (size_t i = 0; i < s.n.size() / 3; ++i)
+    pl.push_back({s.n[3 * i], s.n[3 * i + 1], s.n[3 * i + 2], s.p[3 * i], s.p[3 * i + 1], s.p[3 * i + 2]});
+  for (int a = 0; a < 3; ++a)
+    for (int sg = -1; sg <= 1; sg += 2) {
+      std::array<double, 6> q = {0, 0, 0, 0, 0, 0};
+      q[a] = sg;
+      q[3 + a] = sg * kBoxWorld;
+      pl.push_back(q);
+    }
+  Box b{{INFINITY, INFINITY, INFINITY}, {-INFINITY, -INFINITY, -INFINITY}};
+  const size_t n = pl.size();
+  for (size_t i = 0; i < n; ++i)
+    for (size_t j = i + 1; j < n; ++j)
+      for (size_t k = j + 1; k < n; ++k) {
+        const double* A = pl[i].data();
+        const double* B = pl[j].data();
+        const double* C = pl[k].data();
+        const double det = A[0] * (B[1] * C[2] - B[2] * C[1]) - A[1] * (B[0] * C[2] - B[2] * C[0]) +
+                           A[2] * (B[0] * C[1] - B[1] * C[0]);
+        if (fabs(det) < 1e-12) continue;
+        const double da = A[0] * A[3] + A[1] * A[4] + A[2] * A[5];
+        const double db = B[0] * B[3] + B[1] * B[4] + B[2] * B[5];
+        const double dc = C[0] * C[3] + C[1] * C[4] + C[2] * C[5];
+        double x[3];
+        x[0] = (da * (B[1] * C[2] - B[2] * C[1]) - A[1] * (db * C[2] - B[2] * dc) + A[2] * (db * C[1] - B[1] * dc)) / det;
+        x[1] = (A[0] * (db * C[2] - B[2] * dc) - da * (B[0] * C[2] - B[2] * C[0]) + A[2] * (B[0] * dc - db * C[0])) / det;
+        x[2] = (A[0] * (B[1] * dc - db * C[1]) - A[1] * (B[0] * dc - db * C[0]) + da * (B[0] * C[1] - B[1] * C[0])) / det;
+        bool in = true;
+        for (size_t m = 0; m < n && in; ++m) {
+          const double* P = pl[m].data();
+          const double d = P[0] * (x[0] - P[3]) + P[1] * (x[1] - P[4]) + P[2] * (x[2] - P[5]);
+          const double scale = 1e-9 * (1.0 + fabs(x[0]) + fabs(x[1]) + fabs(x[2]));
+          in = d <= scale;
+        }
+        if (!in) continue;
+        for (int a = 0; a < 3; ++a) {
+          b.lo[a] = std::min(b.lo[a], x[a]);
+          b.hi[a] = std::max(b.hi[a], x[a]);
+        }
+      }
+  return b;  // empty (lo > hi) when the plane set holds nothing inside the world box
+}
+
+static Box shape_box(cm_context* ctx, int id) {
+  const HShape& s = ctx->shapes[id];
+  Box b;
+  switch (s.kind) {
+    case SHAPE_PLANES:
+      return planes_box(s);
+    case SHAPE_SPHERE:
+      for (int a = 0; a < 3; ++a) {
+        b.lo[a] = s.c[a] - s.r;
+        b.hi[a] = s.c[a] + s.r;
+      }
+      return b;
+    case SHAPE_CYLINDER:  // both end discs lie in the spheres of radius r about the end points
+      for (int a = 0; a < 3; ++a) {
+        b.lo[a] = std::min(s.e0[a], s.e0[a] + s.ax[a]) - s.radius;
+        b.hi[a] = std::max(s.e0[a], s.e0[a] + s.ax[a]) + s.radius;
+      }
+      return b;
+    case SHAPE_INTERSECTION:
+    case SHAPE_UNION: {
+      const Box x = shape_box(ctx, s.a), y = shape_box(ctx, s.b);
+      for (int a = 0; a < 3; ++a) {
+        b.lo[a] = s.kind == SHAPE_UNION ? std::min(x.lo[a], y.lo[a]) : std::max(x.lo[a], y.lo[a]);
+        b.hi[a] = s.kind == SHAPE_UNION ? std::max(x.hi[a], y.hi[a]) : std::min(x.hi[a], y.hi[a]);
+      }
+      return b;
+    }
+  }
+  return box_world();
+}
+
 template <typename R>
 static int build_scene(cm_context* ctx, DevScene<R>& ds) {
   if (ds.valid) return 0;
@@ -477,6 +564,13 @@ static int build_scene(cm_context* ctx, DevScene<R>& ds) {
     r.child0 = (int)children.size();
     r.nchild = (int)hr.children.size();
     r.cls = hr.msm < kClasses ? hr.msm : kClasses - 1;
+    // the box in nm, widened so that rounding never excludes a crossing or a point on the surface
+    const Box bx = shape_box(ctx, hr.shape);
+    for (int a = 0; a < 3; ++a) {
+      const double pad = 1e-3 + 1e-9 * std::max(fabs(bx.lo[a]), fabs(bx.hi[a])) * 1e9;
+      r.bb[a] = bx.lo[a] <= -kBoxWorld * 0.999 ? -INFINITY : bx.lo[a] * 1e9 - pad;
+      r.bb[3 + a] = bx.hi[a] >= kBoxWorld * 0.999 ? INFINITY : bx.hi[a] * 1e9 + pad;
+    }
     for (int c : hr.children) children.push_back(c);
     regions.push_back(r);
   }

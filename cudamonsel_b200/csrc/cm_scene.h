@@ -42,6 +42,7 @@ struct Region {
   int parent, msm, shape;
   int child0, nchild;  // children indices in Scene::children
   int cls;             // wave segment of electrons in this region (by material model)
+  double bb[6];        // axis-aligned box holding the region's shape (nm): min xyz, max xyz
 };
 
 // electrons are kept in one wave segment per material class, so that the

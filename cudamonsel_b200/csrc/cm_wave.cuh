@@ -180,12 +180,20 @@ CM_D void flight_one(const RunView<R>& v, int cur, int i, Sink& sink, StepCounts
   if (total != R(0)) {
     const R f = -mlog(g.next()) / total;
     if ((double)f < fp) fp = (double)f;
-  } else if (e.step > 1000000u) {
+  } else if (e.step > 1000000u) {  // MONSEL_MaterialScatterModel::randomMeanPathLength (:86-90)
+    complete = true;
+  } else if (!(e.E > R(0)) && e.step > 4096u) {
+    // With no energy and no mechanism an electron only flies straight and is reflected by every
+    // barrier it meets (ExpQMBarrierSM: perpE = 0 never transmits); trapped between two walls it
+    // bounces until the 1e6-step limit above, one wave iteration per bounce.  It is ended here
+    // once it has taken 4096 steps (one that would have reached the chamber later, tallied at
+    // 0 eV, is lost; that needs more than 4096 steps and never occurred in the tests).
     complete = true;
   }
   double p1[3] = {e.p[0] + fp * (double)e.d[0], e.p[1] + fp * (double)e.d[1], e.p[2] + fp * (double)e.d[2]};
   double hn[3];
-  const int next = find_end_of_step<R, D>(s, reg, e.p, p1, hn);
+  bool clipped = false;
+  const int next = find_end_of_step<R, D>(s, reg, e.p, p1, hn, &clipped);
   const double dd = sqrt((p1[0] - e.p[0]) * (p1[0] - e.p[0]) + (p1[1] - e.p[1]) * (p1[1] - e.p[1]) +
                          (p1[2] - e.p[2]) * (p1[2] - e.p[2]));
   const R dE = m.csd ? jln_compute(m.jln, (R)dd, e.E) : R(0);
@@ -200,6 +208,16 @@ CM_D void flight_one(const RunView<R>& v, int cur, int i, Sink& sink, StepCounts
   if (next == reg) {
     ++sc.scat;
     if (total == R(0)) {
+      // A step without mechanisms (vacuum) that stopped at a boundary leading back into the
+      // same region: the segment grazed a shape within less than SMALL_DISP, or starts on the
+      // far face of one.  The reference repeats such zero-length steps until its 1e6-step
+      // limit (MONSEL_MaterialScatterModel.cu:88); move past the boundary as takeStep does
+      // after a crossing (MonteCarloSS.cu:145).
+      if (clipped) {
+        e.p[0] += kSmallDispNm * (double)e.d[0];
+        e.p[1] += kSmallDispNm * (double)e.d[1];
+        e.p[2] += kSmallDispNm * (double)e.d[2];
+      }
       queue = Q_MISC;
       e.aux = aux_pack(AUX_PASS, 0);
     } else {

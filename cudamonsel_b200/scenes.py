@@ -230,6 +230,46 @@ def lines(nlines=3, pitch=200e-9, height=100e-9, width=40e-9, length=1e-6, angle
     return Scene(s, chamber, vac=vac, si=si, pmma=pm, si_region=sireg, lines=line_regions)
 
 
+def rough_lines(seed=0, nlines=3, pitch=200e-9, height=100e-9, width=40e-9, length=1e-6, angle_deg=3.0,
+                nseg=128, sigma=1.5e-9, tables=None):
+    """The linescan's three PMMA lines with seeded edge roughness: each line is split into nseg segments
+    along y (NShapes::createLine each), every segment's left and right sidewalls offset in x by
+    independent N(0, sigma) draws."""
+    rng = np.random.default_rng(seed)
+    s = SceneSpec()
+    vac = vacuum(s)
+    si = silicon(s, tables)
+    pm = pmma(s)
+    chamber = s.region(None, vac, s.sphere([0.0, 0.0, 0.0], 0.1))
+    surf = s.planes([0.0, 0.0, -1.0], [0.0, 0.0, 0.0])
+    sireg = s.region(chamber, si, surf)
+    th = angle_deg * math.pi / 180.0
+    seg = length / nseg
+    regions = []
+    for i in range(nlines):
+        xc = (i - (nlines - 1) / 2.0) * pitch
+        for k in range(nseg):
+            dl, dr = rng.normal(0.0, sigma, 2)
+            ln = s.line(-height, width + dr - dl, seg, th, th)
+            s.translate(ln, [xc + (dl + dr) / 2.0, -length / 2.0 + (k + 0.5) * seg, 0.0])
+            regions.append(s.region(chamber, pm, ln))
+    return Scene(s, chamber, vac=vac, si=si, pmma=pm, si_region=sireg, segments=regions)
+
+
+def rough_image(seed=0, side=256, step=2e-9, mean_nprim=300, energies_eV=(300.0, 500.0, 1000.0), z=-120e-9):
+    """The batched-image scan: side x side pixels at `step`, primaries per pixel ~ Poisson(mean_nprim), beam
+    energy drawn per row from energies_eV.  Returns centres (m), energies (J), primaries, bins per pixel."""
+    rng = np.random.default_rng(seed + 7919)
+    xs = (np.arange(side) - (side - 1) / 2.0) * step
+    gx, gy = np.meshgrid(xs, xs)  # row = y
+    centers = np.stack([gx.ravel(), gy.ravel(), np.full(side * side, z)], axis=1)
+    row_e = rng.choice(np.asarray(energies_eV), side)
+    e_eV = np.repeat(row_e, side)
+    nprim = rng.poisson(mean_nprim, side * side).astype(np.int32)
+    nbins = (e_eV / 10.0).astype(np.int32)
+    return centers, eV(e_eV), nprim, nbins
+
+
 def features(options=1, tables=None):
     """Si substrate carrying a PMMA cylinder lying along y (radius 30 nm, axis at x = -60 nm, z = -30 nm), a
     rounded PMMA line (NShapes::createLine, corner radii 10 nm, centred at x = +60 nm) and a Si block.

@@ -33,7 +33,7 @@ static const double SMALL_DISP = 1.0e-15;
 #define MAXEL 8
 #define MAXMECH 8
 #define MAXPLANES 16
-#define MAXCHILD 64
+#define MAXCHILD 1024
 
 /* ---------------------------------------------------------------- deviates */
 static uint64_t splitmix64(uint64_t* x)

@@ -166,6 +166,43 @@ def test_features_match_oracle(features_oracle_runs, prec):
         assert abs(zb) < 3.5 and abs(zs) < 3.5
 
 
+ROUGH_XS = np.array([-219.0, -200.0, -180.0, -21.0, 1.0, 21.0]) * 1e-9
+
+
+@pytest.fixture(scope="module")
+def rough_oracle_runs():
+    import pyoracle
+    from cudamonsel_b200 import scenes
+    sc = scenes.rough_lines(seed=4)
+    centers = np.stack([ROUGH_XS, np.linspace(-40e-9, 40e-9, 6), np.full(6, -120e-9)], axis=1)
+    ob, of, tl = pyoracle.run_scene(sc, centers, 1e-9, scenes.eV(500.0), 2000, 13, 50)
+    return centers, ob
+
+
+@pytest.mark.parametrize("prec", [FP64, FP32], ids=["fp64", "fp32"])
+def test_rough_lines_match_oracle(rough_oracle_runs, prec):
+    """The rough-line layout (3 lines x 128 segments with N(0, 1.5 nm) sidewall offsets, 385 regions
+    under the chamber) at 500 eV: engine vs oracle at 6 landing points on and beside the edges."""
+    from cudamonsel_b200 import capi, scenes
+    centers, ob = rough_oracle_runs
+    e = capi.Engine(0)
+    h = scenes.build_engine(scenes.rough_lines(seed=4), e)
+    npix_rep, nprim = 16, 500
+    back, fwd, st = e.run(h["chamber"], np.repeat(centers, npix_rep, axis=0), scenes.eV(500.0), nprim, 50, 1e-9,
+                          seed=21, precision=prec)
+    e.close()
+    for i in range(len(centers)):
+        eb, es = batch_yields(back[i * npix_rep:(i + 1) * npix_rep], nprim, 500.0, 50)
+        rb, rs = batch_yields(ob[i:i + 1], nprim * 4, 500.0, 50)
+        se_b = eb.std(ddof=1) * np.sqrt(1.0 / npix_rep + 1.0 / 4)
+        se_s = es.std(ddof=1) * np.sqrt(1.0 / npix_rep + 1.0 / 4)
+        zb = (eb.mean() - rb[0]) / se_b
+        zs = (es.mean() - rs[0]) / se_s
+        print("x=%6.1f nm BSE %.4f/%.4f z=%.2f SE %.4f/%.4f z=%.2f" % (ROUGH_XS[i] * 1e9, eb.mean(), rb[0], zb,
+                                                                    es.mean(), rs[0], zs))
+        assert abs(zb) < 3.5 and abs(zs) < 3.5
+
+
 def test_deterministic_and_independent_of_batch(half):
     """Same seed -> identical tallies; a pixel's tally is the same alone and inside a larger
     batch of other pixels when it carries the same stream key (the serving guarantee)."""
