@@ -190,27 +190,39 @@ template <typename R> CM_D R uneville3(R f0, R f1, R f2, R f3, R x) {
 }
 
 // ULagrangeInterpolation.cu:35-48
-template <typename R> CM_D R ulagrange_d1(const R* f, int len, R x0, R xinc, R x) {
-  const R reducedx = (x - x0) / xinc;
+// The grid coordinate, the window index and the offset inside the window are
+// computed in double in both precisions: a float coordinate of up to 60 grid
+// steps keeps only ~1e-5 of a step, which the cubic turns into ~1e-6 relative
+// error; the table values and the Neville recursion stay in R.
+template <typename T, typename R> CM_D T ulagrange_d1_as(const R* f, int len, double x0, double xinc, double x) {
+  const double reducedx = (x - x0) / xinc;
   int index0 = (int)reducedx - 1;
   if (index0 < 0) index0 = 0;
   else if (index0 > len - 4) index0 = len - 4;
-  return uneville3(f[index0], f[index0 + 1], f[index0 + 2], f[index0 + 3], reducedx - (R)index0);
+  return uneville3((T)f[index0], (T)f[index0 + 1], (T)f[index0 + 2], (T)f[index0 + 3], (T)(reducedx - (double)index0));
+}
+
+template <typename R> CM_D R ulagrange_d1(const R* f, int len, double x0, double xinc, double x) {
+  return ulagrange_d1_as<R, R>(f, len, x0, xinc, x);
 }
 
 // ULagrangeInterpolation.cu:80-103, f row-major [n0][n1]
-template <typename R> CM_D R ulagrange_d2(const R* f, int n0, int n1, R x00, R x01, R xinc0, R xinc1, R xa, R xb) {
-  const R reducedx1 = (xa - x00) / xinc0;
+template <typename R>
+CM_D R ulagrange_d2(const R* f, int n0, int n1, double x00, double x01, double xinc0, double xinc1, double xa,
+                    double xb) {
+  const double reducedx1 = (xa - x00) / xinc0;
   int index0 = (int)reducedx1 - 1;
   if (index0 < 0) index0 = 0;
   else if (index0 > n0 - 4) index0 = n0 - 4;
-  R y[4];
+  // the recursion runs in double (the NISTMott quantile table is read from its double copy in both
+  // precisions): neighbouring quantiles cancel in the cubic, which cost float up to ~2e-6 of the angle
+  double y[4];
 #pragma unroll
-  for (int i = 0; i < 4; ++i) y[i] = ulagrange_d1(f + (size_t)(index0 + i) * n1, n1, x01, xinc1, xb);
+  for (int i = 0; i < 4; ++i) y[i] = ulagrange_d1_as<double>(f + (size_t)(index0 + i) * n1, n1, x01, xinc1, xb);
   // the final 1-D step runs on the 4 values with x0 moved to the window start
-  const R x0w = x00 + (R)index0 * xinc0;
-  const R reducedx = (xa - x0w) / xinc0;
-  return uneville3(y[0], y[1], y[2], y[3], reducedx);
+  const double x0w = x00 + (double)index0 * xinc0;
+  const double reducedx = (xa - x0w) / xinc0;
+  return (R)uneville3(y[0], y[1], y[2], y[3], reducedx);
 }
 
 // ------------------------------------------------------------ non-uniform Lagrange
@@ -387,7 +399,7 @@ template <typename R, typename G> CM_D R browning_angle(const Mott& m, R E, G& g
 template <typename R> CM_D R nistmott_rate(const SceneView<R>& s, const Mott& m, R kel, R kbrown, R E, R logE) {
   if (E < (R)m.extrapolateBelowEnergy) return (R)m.sfBrowning * browning_sigma(m, E) * kbrown;
   if (E < (R)s.maxMott) {
-    return kel * ulagrange_d1(s.blob + m.off_spwem, 61, (R)s.dl50, (R)s.param, logE);
+    return kel * ulagrange_d1(s.blob + m.off_spwem, 61, s.dl50, s.param, (double)logE);
   }
   // ScreenedRutherfordScatteringAngle.cu:24-30
   return (R)m.rutherfordA / (E + (R)m.rutherfordB) * kbrown;
@@ -397,15 +409,20 @@ template <typename R> CM_D R nistmott_rate(const SceneView<R>& s, const Mott& m,
 template <typename R, typename G> CM_D R nistmott_angle(const SceneView<R>& s, const Mott& m, R E, G& g) {
   if (E < (R)m.extrapolateBelowEnergy) return browning_angle(m, E, g, (s.options & 1) != 0);
   if (E < (R)s.maxMott) {
-    const R lg = mlog(E);
+    const double lg = log((double)E);  // double in both precisions: see ulagrange_d1
     const R u = g.next();
-    const R q = ulagrange_d2(s.blob + m.off_x1, 61, 201, (R)s.dl50, R(0), (R)s.param, R(0.005), lg, u);
-    return angle_from_q(q);
+    const double q = ulagrange_d2(s.mott64 + m.off_x1d, 61, 201, s.dl50, 0.0, s.param, 0.005, lg, (double)u);
+    if (sizeof(R) == 4) {  // theta near pi: asin is ill-conditioned near 1, so q is not rounded to float first
+      const double a = fabs(q);
+      return a >= 1.0 ? (R)kPi : (R)(2.0 * asin(a));
+    }
+    return angle_from_q((R)q);
   }
-  // ScreenedRutherfordScatteringAngle.cu:32-39
-  const R alpha = (R)m.rutherfordAlpha / E;
-  const R r = g.next();
-  return acos_1m(R(2.0) * alpha * r / (1 + alpha - r));
+  // ScreenedRutherfordScatteringAngle.cu:32-39; in double in both precisions (1 + alpha - r cancels for
+  // deviates near 1)
+  const double alpha = m.rutherfordAlpha / (double)E;
+  const double r = (double)g.next();
+  return (R)acos_1m(2.0 * alpha * r / (1 + alpha - r));
 }
 
 // ------------------------------------------------------------ direction algebra

@@ -358,6 +358,7 @@ static int build_scene(cm_context* ctx, DevScene<R>& ds) {
   if (ds.valid) return 0;
   ds.release();
   std::vector<R> blob;
+  std::vector<double> mott64;
   // tables, converted by role to eV / nm units
   std::vector<Table> tabs;
   for (auto& t : ctx->tables) {
@@ -389,8 +390,9 @@ static int build_scene(cm_context* ctx, DevScene<R>& ds) {
     mott_constants(kv.first, kv.second, m);
     m.off_spwem = (int)blob.size();
     for (double v : kv.second.spwem) blob.push_back((R)v);
-    m.off_x1 = (int)blob.size();
-    for (double v : kv.second.x1) blob.push_back((R)v);
+    m.off_x1 = -1;
+    m.off_x1d = (int)mott64.size();  // the quantile table in double as well (the angle's cubic needs it)
+    for (double v : kv.second.x1) mott64.push_back(v);
     mottIndex[kv.first] = (int)motts.size();
     motts.push_back(m);
   }
@@ -581,7 +583,7 @@ static int build_scene(cm_context* ctx, DevScene<R>& ds) {
       (rc = dev_copy(ds.allocs, regions, &v.regions, h)) || (rc = dev_copy(ds.allocs, children, &v.children, h)) ||
       (rc = dev_copy(ds.allocs, msms, &v.msms, h)) || (rc = dev_copy(ds.allocs, mechs, &v.mechs, h)) ||
       (rc = dev_copy(ds.allocs, motts, &v.mott, h)) || (rc = dev_copy(ds.allocs, tabs, &v.tables, h)) ||
-      (rc = dev_copy(ds.allocs, blob, &v.blob, h)))
+      (rc = dev_copy(ds.allocs, blob, &v.blob, h)) || (rc = dev_copy(ds.allocs, mott64, &v.mott64, h)))
     return rc;
   v.chamber = 0;
   v.options = ctx->options;

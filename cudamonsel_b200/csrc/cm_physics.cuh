@@ -82,7 +82,15 @@ CM_D bool tabulated_scatter(const SceneView<R>& s, const Mech& k, R d[3], R& E, 
   E = kE0 - deltaE;
   if (deltaE < bandgap) return false;
   R ct = mcos(theta);
-  const R Eq = (R(2) * kE) - deltaE - (R(2) * msqrt(kE * (kE - deltaE)) * ct);
+  // momentum-transfer energy; in FP32 the reference's form loses everything to cancellation for small
+  // losses and angles, so it is evaluated in double as (sqrt(E) - sqrt(E - dE))^2 + 4 sqrt(E (E - dE)) sin^2(theta/2)
+  R Eq;
+  if (sizeof(R) == 4) {
+    const double a = sqrt((double)kE), b = sqrt((double)kE - (double)deltaE), sh = sin(0.5 * (double)theta);
+    Eq = (R)(((a - b) * (a - b)) + (4.0 * a * b * sh * sh));
+  } else {
+    Eq = (R(2) * kE) - deltaE - (R(2) * msqrt(kE * (kE - deltaE)) * ct);
+  }
   const R bEref = (R)k.bEref, ecb = (R)k.energyCBbottom, minGen = (R)k.minEgenSE, off = (R)k.energyOffset;
   R energySE;
   const R be = pick_be(k, deltaE);
@@ -114,18 +122,19 @@ CM_D bool tabulated_scatter(const SceneView<R>& s, const Mech& k, R d[3], R& E, 
   const R sum = (R(2) * oFE) + deltaE;
   const R Eqmin = sum - root, Eqmax = sum + root;
   if ((Eqmin <= Eq) && (Eq <= Eqmax)) {  // single electron: simESEf (TabulatedInelasticSM.cu:87-101)
-    const R q = msqrt(Eq);
-    const R kz = (deltaE - Eq) / R(2) / q;
-    const R kzf = kz + q;
-    const R Ezq = kzf * kzf;
-    R minE = (oFE + bandgap) - Ezq;
-    if (minE < R(0)) minE = 0;
-    const R maxE = oFE - (kz * kz);
-    const R r = randoms[3];
-    const R Exy = (minE * (R(1) - r)) + (maxE * r);
-    const R ESEf = Exy + Ezq;
-    const R th1 = macos(kzf / msqrt(ESEf));
-    energySE = ESEf - off;
+    // in double in both precisions (a rare branch whose differences cancel in float)
+    const double q = sqrt((double)Eq);
+    const double kz = ((double)deltaE - (double)Eq) / 2. / q;
+    const double kzf = kz + q;
+    const double Ezq = kzf * kzf;
+    double minE = ((double)oFE + (double)bandgap) - Ezq;
+    if (minE < 0.) minE = 0;
+    const double maxE = (double)oFE - (kz * kz);
+    const double r = (double)randoms[3];
+    const double Exy = (minE * (1. - r)) + (maxE * r);
+    const double ESEf = Exy + Ezq;
+    const R th1 = (R)acos(kzf / sqrt(ESEf));
+    energySE = (R)(ESEf - (double)off);
     if ((energySE + ecb) < minGen) return false;
     R nth = R(kPi / 2) - theta, nph = phi + R(kPi);
     update_angles(nth, nph, th1, R(2) * R(kPi) * g.next());

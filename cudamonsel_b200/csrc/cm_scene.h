@@ -95,7 +95,8 @@ struct Msm {
 // NISTMottRS (method 1) per element; the tables live in the precision blob
 struct Mott {
   int Z;
-  int off_spwem, off_x1;     // element offsets into the table blob
+  int off_spwem, off_x1;     // offsets of the cross sections in the table blob (off_x1 unused: -1)
+  int off_x1d;               // offset of the 61 x 201 quantile table in the double copy (mott64)
   double extrapolateBelowEnergy;  // eV
   double sfBrowning;
   double zp17, zp2, zp3;
@@ -125,6 +126,7 @@ struct SceneView {
   const Mott* mott;
   const Table* tables;
   const R* blob;             // table data in compute precision
+  const double* mott64;      // NISTMott quantile tables in double (sampled angles within 1e-6 in FP32 too)
   int chamber;
   int options;               // bit 0: JMONSEL fixes, bit 1: exact CSG in FP32
   int depth;                 // deepest intersection nesting; 0 = every shape is a leaf (plane set or sphere)

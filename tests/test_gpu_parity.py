@@ -8,10 +8,10 @@ Tolerances, written per check:
   FP64 kernels: values within 1e-9 relative (the engine computes in eV/nm, the
     reference in J/m, so results differ by a few ulp), table-window and
     mechanism/element selections identical;
-  FP32 kernels: values within the relative bound stated at each assert
-    (2e-5 for interpolated tables and cross sections, 1e-4 for
-    directions), selections identical except where the reference's value lies
-    within float rounding of a decision boundary (counted, < 0.5 %).
+  FP32 kernels: cross sections, rates, table values, sampled angles, energy
+    losses and SE energies within 1e-6 relative; directions within 1e-6
+    (inelastic) and 5e-6 (elastic, 99.9 %) absolute; selections identical except where the reference's
+    value lies within float rounding of a decision boundary (counted, < 0.5 %).
 The reference's 3-D theta interpolation extrapolates from the first four
 energy nodes (NULagrangeInterpolation.cu:236); its result amplifies rounding
 by up to (E/E3)^3, so directions after such events are compared only where
@@ -123,10 +123,12 @@ def test_nistmott_fp32(lines_engine, oracle_lines, Z):
     rs, rt = oracle_nistmott(b, Z, E, u)
     r = rel(sig, rs)
     print("Z=%d FP32 sigma max rel %.3g" % (Z, r.max()))
-    assert r.max() < 2e-5
+    assert r.max() < 1e-6
     d = np.abs(th - rt) / np.maximum(rt, 1e-6)
     print("Z=%d FP32 theta max rel %.3g, median %.3g" % (Z, d.max(), np.median(d)))
-    assert np.quantile(d, 0.99) < 1e-4 and d.max() < 5e-3
+    for k in np.argsort(d)[-3:]:
+        print("  E %.6g eV u %.6g %.6g theta %.9g ref %.9g" % (E[k] / EV, u[k, 0], u[k, 1], th[k], rt[k]))
+    assert d.max() < 1e-6
 
 
 def oracle_eval(b, fn, args, inp, nout):
@@ -170,11 +172,11 @@ def test_tables(lines_engine, oracle_lines, prec):
             print("table %d prec %d first-window max rel %.3g, extrapolated median rel %.3g" % (
                 t, prec, r[first].max(), np.median(r[~first])))
             assert first.sum() > 20
-            assert r[first].max() < (1e-9 if prec == FP64 else 2e-5)
+            assert r[first].max() < (1e-9 if prec == FP64 else 1e-6)
             assert np.median(r[~first]) < (1e-6 if prec == FP64 else 5e-2)
         else:
             print("table %d prec %d max rel %.3g" % (t, prec, r.max()))
-            assert r.max() < (1e-9 if prec == FP64 else 2e-5)
+            assert r.max() < (1e-9 if prec == FP64 else 1e-6)
 
 
 def tabulated_inputs_and_ref(rows, prec, b, ho):
@@ -203,7 +205,7 @@ def test_tabulated_inelastic(lines_engine, oracle_lines, prec):
     out = e.eval_tabulated(h["si"], 1, inp, prec)
     first = theta_window(b, inp[:, 0] + scenes_eV(13.54)) == 0
     print("cases %d, first-window %d" % (len(inp), first.sum()))
-    tol = 1e-9 if prec == FP64 else 2e-5
+    tol = 1e-9 if prec == FP64 else 1e-6
     r = rel(out[:, 0], ref[:, 0])
     print("prec %d rate max rel %.3g" % (prec, r.max()))
     assert r.max() < tol
@@ -224,25 +226,25 @@ def test_tabulated_inelastic(lines_engine, oracle_lines, prec):
         assert np.quantile(r, 0.999) < 1e-9
     else:
         # in FP32 the loss is read off the float energy E' = E - dE, whose rounding is up to half a
-        # float spacing of E: the bound is 2e-5 of the loss plus one spacing of E
+        # float spacing of E: the bound is 1e-6 of the loss plus one spacing of E
         spacing = np.spacing(np.float32(inp[:, 0] * FROMSI)).astype(np.float64) / FROMSI
-        q = (np.abs(dE1 - dE0) / (2e-5 * np.abs(dE0) + spacing))[ok]
+        q = (np.abs(dE1 - dE0) / (1e-6 * np.abs(dE0) + spacing))[ok]
         print("energy loss error / bound: max %.3g, 99.9%% %.3g" % (q.max(), np.quantile(q, 0.999)))
         assert np.quantile(q, 0.999) < 1.0
     th = rel(out[first, 11], ref[first, 9])
     print("theta (first window) max rel %.3g" % th.max())
-    assert np.quantile(th, 0.999) < (1e-9 if prec == FP64 else 1e-4)
+    assert np.quantile(th, 0.999) < (1e-9 if prec == FP64 else 1e-6)
     se = ok & first & (ref[:, 4] == 1)
     r = rel(out[se, 6], ref[se, 5])
     print("SE energy max rel %.3g over %d" % (r.max(), se.sum()))
-    assert np.quantile(r, 0.999) < (1e-9 if prec == FP64 else 1e-4)
+    assert np.quantile(r, 0.999) < (1e-9 if prec == FP64 else 1e-6)
     tame = ok & first
     err = np.abs(out[:, 2:5] - unit(ref[:, 2], ref[:, 3])).max(axis=1)
     print("PE direction max abs err (first window) %.3g over %d" % (err[tame].max(), tame.sum()))
-    assert np.quantile(err[tame], 0.999) < (1e-7 if prec == FP64 else 1e-3)
+    assert np.quantile(err[tame], 0.999) < (1e-7 if prec == FP64 else 1e-6)
     serr = np.abs(out[:, 7:10] - unit(ref[:, 6], ref[:, 7])).max(axis=1)
     print("SE direction max abs err %.3g over %d" % (serr[se].max(), se.sum()))
-    assert np.quantile(serr[se], 0.999) < (1e-7 if prec == FP64 else 1e-3)
+    assert np.quantile(serr[se], 0.999) < (1e-7 if prec == FP64 else 1e-6)
 
 
 def scenes_eV(x):
@@ -267,13 +269,13 @@ def test_elastic(lines_engine, oracle_lines, mat, prec):
     out = e.eval_elastic(msm, 0, inp, prec)
     r = rel(out[:, 0], ref[:, 0])
     print("mat %d prec %d rate max rel %.3g" % (mat, prec, r.max()))
-    assert r.max() < (1e-9 if prec == FP64 else 2e-5)
+    assert r.max() < (1e-9 if prec == FP64 else 1e-6)
     sameZ = out[:, 4] == ref[:, 3]
     print("element agreement %.5f" % sameZ.mean())
     assert sameZ.all() if prec == FP64 else sameZ.mean() > 0.995
     err = np.abs(out[:, 1:4] - unit(ref[:, 1], ref[:, 2])).max(axis=1)[sameZ]
     print("direction max abs err %.3g, 99.9%% %.3g" % (err.max(), np.quantile(err, 0.999)))
-    assert np.quantile(err, 0.999) < (1e-8 if prec == FP64 else 2e-4)
+    assert np.quantile(err, 0.999) < (1e-8 if prec == FP64 else 5e-6)
     assert (out[:, 5] == ref[:, 4]).all()
 
 
@@ -293,7 +295,7 @@ def test_csd_fitted_polaron(lines_engine, oracle_lines, prec):
     for k, name in enumerate(("csd", "fitted", "polaron")):
         r = rel(out[:, k], ref[:, k])
         print("%s prec %d max rel %.3g, 99.9%% %.3g" % (name, prec, r.max(), np.quantile(r, 0.999)))
-        assert np.quantile(r, 0.999) < (1e-9 if prec == FP64 else 1e-4)
+        assert np.quantile(r, 0.999) < (1e-9 if prec == FP64 else 1e-6)
 
 
 def test_shapes(engine):
@@ -412,7 +414,7 @@ def test_freepath(engine, prec):
     out = engine.eval_freepath(h["si"], inp, prec)
     r = rel(out, ref)
     print("free path prec %d max rel %.3g" % (prec, r.max()))
-    assert r.max() < (1e-9 if prec == FP64 else 2e-5)
+    assert r.max() < (1e-9 if prec == FP64 else 1e-6)
 
 
 def test_random_inputs_against_oracle(lines_engine, oracle_lines):
