@@ -643,8 +643,7 @@ __device__ __forceinline__ void flush_counts(Counters* c, StepCounts& sc) {
   }
 }
 
-template <typename R, int D>
-__global__ void __launch_bounds__(256) k_flight(RunView<R> v, int cur) {
+template <typename R, int D> __device__ __forceinline__ void flight_loop(const RunView<R>& v, int cur) {
   DeviceSink sink;
   StepCounts sc;
   const int n = v.c->n[cur];
@@ -657,6 +656,16 @@ __global__ void __launch_bounds__(256) k_flight(RunView<R> v, int cur) {
   }
   flush_counts(v.c, sc);
 }
+
+// FP64 flight: register-hungry double geometry and physics, compiled without an occupancy target
+template <typename R, int D> __global__ void __launch_bounds__(256) k_flight(RunView<R> v, int cur) {
+  flight_loop<R, D>(v, cur);
+}
+
+// FP32 flight over leaf shapes compiled for 4 resident CTAs per SM (64 registers): the kernel is
+// latency-bound and the extra warps hide more than the spills cost (linescan -3 %, rough image -14 %
+// against 2 CTAs per SM).  Tree walks (D > 0) spill too much at 64 registers and keep k_flight.
+__global__ void __launch_bounds__(256, 4) k_flight32_leaf(RunView<float> v, int cur) { flight_loop<float, 0>(v, cur); }
 
 template <typename R>
 __global__ void __launch_bounds__(256) k_elastic(RunView<R> v, int cur) {
@@ -685,10 +694,16 @@ __global__ void __launch_bounds__(256) k_misc(RunView<R> v, int cur) {
 }
 
 // the kernels are compiled for the intersection nestings 0 (leaf shapes only), 2 and 4
-template <typename R> static void launch_flight(const RunView<R>& v, int cur, int grid, cudaStream_t s) {
-  if (v.s.depth == 0) k_flight<R, 0><<<grid, 256, 0, s>>>(v, cur);
-  else if (v.s.depth <= 2) k_flight<R, 2><<<grid, 256, 0, s>>>(v, cur);
-  else k_flight<R, kMaxShapeDepth><<<grid, 256, 0, s>>>(v, cur);
+static void launch_flight(const RunView<double>& v, int cur, int grid, cudaStream_t s) {
+  if (v.s.depth == 0) k_flight<double, 0><<<grid, 256, 0, s>>>(v, cur);
+  else if (v.s.depth <= 2) k_flight<double, 2><<<grid, 256, 0, s>>>(v, cur);
+  else k_flight<double, kMaxShapeDepth><<<grid, 256, 0, s>>>(v, cur);
+}
+
+static void launch_flight(const RunView<float>& v, int cur, int grid, cudaStream_t s) {
+  if (v.s.depth == 0) k_flight32_leaf<<<grid, 256, 0, s>>>(v, cur);
+  else if (v.s.depth <= 2) k_flight<float, 2><<<grid, 256, 0, s>>>(v, cur);
+  else k_flight<float, kMaxShapeDepth><<<grid, 256, 0, s>>>(v, cur);
 }
 
 template <typename R> static void launch_misc(const RunView<R>& v, int cur, int grid, cudaStream_t s) {
@@ -830,7 +845,7 @@ static int run_device_once(cm_context* ctx, const cm_run_desc* d, uint32_t* back
   for (int it = 0; it < 2 * K; ++it) {
     const int cur = it & 1;
     cudaEvent_t* ev = d->profile ? &pev[(size_t)it * 6 + 1] : nullptr;
-    launch_flight<R>(v, cur, grid, stream);
+    launch_flight(v, cur, grid, stream);
     if (ev) cudaEventRecordWithFlags(ev[0], stream, cudaEventRecordExternal);
     k_elastic<R><<<grid, 256, 0, stream>>>(v, cur);
     if (ev) cudaEventRecordWithFlags(ev[1], stream, cudaEventRecordExternal);
@@ -2020,7 +2035,7 @@ static int run_noalloc(cm_context* ctx, const cm_run_desc* d, uint32_t* back, ui
   for (;;) {
     for (int k = 0; k < 16; ++k, ++it) {
       const int cur = it & 1;
-      launch_flight<R>(v, cur, grid, s);
+      launch_flight(v, cur, grid, s);
       k_elastic<R><<<grid, 256, 0, s>>>(v, cur);
       k_inelastic<R><<<grid, 256, 0, s>>>(v, cur);
       launch_misc<R>(v, cur, grid, s);
