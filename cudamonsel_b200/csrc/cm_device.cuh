@@ -1045,15 +1045,40 @@ CM_D bool segment_meets_box(const double* bb, const double* p0, const double* p1
 }
 
 // RegionBase.cu:50-60, iterative: the first child whose shape holds p owns it
+// the first child of r (in list order) whose shape holds p, or -1
+template <typename R, int D> CM_D int first_child_holding(const SceneView<R>& s, const Region& r, const double* p) {
+  if (r.grid < 0) {
+    for (int i = 0; i < r.nchild; ++i) {
+      const int c = s.children[r.child0 + i];
+      if (point_in_box(s.regions[c].bb, p) && shape_contains<R, D>(s, s.regions[c].shape, p)) return c;
+    }
+    return -1;
+  }
+  // the cell's children and the unbounded ones, merged in list order
+  const ChildGrid& g = s.grids[r.grid];
+  int a = 0, na = 0;
+  const double fx = floor((p[0] - g.x0) / g.dx), fy = floor((p[1] - g.y0) / g.dy);
+  if (fx >= 0.0 && fy >= 0.0 && fx < (double)g.nx && fy < (double)g.ny) {
+    const int cell = g.cell0 + (int)fy * g.nx + (int)fx;
+    a = s.cell_start[cell];
+    na = s.cell_start[cell + 1] - a;
+  }
+  const int b = g.unb0, nb = g.nunb;
+  int ia = 0, ib = 0;
+  while (ia < na || ib < nb) {
+    int pos;
+    if (ib >= nb || (ia < na && s.grid_items[a + ia] < s.grid_items[b + ib])) pos = s.grid_items[a + ia++];
+    else pos = s.grid_items[b + ib++];
+    const int c = s.children[r.child0 + pos];
+    if (point_in_box(s.regions[c].bb, p) && shape_contains<R, D>(s, s.regions[c].shape, p)) return c;
+  }
+  return -1;
+}
+
 template <typename R, int D = kMaxShapeDepth> CM_D int containing_subregion(const SceneView<R>& s, int reg, const double* p) {
   if (!shape_contains<R, D>(s, s.regions[reg].shape, p)) return -1;
   for (int depth = 0; depth < 64; ++depth) {
-    const Region& r = s.regions[reg];
-    int found = -1;
-    for (int i = 0; i < r.nchild; ++i) {
-      const int c = s.children[r.child0 + i];
-      if (point_in_box(s.regions[c].bb, p) && shape_contains<R, D>(s, s.regions[c].shape, p)) { found = c; break; }
-    }
+    const int found = first_child_holding<R, D>(s, s.regions[reg], p);
     if (found < 0) return reg;
     reg = found;
   }
@@ -1081,14 +1106,77 @@ CM_D int find_end_of_step(const SceneView<R>& s, int reg, const double* p0, doub
   double t = nv.u;
   hitn[0] = nv.n[0]; hitn[1] = nv.n[1]; hitn[2] = nv.n[2];
   if ((t <= 1.0) && r.parent >= 0) base = r.parent;
-  for (int i = 0; i < r.nchild; ++i) {
-    const int c = s.children[r.child0 + i];
-    if (!segment_meets_box(s.regions[c].bb, p0, p1)) continue;
-    NV cn = shape_first_normal<R, D>(s, s.regions[c].shape, p0, p1);
-    if ((cn.u <= 1.0) && (cn.u < t)) {
-      t = cn.u;
-      base = c;
-      hitn[0] = cn.n[0]; hitn[1] = cn.n[1]; hitn[2] = cn.n[2];
+  if (r.grid < 0) {
+    for (int i = 0; i < r.nchild; ++i) {
+      const int c = s.children[r.child0 + i];
+      if (!segment_meets_box(s.regions[c].bb, p0, p1)) continue;
+      NV cn = shape_first_normal<R, D>(s, s.regions[c].shape, p0, p1);
+      if ((cn.u <= 1.0) && (cn.u < t)) {
+        t = cn.u;
+        base = c;
+        hitn[0] = cn.n[0]; hitn[1] = cn.n[1]; hitn[2] = cn.n[2];
+      }
+    }
+  } else {
+    // the in-order scan keeps the first child of smallest u below the region's own crossing:
+    // here children come cell by cell, so ties go to the lower list position explicitly
+    int bpos = 0x7fffffff;
+    auto visit = [&](int pos) {
+      const int c = s.children[r.child0 + pos];
+      if (!segment_meets_box(s.regions[c].bb, p0, p1)) return;
+      NV cn = shape_first_normal<R, D>(s, s.regions[c].shape, p0, p1);
+      if ((cn.u <= 1.0) && ((cn.u < t) || (cn.u == t && bpos != 0x7fffffff && pos < bpos))) {
+        t = cn.u;
+        base = c;
+        bpos = pos;
+        hitn[0] = cn.n[0]; hitn[1] = cn.n[1]; hitn[2] = cn.n[2];
+      }
+    };
+    const ChildGrid& g = s.grids[r.grid];
+    for (int k = 0; k < g.nunb; ++k) visit(s.grid_items[g.unb0 + k]);
+    // cells crossed by the step's x-y projection, in order along the step, until past the best crossing
+    const double ex = p1[0] - p0[0], ey = p1[1] - p0[1];
+    const double X1 = g.x0 + g.nx * g.dx, Y1 = g.y0 + g.ny * g.dy;
+    double tlo = 0.0, thi = 1.0;
+    bool hit = true;
+    if (ex == 0.0) hit = p0[0] >= g.x0 && p0[0] <= X1;
+    else {
+      double a0 = (g.x0 - p0[0]) / ex, a1 = (X1 - p0[0]) / ex;
+      if (a0 > a1) { const double q = a0; a0 = a1; a1 = q; }
+      tlo = a0 > tlo ? a0 : tlo;
+      thi = a1 < thi ? a1 : thi;
+    }
+    if (ey == 0.0) hit = hit && p0[1] >= g.y0 && p0[1] <= Y1;
+    else {
+      double a0 = (g.y0 - p0[1]) / ey, a1 = (Y1 - p0[1]) / ey;
+      if (a0 > a1) { const double q = a0; a0 = a1; a1 = q; }
+      tlo = a0 > tlo ? a0 : tlo;
+      thi = a1 < thi ? a1 : thi;
+    }
+    if (hit && tlo <= thi) {
+      int ix = (int)floor((p0[0] + tlo * ex - g.x0) / g.dx), iy = (int)floor((p0[1] + tlo * ey - g.y0) / g.dy);
+      ix = ix < 0 ? 0 : (ix >= g.nx ? g.nx - 1 : ix);
+      iy = iy < 0 ? 0 : (iy >= g.ny ? g.ny - 1 : iy);
+      const int sx = ex > 0.0 ? 1 : (ex < 0.0 ? -1 : 0), sy = ey > 0.0 ? 1 : (ey < 0.0 ? -1 : 0);
+      double tx = sx == 0 ? INFINITY : ((g.x0 + (ix + (sx > 0 ? 1 : 0)) * g.dx) - p0[0]) / ex;
+      double ty = sy == 0 ? INFINITY : ((g.y0 + (iy + (sy > 0 ? 1 : 0)) * g.dy) - p0[1]) / ey;
+      const double dtx = sx == 0 ? INFINITY : g.dx / fabs(ex), dty = sy == 0 ? INFINITY : g.dy / fabs(ey);
+      double tentry = tlo;
+      for (int guard = 0; guard < g.nx + g.ny + 2; ++guard) {
+        if (tentry > thi || (t <= 1.0 && tentry > t)) break;
+        const int cell = g.cell0 + iy * g.nx + ix;
+        for (int k = s.cell_start[cell]; k < s.cell_start[cell + 1]; ++k) visit(s.grid_items[k]);
+        if (tx < ty) {
+          ix += sx;
+          tentry = tx;
+          tx += dtx;
+        } else {
+          iy += sy;
+          tentry = ty;
+          ty += dty;
+        }
+        if (ix < 0 || iy < 0 || ix >= g.nx || iy >= g.ny) break;
+      }
     }
   }
   if (clipped) *clipped = t <= 1.0;

@@ -342,6 +342,28 @@ static Box shape_box(cm_context* ctx, int id) {
       return b;
     case SHAPE_INTERSECTION:
     case SHAPE_UNION: {
+      if (s.kind == SHAPE_INTERSECTION) {
+        // an intersection of plane sets is one convex polytope: box its vertices, which is far
+        // tighter than intersecting the boxes of slanted half-spaces (a sidewall alone spans the world)
+        HShape all;
+        all.kind = SHAPE_PLANES;
+        std::vector<int> todo{id};
+        bool planar = true;
+        while (!todo.empty() && planar) {
+          const HShape& h = ctx->shapes[todo.back()];
+          todo.pop_back();
+          if (h.kind == SHAPE_INTERSECTION) {
+            todo.push_back(h.a);
+            todo.push_back(h.b);
+          } else if (h.kind == SHAPE_PLANES) {
+            all.n.insert(all.n.end(), h.n.begin(), h.n.end());
+            all.p.insert(all.p.end(), h.p.begin(), h.p.end());
+          } else {
+            planar = false;
+          }
+        }
+        if (planar) return planes_box(all);
+      }
       const Box x = shape_box(ctx, s.a), y = shape_box(ctx, s.b);
       for (int a = 0; a < 3; ++a) {
         b.lo[a] = s.kind == SHAPE_UNION ? std::min(x.lo[a], y.lo[a]) : std::max(x.lo[a], y.lo[a]);
@@ -574,7 +596,58 @@ static int build_scene(cm_context* ctx, DevScene<R>& ds) {
       r.bb[3 + a] = bx.hi[a] >= kBoxWorld * 0.999 ? INFINITY : bx.hi[a] * 1e9 + pad;
     }
     for (int c : hr.children) children.push_back(c);
+    r.grid = -1;
     regions.push_back(r);
+  }
+  // grids over the children of regions with many of them (a rough-line layout: hundreds of segments)
+  std::vector<ChildGrid> grids;
+  std::vector<int> cell_start, grid_items;
+  for (Region& r : regions) {
+    if (r.nchild < kGridMinChildren || (ctx->options & CM_OPT_SCAN_CHILDREN)) continue;
+    std::vector<int> bounded, unbounded;
+    double lo[2] = {INFINITY, INFINITY}, hi[2] = {-INFINITY, -INFINITY};
+    for (int i = 0; i < r.nchild; ++i) {
+      const double* bb = regions[children[r.child0 + i]].bb;
+      if (std::isinf(bb[0]) || std::isinf(bb[1]) || std::isinf(bb[3]) || std::isinf(bb[4]) || bb[0] > bb[3] ||
+          bb[1] > bb[4]) {
+        unbounded.push_back(i);
+        continue;
+      }
+      bounded.push_back(i);
+      for (int a = 0; a < 2; ++a) {
+        lo[a] = std::min(lo[a], bb[a]);
+        hi[a] = std::max(hi[a], bb[3 + a]);
+      }
+    }
+    if ((int)bounded.size() < kGridMinChildren) continue;
+    ChildGrid g;
+    const double wx = std::max(hi[0] - lo[0], 1e-3), wy = std::max(hi[1] - lo[1], 1e-3);
+    const double cells = std::min(65536.0, std::max(16.0, 2.0 * bounded.size()));
+    g.nx = std::max(1, std::min(4096, (int)ceil(sqrt(cells * wx / wy))));
+    g.ny = std::max(1, std::min(4096, (int)ceil(cells / g.nx)));
+    g.x0 = lo[0];
+    g.y0 = lo[1];
+    g.dx = wx / g.nx;
+    g.dy = wy / g.ny;
+    std::vector<std::vector<int>> lists((size_t)g.nx * g.ny);
+    for (int i : bounded) {  // ascending positions, so every cell list is ascending
+      const double* bb = regions[children[r.child0 + i]].bb;
+      const int ix0 = std::max(0, (int)floor((bb[0] - g.x0) / g.dx)), ix1 = std::min(g.nx - 1, (int)floor((bb[3] - g.x0) / g.dx));
+      const int iy0 = std::max(0, (int)floor((bb[1] - g.y0) / g.dy)), iy1 = std::min(g.ny - 1, (int)floor((bb[4] - g.y0) / g.dy));
+      for (int iy = iy0; iy <= iy1; ++iy)
+        for (int ix = ix0; ix <= ix1; ++ix) lists[(size_t)iy * g.nx + ix].push_back(i);
+    }
+    g.cell0 = (int)cell_start.size();
+    for (auto& l : lists) {
+      cell_start.push_back((int)grid_items.size());
+      grid_items.insert(grid_items.end(), l.begin(), l.end());
+    }
+    cell_start.push_back((int)grid_items.size());
+    g.unb0 = (int)grid_items.size();
+    g.nunb = (int)unbounded.size();
+    grid_items.insert(grid_items.end(), unbounded.begin(), unbounded.end());
+    r.grid = (int)grids.size();
+    grids.push_back(g);
   }
   SceneView<R>& v = ds.view;
   int rc = 0;
@@ -583,7 +656,9 @@ static int build_scene(cm_context* ctx, DevScene<R>& ds) {
       (rc = dev_copy(ds.allocs, regions, &v.regions, h)) || (rc = dev_copy(ds.allocs, children, &v.children, h)) ||
       (rc = dev_copy(ds.allocs, msms, &v.msms, h)) || (rc = dev_copy(ds.allocs, mechs, &v.mechs, h)) ||
       (rc = dev_copy(ds.allocs, motts, &v.mott, h)) || (rc = dev_copy(ds.allocs, tabs, &v.tables, h)) ||
-      (rc = dev_copy(ds.allocs, blob, &v.blob, h)) || (rc = dev_copy(ds.allocs, mott64, &v.mott64, h)))
+      (rc = dev_copy(ds.allocs, blob, &v.blob, h)) || (rc = dev_copy(ds.allocs, mott64, &v.mott64, h)) ||
+      (rc = dev_copy(ds.allocs, grids, &v.grids, h)) || (rc = dev_copy(ds.allocs, cell_start, &v.cell_start, h)) ||
+      (rc = dev_copy(ds.allocs, grid_items, &v.grid_items, h)))
     return rc;
   v.chamber = 0;
   v.options = ctx->options;

@@ -13,6 +13,7 @@ constexpr int kMaxMech = 8;
 constexpr int kMaxElem = 8;
 constexpr int kMaxCore = 16;
 constexpr int kMaxShapeDepth = 4;
+constexpr int kGridMinChildren = 24;  // regions with at least this many bounded children get a ChildGrid
 
 // NISTMonte/MonteCarloSS.cu:32-33 in nm
 constexpr double kChamberRadiusNm = 0.1e9;
@@ -43,6 +44,18 @@ struct Region {
   int child0, nchild;  // children indices in Scene::children
   int cls;             // wave segment of electrons in this region (by material model)
   double bb[6];        // axis-aligned box holding the region's shape (nm): min xyz, max xyz
+  int grid;            // index of the grid over this region's children, -1: scan them in order
+};
+
+// A uniform x-y grid over the children of a region with many of them.  Each cell lists, ascending,
+// the positions (in the region's child list) of the children whose box overlaps it; children whose
+// box is unbounded in x or y are listed once apart.  Searches visit only the listed children and
+// resolve ties by position, so they find what the in-order scan finds.
+struct ChildGrid {
+  double x0, y0, dx, dy;  // nm
+  int nx, ny;
+  int cell0;              // cell (ix, iy) lists grid_items[cell_start[cell0 + iy * nx + ix] .. next)
+  int unb0, nunb;         // the unbounded children: grid_items[unb0 .. unb0 + nunb)
 };
 
 // electrons are kept in one wave segment per material class, so that the
@@ -125,6 +138,9 @@ struct SceneView {
   const Mech* mechs;
   const Mott* mott;
   const Table* tables;
+  const ChildGrid* grids;
+  const int* cell_start;
+  const int* grid_items;
   const R* blob;             // table data in compute precision
   const double* mott64;      // NISTMott quantile tables in double (sampled angles within 1e-6 in FP32 too)
   int chamber;

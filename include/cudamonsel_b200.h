@@ -44,6 +44,8 @@ extern "C" {
 #define CM_OPT_JMONSEL_FIXES 1 /* refraction at barriers, d3 abscissae; default is the reference as written */
 #define CM_OPT_EXACT_CSG 2     /* FP32 too walks NormalIntersectionShape trees as the reference does; by default
                                   FP32 merges intersections of plane sets into single plane sets */
+#define CM_OPT_SCAN_CHILDREN 4 /* test every child of a region in order, as RegionBase does; by default a region
+                                  with many children finds them through an x-y grid (same results) */
 
 typedef struct cm_context cm_context;
 

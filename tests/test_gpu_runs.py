@@ -203,6 +203,26 @@ def test_rough_lines_match_oracle(rough_oracle_runs, prec):
         assert abs(zb) < 3.5 and abs(zs) < 3.5
 
 
+@pytest.mark.parametrize("prec", [FP64, FP32], ids=["fp64", "fp32"])
+def test_child_grid_finds_what_the_scan_finds(prec):
+    """The rough-line chamber (385 children) searched through its x-y grid and by the in-order scan
+    (CM_OPT_SCAN_CHILDREN) gives identical tallies on a 24 x 24 image at 300-1000 eV."""
+    from cudamonsel_b200 import capi, scenes
+    ic, ie, inp, inb = scenes.rough_image(seed=2, side=24, mean_nprim=150)
+    keys = np.arange(len(ic), dtype=np.uint64) + np.uint64(99)
+    out = []
+    for opt in (0, 4):
+        e = capi.Engine(0)
+        sc = scenes.rough_lines(seed=2)
+        sc.spec.options = opt
+        h = scenes.build_engine(sc, e)
+        back, fwd, st = e.run(h["chamber"], ic, ie, inp, inb, 1e-9, 0, precision=prec, pixel_keys=keys)
+        e.close()
+        out.append((back, fwd, st.steps))
+    assert out[0][2] == out[1][2]
+    assert (out[0][0] == out[1][0]).all() and (out[0][1] == out[1][1]).all()
+
+
 def test_deterministic_and_independent_of_batch(half):
     """Same seed -> identical tallies; a pixel's tally is the same alone and inside a larger
     batch of other pixels when it carries the same stream key (the serving guarantee)."""
