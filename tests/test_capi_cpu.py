@@ -62,3 +62,24 @@ def test_yields_histogram_convention():
     bse, se = scenes.yields(back, 10, 1000.0, 100)
     assert abs(se[0] - 1.5) < 1e-7
     assert abs(bse[0] - (25 / 10 - 1.5)) < 1e-7
+
+
+def test_scan_output_format(tmp_path):
+    """The scan read-out writes LinesOnLayers' output.txt layout (std::to_string numbers) and PGM images."""
+    import numpy as np
+    from cudamonsel_b200 import scan
+    assert scan.to_string(500.0) == "500.000000" and scan.to_string(3) == "3"
+    txt = scan.output_text([(500.0, -1.5, 0.0, 0.1245, 2.335)], ["# Trajectories at each landing position: 100"],
+                           12.5)
+    assert txt == ("\n# Trajectories at each landing position: 100\n\nbeamE (eV)\tx(nm)\ty (nm)\tBSE yield\tSE yield"
+                   "\n500.000000 -1.500000 0.000000 0.124500 2.335000\n12.500000")
+    # yields from a histogram: 10 eV bins of a 500 eV beam, SE = bins below 50 eV
+    back = np.zeros((1, 52), dtype=np.int64)
+    back[0, 1:6] = 10     # 50 SE (bins 0..4)
+    back[0, 30] = 20      # 20 BSE
+    rows = scan.scan_rows(back, [[1e-9, 2e-9, -120e-9]], 500.0, 100, 50)
+    assert abs(rows[0][3] - 0.2) < 1e-6 and abs(rows[0][4] - 0.5) < 1e-6 and abs(rows[0][1] - 1.0) < 1e-9
+    img = np.arange(12, dtype=float).reshape(3, 4)
+    scan.write_pgm(tmp_path / "a.pgm", img)
+    g = scan.read_pgm(tmp_path / "a.pgm")
+    assert g.shape == (3, 4) and g[0, 0] == 0 and g[2, 3] == 255
