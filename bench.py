@@ -172,6 +172,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-serving", action="store_true", help="skip the served-stream latency measurement")
     ap.add_argument("--no-image", action="store_true", help="skip the rough-line image (FP32 vs FP64)")
+    ap.add_argument("--no-deep", action="store_true", help="skip the 10 keV deep-penetration layout")
     ap.add_argument("--profile-run", action="store_true",
                     help="run one FP32 step of the workload and exit (the case for ncu captures)")
     a = ap.parse_args()
@@ -335,6 +336,47 @@ def main():
                       "electron_steps_fp32": int(runs["fp32"][1].steps),
                       "yield_error_vs_fp64": err}
 
+    # deep penetration: 16 x 16 seed-placed blocks and cylinders (PMMA or Si, 20-300 nm) on Si, 10 keV,
+    # a 64 x 64 scan at 80 nm over the 5.12 um layout, 100 primaries per pixel, FP32 against FP64
+    deep_line = None
+    if not a.no_deep:
+        dsc, dtop = scenes.deep_features(seed=0)
+        edeep = capi.Engine(local)
+        hd = scenes.build_engine(dsc, edeep)
+        side, step = 64, 80e-9
+        xs = (np.arange(side) - (side - 1) / 2.0) * step
+        gx, gy = np.meshgrid(xs, xs)
+        dc = np.stack([gx.ravel(), gy.ravel(), np.full(side * side, -(dtop + 20e-9))], axis=1)
+        dkeys = np.arange(side * side, dtype=np.uint64) + np.uint64(5_000_011 * (rank + 1))
+        druns = {}
+        for name, pr in (("fp32", capi.PREC_FP32), ("fp64", capi.PREC_FP64)):
+            db, _, dst = edeep.run(hd["chamber"], dc, scenes.eV(10000.0), 100, 1000, 1e-9, 0, precision=pr,
+                                   pixel_keys=dkeys)
+            druns[name] = (db, dst)
+        edeep.close()
+        y32 = scenes.yields(druns["fp32"][0].astype(np.int64), 100, 10000.0, 1000)
+        y64 = scenes.yields(druns["fp64"][0].astype(np.int64), 100, 10000.0, 1000)
+        nd = side * side * 100
+        deep_line = {"workload": "16 x 16 blocks/cylinders (PMMA or Si, 20-300 nm) on Si, 10 keV, 64 x 64 px at "
+                                 "80 nm, 100 primaries/px", "primaries": nd,
+                     "fp32_primaries_per_s": nd / (druns["fp32"][1].device_ms / 1e3),
+                     "fp64_primaries_per_s": nd / (druns["fp64"][1].device_ms / 1e3),
+                     "fp32_over_fp64": druns["fp64"][1].device_ms / druns["fp32"][1].device_ms,
+                     "electron_steps_fp32": int(druns["fp32"][1].steps),
+                     "yield_error_map_vs_fp64": {
+                         "bse_mean_abs": float(np.abs(y32[0] - y64[0]).mean()),
+                         "bse_max_abs": float(np.abs(y32[0] - y64[0]).max()),
+                         "se_mean_abs": float(np.abs(y32[1] - y64[1]).mean()),
+                         "se_max_abs": float(np.abs(y32[1] - y64[1]).max()),
+                         "bse_image_mean_rel_err": float(abs(y32[0].mean() - y64[0].mean()) / y64[0].mean()),
+                         "se_image_mean_rel_err": float(abs(y32[1].mean() - y64[1].mean()) / y64[1].mean()),
+                         # at 10 keV the FP32 and FP64 trajectories decorrelate after a few hundred steps, so
+                         # the difference is statistical: z = difference / combined standard error of the means
+                         "bse_image_mean_z": float((y32[0].mean() - y64[0].mean()) / np.sqrt(
+                             (y32[0].var(ddof=1) + y64[0].var(ddof=1)) / y32[0].size)),
+                         "se_image_mean_z": float((y32[1].mean() - y64[1].mean()) / np.sqrt(
+                             (y32[1].var(ddof=1) + y64[1].var(ddof=1)) / y32[1].size))}}
+
     # served stream: random scan jobs (1-8 lines/cylinders on Si, 200-5000 eV, images or linescans) at
     # Poisson arrivals through the job server, sizes scaled by SERVE_SCALE; p50/p99 of submit-to-done latency
     serving_line = None
@@ -376,7 +418,7 @@ def main():
                 "clocks": clk, "gpu_launches": launches,
                 "e2e": {"value": e2e_value, "unit": "primaries/s", "h2d_bytes_per_step": h2d,
                         "d2h_bytes_per_step": d2h},
-                "cpu_baseline": cpu, "serving": serving_line, "image": image_line}
+                "cpu_baseline": cpu, "serving": serving_line, "image": image_line, "deep": deep_line}
         print(json.dumps(line), flush=True)
     eng.close()
     if world > 1:

@@ -270,6 +270,58 @@ def rough_image(seed=0, side=256, step=2e-9, mean_nprim=300, energies_eV=(300.0,
     return centers, eV(e_eV), nprim, nbins
 
 
+def deep_features(seed=0, cells=16, cell=320e-9, tables=None):
+    """The deep-penetration layout: a Si substrate carrying cells x cells seed-placed features, one per
+    cell of a square grid of pitch `cell` centred on the origin; each is PMMA or Si, a block
+    (6-plane NormalMultiPlaneShape) or a cylinder lying along x or y, with sizes ~U(20, 300) nm.
+    Cylinders are built with their axis normalised (the reference's as-compiled cylinders are never
+    struck)."""
+    rng = np.random.default_rng(seed)
+    s = SceneSpec()
+    vac = vacuum(s)
+    si = silicon(s, tables)
+    pm = pmma(s)
+    chamber = s.region(None, vac, s.sphere([0.0, 0.0, 0.0], 0.1))
+    surf = s.planes([0.0, 0.0, -1.0], [0.0, 0.0, 0.0])
+    sireg = s.region(chamber, si, surf)
+    feats = []
+    half = cells * cell / 2.0
+    top = 0.0
+    for iy in range(cells):
+        for ix in range(cells):
+            cx = -half + (ix + 0.5) * cell
+            cy = -half + (iy + 0.5) * cell
+            msm = pm if rng.random() < 0.5 else si
+            size = rng.uniform(20e-9, 300e-9, 3)
+            size[:2] = np.minimum(size[:2], cell - 10e-9)
+            if rng.random() < 0.5:
+                hw = size / 2.0
+                c = (cx, cy, -hw[2])
+                n, p = [], []
+                for a in range(3):
+                    for sg in (-1.0, 1.0):
+                        nn = [0.0, 0.0, 0.0]
+                        pp = list(c)
+                        nn[a] = sg
+                        pp[a] += sg * hw[a]
+                        n += nn
+                        p += pp
+                shp = s.planes(n, p)
+                top = max(top, size[2])
+            else:
+                r = min(size[0], cell - 10e-9) / 2.0
+                ln = min(size[1], cell - 10e-9)
+                s.set_options(1)
+                if rng.random() < 0.5:
+                    shp = s.cylinder([cx - ln / 2, cy, -r], [cx + ln / 2, cy, -r], r)
+                else:
+                    shp = s.cylinder([cx, cy - ln / 2, -r], [cx, cy + ln / 2, -r], r)
+                s.set_options(0)
+                top = max(top, 2 * r)
+            feats.append(s.region(chamber, msm, shp))
+    return Scene(s, chamber, vac=vac, si=si, pmma=pm, si_region=sireg, features=feats), top
+
+
 def features(options=1, tables=None):
     """Si substrate carrying a PMMA cylinder lying along y (radius 30 nm, axis at x = -60 nm, z = -30 nm), a
     rounded PMMA line (NShapes::createLine, corner radii 10 nm, centred at x = +60 nm) and a Si block.

@@ -223,6 +223,33 @@ def test_child_grid_finds_what_the_scan_finds(prec):
     assert (out[0][0] == out[1][0]).all() and (out[0][1] == out[1][1]).all()
 
 
+@pytest.mark.parametrize("prec", [FP64, FP32], ids=["fp64", "fp32"])
+def test_deep_features_match_oracle(prec):
+    """4 x 4 seed-placed blocks and cylinders on Si at 10 keV: engine vs oracle at 4 landing points."""
+    import pyoracle
+    from cudamonsel_b200 import capi, scenes
+    sc, top = scenes.deep_features(seed=3, cells=4, cell=320e-9)
+    xs = np.array([-480.0, -160.0, 160.0, 480.0]) * 1e-9
+    centers = np.stack([xs, np.array([-160.0, 160.0, -160.0, 160.0]) * 1e-9, np.full(4, -(top + 20e-9))], axis=1)
+    ob, of, tl = pyoracle.run_scene(sc, centers, 1e-9, scenes.eV(10000.0), 400, 17, 1000)
+    e = capi.Engine(0)
+    h = scenes.build_engine(sc, e)
+    npix_rep, nprim = 16, 100
+    back, fwd, st = e.run(h["chamber"], np.repeat(centers, npix_rep, axis=0), scenes.eV(10000.0), nprim, 1000, 1e-9,
+                          seed=23, precision=prec)
+    e.close()
+    for i in range(len(centers)):
+        eb, es = batch_yields(back[i * npix_rep:(i + 1) * npix_rep], nprim, 10000.0, 1000)
+        rb, rs = batch_yields(ob[i:i + 1], 400, 10000.0, 1000)
+        se_b = eb.std(ddof=1) * np.sqrt(1.0 / npix_rep + 1.0 / 4)
+        se_s = es.std(ddof=1) * np.sqrt(1.0 / npix_rep + 1.0 / 4)
+        zb = (eb.mean() - rb[0]) / max(se_b, 1e-12)
+        zs = (es.mean() - rs[0]) / max(se_s, 1e-12)
+        print("x=%6.1f nm BSE %.4f/%.4f z=%.2f SE %.4f/%.4f z=%.2f" % (xs[i] * 1e9, eb.mean(), rb[0], zb, es.mean(),
+                                                                    rs[0], zs))
+        assert abs(zb) < 3.5 and abs(zs) < 3.5
+
+
 def test_deterministic_and_independent_of_batch(half):
     """Same seed -> identical tallies; a pixel's tally is the same alone and inside a larger
     batch of other pixels when it carries the same stream key (the serving guarantee)."""
