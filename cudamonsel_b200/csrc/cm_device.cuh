@@ -304,6 +304,19 @@ template <typename R> CM_D R nu_d1_4(const R* fv, const R* xv, R x) {
   return nu_neville3(fv, xv, nearest - first, x);
 }
 
+// Lagrange weights of the cubic through the 4 abscissae xv at x.  d2 and d3 evaluate many cubics on
+// the same abscissae at the same point (every row of a window), so the weights are formed once and
+// each row is a 4-term dot product instead of a Neville tableau; the value is the same polynomial.
+template <typename R> CM_D void lag4(const R* xv, R x, R w[4]) {
+  const R d0 = x - xv[0], d1 = x - xv[1], d2 = x - xv[2], d3 = x - xv[3];
+  w[0] = (d1 * d2 * d3) / ((xv[0] - xv[1]) * (xv[0] - xv[2]) * (xv[0] - xv[3]));
+  w[1] = (d0 * d2 * d3) / ((xv[1] - xv[0]) * (xv[1] - xv[2]) * (xv[1] - xv[3]));
+  w[2] = (d0 * d1 * d3) / ((xv[2] - xv[0]) * (xv[2] - xv[1]) * (xv[2] - xv[3]));
+  w[3] = (d0 * d1 * d2) / ((xv[3] - xv[0]) * (xv[3] - xv[1]) * (xv[3] - xv[2]));
+}
+
+template <typename R> CM_D R dot4(const R w[4], const R* f) { return w[0] * f[0] + w[1] * f[1] + w[2] * f[2] + w[3] * f[3]; }
+
 // NULagrangeInterpolation.cu:169-192 on a 2-D table (order 3)
 template <typename R> CM_D R nu_d2(const R* f, const R* xs0, int n0, const R* xs1, int n1, R xa, R xb) {
   int i0, near0;
@@ -311,15 +324,15 @@ template <typename R> CM_D R nu_d2(const R* f, const R* xs0, int n0, const R* xs
   int j0, near1;
   nu_locate(xb, xs1, n1, 3, j0, near1);
   R xv1[4] = {xs1[j0], xs1[j0 + 1], xs1[j0 + 2], xs1[j0 + 3]};
+  R w1[4];
+  lag4(xv1, xb, w1);
   R y[4];
 #pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    const R* row = f + (size_t)(i0 + i) * n1 + j0;
-    R fv[4] = {row[0], row[1], row[2], row[3]};
-    y[i] = nu_neville3(fv, xv1, near1 - j0, xb);
-  }
+  for (int i = 0; i < 4; ++i) y[i] = dot4(w1, f + (size_t)(i0 + i) * n1 + j0);
   R xv0[4] = {xs0[i0], xs0[i0 + 1], xs0[i0 + 2], xs0[i0 + 3]};
-  return nu_d1_4(y, xv0, xa);
+  R w0[4];
+  lag4(xv0, xa, w0);
+  return dot4(w0, y);
 }
 
 // NULagrangeInterpolation.cu:215-240 on a 3-D table (order 3).  The reference's
@@ -333,21 +346,22 @@ template <typename R> CM_D R nu_d3(const R* f, const R* xs0, int n0, const R* xs
   nu_locate(xc, xs2, n2, 3, k0, near2);
   R xv1[4] = {xs1[j0], xs1[j0 + 1], xs1[j0 + 2], xs1[j0 + 3]};
   R xv2[4] = {xs2[k0], xs2[k0 + 1], xs2[k0 + 2], xs2[k0 + 3]};
+  R w1[4], w2[4];
+  lag4(xv1, xb, w1);
+  lag4(xv2, xc, w2);
   R y[4];
 #pragma unroll
   for (int i = 0; i < 4; ++i) {
     R z[4];
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      const R* row = f + ((size_t)(i0 + i) * n1 + (j0 + j)) * n2 + k0;
-      R fv[4] = {row[0], row[1], row[2], row[3]};
-      z[j] = nu_neville3(fv, xv2, near2 - k0, xc);
-    }
-    y[i] = nu_d1_4(z, xv1, xb);
+    for (int j = 0; j < 4; ++j) z[j] = dot4(w2, f + ((size_t)(i0 + i) * n1 + (j0 + j)) * n2 + k0);
+    y[i] = dot4(w1, z);
   }
   const int base = fixes ? i0 : 0;
   R xv0[4] = {xs0[base], xs0[base + 1], xs0[base + 2], xs0[base + 3]};
-  return nu_d1_4(y, xv0, xa);
+  R w0[4];
+  lag4(xv0, xa, w0);
+  return dot4(w0, y);
 }
 
 // NUTableInterpolation::interpolate (JMONSEL/NUTableInterpolation.cu:98-115)
