@@ -112,7 +112,7 @@ def load(path=LIBPATH):
         "cm_job_wait": [C.c_void_p, C.c_int, C.c_double, C.POINTER(JobInfo)],
         "cm_job_cancel": [C.c_void_p, C.c_int],
         "cm_job_result": [C.c_void_p, C.c_int, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.POINTER(RunStats)],
-        "cm_eval_nistmott": [ctx, C.c_int, C.c_int, d, d, d, d, C.c_int],
+        "cm_eval_nistmott": [ctx, C.c_int, C.c_int, C.c_int, d, d, d, d, C.c_int],
         "cm_eval_table": [ctx, C.c_int, C.c_int, d, C.c_int, d, C.c_int],
         "cm_eval_tabulated": [ctx, C.c_int, C.c_int, C.c_int, d, d, C.c_int],
         "cm_eval_elastic": [ctx, C.c_int, C.c_int, C.c_int, d, d, C.c_int],
@@ -292,12 +292,12 @@ class Engine:
         return st
 
     # ---- per-function entry points
-    def eval_nistmott(self, Z, E, u, precision=PREC_FP64):
+    def eval_nistmott(self, Z, E, u, precision=PREC_FP64, method=1):
         E, pE = _d(E)
         u, pu = _d(u)
         s = np.zeros(len(E))
         t = np.zeros(len(E))
-        self._check(self.L.cm_eval_nistmott(self.h, Z, len(E), pE, pu, s.ctypes.data_as(C.POINTER(C.c_double)),
+        self._check(self.L.cm_eval_nistmott(self.h, Z, method, len(E), pE, pu, s.ctypes.data_as(C.POINTER(C.c_double)),
                                             t.ctypes.data_as(C.POINTER(C.c_double)), precision))
         return s, t
 

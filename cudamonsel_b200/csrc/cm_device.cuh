@@ -409,9 +409,13 @@ template <typename R, typename G> CM_D R browning_angle(const Mott& m, R E, G& g
   return iso_angle(r2);
 }
 
-// JMONSEL/NISTMottRS.cu:103-119 times the SelectableElasticSM rate factor (1/nm)
-template <typename R> CM_D R nistmott_rate(const SceneView<R>& s, const Mott& m, R kel, R kbrown, R E, R logE) {
-  if (E < (R)m.extrapolateBelowEnergy) return (R)m.sfBrowning * browning_sigma(m, E) * kbrown;
+// JMONSEL/NISTMottRS.cu:103-119 times the SelectableElasticSM rate factor (1/nm); below the
+// extrapolation energy method 3 is linear in E, methods 1 and 2 scale Browning's cross section
+template <typename R> CM_D R nistmott_rate(const SceneView<R>& s, const Mott& m, int method, R kel, R kbrown, R E, R logE) {
+  if (E < (R)m.extrapolateBelowEnergy[method]) {
+    if (method == 3) return kel * (R)m.mottXSatMin[3] * E / (R)m.extrapolateBelowEnergy[3];
+    return (R)m.sfBrowning[method] * browning_sigma(m, E) * kbrown;
+  }
   if (E < (R)s.maxMott) {
     return kel * ulagrange_d1(s.blob + m.off_spwem, 61, s.dl50, s.param, (double)logE);
   }
@@ -419,9 +423,9 @@ template <typename R> CM_D R nistmott_rate(const SceneView<R>& s, const Mott& m,
   return (R)m.rutherfordA / (E + (R)m.rutherfordB) * kbrown;
 }
 
-// NISTMottRS.cu:121-154
-template <typename R, typename G> CM_D R nistmott_angle(const SceneView<R>& s, const Mott& m, R E, G& g) {
-  if (E < (R)m.extrapolateBelowEnergy) return browning_angle(m, E, g, (s.options & 1) != 0);
+// NISTMottRS.cu:121-154 (Browning's angles below the extrapolation energy for every method)
+template <typename R, typename G> CM_D R nistmott_angle(const SceneView<R>& s, const Mott& m, int method, R E, G& g) {
+  if (E < (R)m.extrapolateBelowEnergy[method]) return browning_angle(m, E, g, (s.options & 1) != 0);
   if (E < (R)s.maxMott) {
     const double lg = log((double)E);  // double in both precisions: see ulagrange_d1
     const R u = g.next();

@@ -223,43 +223,47 @@ static Jln make_jln(const HMaterial& mt, double breakE) {
 
 static double efermi(const HMaterial& m) { return -m.ecb - m.workfunction; }
 
-// NISTMottRS constructor members (JMONSEL/NISTMottRS.cu:76-91), method 1, SI
+// NISTMottRS constructor members (JMONSEL/NISTMottRS.cu:76-91) for methods 1..3, SI
 static void mott_constants(int Z, const HMott& hm, Mott& m) {
   m.Z = Z;
   m.zp17 = pow(Z, 1.7);
   m.zp2 = pow(Z, 2.0);
   m.zp3 = pow(Z, 3.0);
-  const double ext = kEV * 50.;
   const double dl50 = log(0.050 * kToSIkeV);
   const double param = (log(20.0 * kToSIkeV) - dl50) / 60.0;
-  // ULagrangeInterpolation::d1 at the extrapolation energy, in double on the host
-  const double x = log(ext);
-  const double reducedx = (x - dl50) / param;
-  int index0 = (int)reducedx - 1;
-  if (index0 < 0) index0 = 0;
-  if (index0 > 61 - 4) index0 = 61 - 4;
-  double xx = reducedx - index0;
-  const double* f = hm.spwem.data() + index0;
-  int ns = (int)round(xx);
-  if (ns < 0) ns = 0;
-  else if (ns > 3) ns = 3;
-  double c[4] = {f[0], f[1], f[2], f[3]}, d[4] = {f[0], f[1], f[2], f[3]};
-  double y = c[ns--], dy = 0;
-  for (int mm = 1; mm <= 3; mm++) {
-    for (int i = 0; i <= 3 - mm; i++) {
-      double ho = i - xx, hp = i + mm - xx, w = c[i + 1] - d[i];
-      d[i] = -hp * w / mm;
-      c[i] = -ho * w / mm;
+  for (int method = 0; method < 4; ++method) {
+    // 50 eV for method 1, 100 eV for methods 2 and 3 (NISTMottRS.cu:82)
+    const double ext = kEV * (method <= 1 ? 50. : 100.);
+    // ULagrangeInterpolation::d1 at the extrapolation energy, in double on the host
+    const double x = log(ext);
+    const double reducedx = (x - dl50) / param;
+    int index0 = (int)reducedx - 1;
+    if (index0 < 0) index0 = 0;
+    if (index0 > 61 - 4) index0 = 61 - 4;
+    double xx = reducedx - index0;
+    const double* f = hm.spwem.data() + index0;
+    int ns = (int)round(xx);
+    if (ns < 0) ns = 0;
+    else if (ns > 3) ns = 3;
+    double c[4] = {f[0], f[1], f[2], f[3]}, d[4] = {f[0], f[1], f[2], f[3]};
+    double y = c[ns--], dy = 0;
+    for (int mm = 1; mm <= 3; mm++) {
+      for (int i = 0; i <= 3 - mm; i++) {
+        double ho = i - xx, hp = i + mm - xx, w = c[i + 1] - d[i];
+        d[i] = -hp * w / mm;
+        c[i] = -ho * w / mm;
+      }
+      dy = (2 * ns < (3 - 1 - mm)) ? c[ns + 1] : d[ns--];
+      y += dy;
     }
-    dy = (2 * ns < (3 - 1 - mm)) ? c[ns + 1] : d[ns--];
-    y += dy;
+    const double mottXS = (kBohr * kBohr) * y;
+    const double e = ext * (1.0 / (1.60217653e-19 * 1.0e3));
+    const double re = sqrt(e);
+    const double browning = 3.0e-22 * m.zp17 / (e + 0.005 * m.zp17 * re + 0.0007 * m.zp2 / re);
+    m.sfBrowning[method] = mottXS / browning;
+    m.mottXSatMin[method] = y;
+    m.extrapolateBelowEnergy[method] = ext * kFromSIeV;
   }
-  const double mottXS = (kBohr * kBohr) * y;
-  const double e = ext * (1.0 / (1.60217653e-19 * 1.0e3));
-  const double re = sqrt(e);
-  const double browning = 3.0e-22 * m.zp17 / (e + 0.005 * m.zp17 * re + 0.0007 * m.zp2 / re);
-  m.sfBrowning = mottXS / browning;
-  m.extrapolateBelowEnergy = ext * kFromSIeV;
   const double zz = Z;
   const double zp = pow(zz, 1.0 / 3.0);
   m.rutherfordA = 7.670843088080456e-38 * zp * (1.0 + zz) * kFromSIeV;
@@ -450,6 +454,7 @@ static int build_scene(cm_context* ctx, DevScene<R>& ds) {
           auto it = mottIndex.find(mt.Z[i]);
           if (it == mottIndex.end()) return fail(CM_ESTATE, "no NIST Mott table for Z=" + std::to_string(mt.Z[i]));
           k.mott[i] = it->second;
+          k.mottMethod = hk.method;
           const double sf = (1000. * mt.wf[i]) / mt.A[i];
           k.kbrown[i] = sf * densityNa * 1e-9;
           k.kel[i] = (kBohr * kBohr) * sf * densityNa * 1e-9;
@@ -1040,16 +1045,16 @@ static int run_device(cm_context* ctx, const cm_run_desc* d, uint32_t* back, uin
 }
 
 // ------------------------------------------------------------------ per-function kernels
-template <typename R> __global__ void k_eval_nistmott(SceneView<R> s, int mi, int n, const double* E, const double* u, double* sig,
-                                                      double* th) {
+template <typename R> __global__ void k_eval_nistmott(SceneView<R> s, int mi, int method, int n, const double* E, const double* u,
+                                                      double* sig, double* th) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const Mott& m = s.mott[mi];
   const R e = (R)(E[i] * kFromSIeV);
   // cross section in m^2 (rate factor 1/kbrown folded back): kel = a0^2, kbrown = 1
-  sig[i] = (double)nistmott_rate(s, m, (R)(kBohr * kBohr), R(1), e, mlog(e));
+  sig[i] = (double)nistmott_rate(s, m, method, (R)(kBohr * kBohr), R(1), e, mlog(e));
   FixedRng<R> g{u + 2 * i, 2, 0};
-  th[i] = (double)nistmott_angle(s, m, e, g);
+  th[i] = (double)nistmott_angle(s, m, method, e, g);
 }
 
 template <typename R> __global__ void k_eval_table(SceneView<R> s, int t, int n, const double* x, double f0, double vf, int order,
@@ -1343,7 +1348,7 @@ static int add_mech(cm_context* ctx, int msm, const HMech& k, int* out) {
 }
 
 int cm_msm_add_nistmott(cm_context* ctx, int msm, int method, int* out) {
-  if (method != 1) return fail(CM_EINVAL, "only NISTMottRS method 1 (NISTMottRS::Factory) is supported");
+  if (method < 1 || method > 3) return fail(CM_EINVAL, "NISTMottRS method must be 1, 2 or 3");
   HMech k;
   memset(&k, 0, sizeof(k));
   k.kind = MECH_NISTMOTT;
@@ -1821,8 +1826,9 @@ static int mech_index(cm_context* ctx, int msm, int mech, int kind) {
   return base + mech;
 }
 
-int cm_eval_nistmott(cm_context* ctx, int Z, int n, const double* E, const double* u, double* sigma, double* theta,
-                     int precision) {
+int cm_eval_nistmott(cm_context* ctx, int Z, int method, int n, const double* E, const double* u, double* sigma,
+                     double* theta, int precision) {
+  if (method < 1 || method > 3) return fail(CM_EINVAL, "NISTMottRS method must be 1, 2 or 3");
   int rc = scene_for(ctx, precision);
   if (rc) return rc;
   auto it = ctx->mott.find(Z);
@@ -1837,9 +1843,9 @@ int cm_eval_nistmott(cm_context* ctx, int Z, int n, const double* E, const doubl
   rc = eval_launch(ctx, 1, in.data(), 3 * (size_t)n, out.data(), 2 * (size_t)n, [&](double* din, double* dout, int) {
     const int g = (n + 127) / 128;
     if (precision == CM_PREC_FP64)
-      k_eval_nistmott<double><<<g, 128>>>(ctx->d64.view, mi, n, din, din + n, dout, dout + n);
+      k_eval_nistmott<double><<<g, 128>>>(ctx->d64.view, mi, method, n, din, din + n, dout, dout + n);
     else
-      k_eval_nistmott<float><<<g, 128>>>(ctx->d32.view, mi, n, din, din + n, dout, dout + n);
+      k_eval_nistmott<float><<<g, 128>>>(ctx->d32.view, mi, method, n, din, din + n, dout, dout + n);
   });
   if (rc) return rc;
   for (int i = 0; i < n; ++i) {

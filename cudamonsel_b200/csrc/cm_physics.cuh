@@ -12,7 +12,7 @@ template <typename R> CM_D R mech_rate(const SceneView<R>& s, const Mech& k, R E
   switch (k.kind) {
     case MECH_NISTMOTT: {  // SelectableElasticSM.cu:25-47
       R total = 0;
-      for (int i = 0; i < k.nel; ++i) total += nistmott_rate(s, s.mott[k.mott[i]], (R)k.kel[i], (R)k.kbrown[i], E, logE);
+      for (int i = 0; i < k.nel; ++i) total += nistmott_rate(s, s.mott[k.mott[i]], k.mottMethod, (R)k.kel[i], (R)k.kbrown[i], E, logE);
       return total;
     }
     case MECH_TABULATED:
@@ -166,13 +166,13 @@ template <typename R, typename G> CM_D int elastic_scatter(const SceneView<R>& s
     R cum[kMaxElem];
     R tot = 0;
     for (int i = 0; i < k.nel; ++i) {
-      tot += nistmott_rate(s, s.mott[k.mott[i]], (R)k.kel[i], (R)k.kbrown[i], Ep, logE);
+      tot += nistmott_rate(s, s.mott[k.mott[i]], k.mottMethod, (R)k.kel[i], (R)k.kbrown[i], Ep, logE);
       cum[i] = tot;
     }
     const R r = u * tot;
     while (el < k.nel - 1 && cum[el] < r) ++el;
   }
-  const R alpha = nistmott_angle(s, s.mott[k.mott[el]], Ep, g);
+  const R alpha = nistmott_angle(s, s.mott[k.mott[el]], k.mottMethod, Ep, g);
   const R beta = R(2 * kPi) * g.next();
   update_dir(d, alpha, beta);
   return el;

@@ -76,6 +76,7 @@ struct Mech {
   // NISTMott via SelectableElasticSM: per element mott index and rate factor
   int nel;
   int mott[kMaxElem];        // index into Scene::mott
+  int mottMethod;            // NISTMottRS method 1..3
   double kel[kMaxElem];      // a0^2 * scalefactor * density * N_A in nm^-1 per (table unit)
   double kbrown[kMaxElem];   // the same factor for a Browning/Rutherford cross section in nm^2
   // TabulatedInelasticSM (JMONSEL/TabulatedInelasticSM.cu:461-498), energies in eV
@@ -105,13 +106,15 @@ struct Msm {
   double lambda, lambdaFactor;  // lambdaFactor in 1/sqrt(eV)
 };
 
-// NISTMottRS (method 1) per element; the tables live in the precision blob
+// NISTMottRS per element; the tables live in the precision blob, the extrapolation constants are
+// indexed by method (1: Factory, 2: Factory100, 3: Factory100Lin; entry 0 copies method 1)
 struct Mott {
   int Z;
   int off_spwem, off_x1;     // offsets of the cross sections in the table blob (off_x1 unused: -1)
   int off_x1d;               // offset of the 61 x 201 quantile table in the double copy (mott64)
-  double extrapolateBelowEnergy;  // eV
-  double sfBrowning;
+  double extrapolateBelowEnergy[4];  // eV
+  double sfBrowning[4];
+  double mottXSatMin[4];             // table value (units of a0^2) at extrapolateBelowEnergy
   double zp17, zp2, zp3;
   double rutherfordA, rutherfordB;  // sigma = A / (E + B) in nm^2 with E in eV
   double rutherfordAlpha;           // alpha = rutherfordAlpha / E

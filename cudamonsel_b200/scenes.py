@@ -150,15 +150,16 @@ def vacuum(spec):
     return spec.msm(mat)
 
 
-def silicon(spec, tables=None, phonon=False):
-    """Si as LinesOnLayers.cu:172-205 (phonon mechanism optional)."""
+def silicon(spec, tables=None, phonon=False, mott_method=1):
+    """Si as LinesOnLayers.cu:172-205 (phonon mechanism optional; mott_method picks the NISTMottRS factory,
+    1 as there)."""
     workfun, bandgap = 4.85, 1.1
     efermi = -bandgap
     potU = -workfun - efermi
     mat = spec.material([14], [data.atomic_weight(14)], [1.0], 2330.0, eV(workfun), eV(potU), eV(bandgap),
                         [eV(99.2), eV(99.8), eV(149.7), eV(1839.0)])
     m = spec.msm(mat)
-    spec.nistmott(m, 1)
+    spec.nistmott(m, mott_method)
     paths = tables or data.si_tables()
     t = [spec.table(p) for p in paths]
     spec.tabulated(m, 3, eV(13.54), t)
@@ -174,8 +175,8 @@ PMMA_Z = (1, 8, 6)
 PMMA_WF = (0.080541919183721306, 0.3196178155473462, 0.59984026526893253)
 
 
-def pmma(spec):
-    """PMMA as LinesOnLayers.cu:86-127."""
+def pmma(spec, mott_method=1):
+    """PMMA as LinesOnLayers.cu:86-127 (mott_method picks the NISTMottRS factory, 1 as there)."""
     breakE = eV(45.0)
     workfun, bandgap = 5.5, 5.0
     efermi = -bandgap
@@ -183,7 +184,7 @@ def pmma(spec):
     mat = spec.material(list(PMMA_Z), [data.atomic_weight(z) for z in PMMA_Z], list(PMMA_WF), 1190.0, eV(workfun),
                         eV(potU), eV(bandgap))
     m = spec.msm(mat)
-    spec.nistmott(m, 1)
+    spec.nistmott(m, mott_method)
     spec.fitted(m, eV(65.4), breakE)
     spec.polaron(m, 2.0e7, 1.0 / eV(4.0))
     spec.csd_jln(m, breakE)
@@ -199,11 +200,12 @@ class Scene:
         self.h = handles
 
 
-def halfspace(tables=None):
-    """Flat Si filling z >= 0 (plane normal (0,0,-1) through the origin), in a 0.1 m vacuum chamber."""
+def halfspace(tables=None, material="si", mott_method=1):
+    """Flat Si (or PMMA: material="pmma") filling z >= 0 (plane normal (0,0,-1) through the origin), in a
+    0.1 m vacuum chamber."""
     s = SceneSpec()
     vac = vacuum(s)
-    si = silicon(s, tables)
+    si = silicon(s, tables, mott_method=mott_method) if material == "si" else pmma(s, mott_method)
     sphere = s.sphere([0.0, 0.0, 0.0], 0.1)
     chamber = s.region(None, vac, sphere)
     surf = s.planes([0.0, 0.0, -1.0], [0.0, 0.0, 0.0])

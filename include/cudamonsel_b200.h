@@ -75,7 +75,9 @@ int cm_add_material(cm_context* ctx, int nel, const int* Z, const double* atomic
                     const double* core_energies, int* out_material);
 /* MONSEL_MaterialScatterModel(mat, ExpQMBarrierSM(mat)) (JMONSEL/MONSEL_MaterialScatterModel.cu:13-37) */
 int cm_add_msm(cm_context* ctx, int material, int* out_msm);
-/* SelectableElasticSM(mat, NISTMottRS::Factory) (JMONSEL/SelectableElasticSM.cu:10-18); method 1 only */
+/* SelectableElasticSM(mat, NISTMottRS factory) (JMONSEL/SelectableElasticSM.cu:10-18).  method 1 =
+ * NISTMottRS::Factory (Browning-scaled below 50 eV), 2 = Factory100 (Browning-scaled below 100 eV),
+ * 3 = Factory100Lin (cross section linear in energy below 100 eV); JMONSEL/NISTMottRS.cu:76-119, :506-512 */
 int cm_msm_add_nistmott(cm_context* ctx, int msm, int method, int* out_mech);
 /* TabulatedInelasticSM(mat, methodSE, tables, energyOffset) (JMONSEL/TabulatedInelasticSM.cu:23-66);
  * tables = {IIMFP, reduced deltaE, theta, SE E0} */
@@ -224,8 +226,8 @@ int cm_job_result(cm_server* server, int job, uint32_t* back, uint32_t* fwd, cm_
 /* ---- per-function entry points (parity checks; host arrays, SI units) -------
  * Deviates are injected from u arrays so that each result can be compared
  * with the reference on the same inputs.  precision selects the kernel. */
-/* NISTMottRS::totalCrossSection / randomScatteringAngle (JMONSEL/NISTMottRS.cu:103-154); u[2n] */
-int cm_eval_nistmott(cm_context* ctx, int Z, int n, const double* E, const double* u, double* sigma, double* theta,
+/* NISTMottRS::totalCrossSection / randomScatteringAngle (JMONSEL/NISTMottRS.cu:103-154) of method 1..3; u[2n] */
+int cm_eval_nistmott(cm_context* ctx, int Z, int method, int n, const double* E, const double* u, double* sigma, double* theta,
                      int precision);
 /* NUTableInterpolation::interpolate (JMONSEL/NUTableInterpolation.cu:98-115); x[3n] */
 int cm_eval_table(cm_context* ctx, int table, int n, const double* x, int order, double* out, int precision);

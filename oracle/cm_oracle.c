@@ -269,8 +269,8 @@ typedef struct {
    int Z;
    double spwem[61];
    double* x1; /* [61][201] */
-   /* NISTMottRS members (JMONSEL/NISTMottRS.cu:76-91) for method 1 */
-   double extrapolateBelowEnergy, mottXSatMin, sfBrowning;
+   /* NISTMottRS members (JMONSEL/NISTMottRS.cu:76-91), indexed by method 1..3 */
+   double extrapolateBelowEnergy[4], mottXSatMin[4], sfBrowning[4];
    /* BrowningEmpiricalCrossSection.cu:11-17 */
    double zp17, zp2, zp3;
 } mott_elem;
@@ -324,18 +324,22 @@ static double rutherford_angle(int Z, double energy, cmo_rng* r)
 static double dl50(void) { return log(0.050 * TOSI_KEV); }
 static double param(void) { return (log(20.0 * TOSI_KEV) - dl50()) / 60.0; }
 
-/* JMONSEL/NISTMottRS.cu:103-119 (method 1) */
-static double nistmott_sigma(const mott_elem* m, double energy)
+/* JMONSEL/NISTMottRS.cu:103-119: below extrapolateBelowEnergy method 3 is linear in energy, methods 1
+ * and 2 scale Browning's cross section */
+static double nistmott_sigma(const mott_elem* m, double energy, int method)
 {
-   if (energy < m->extrapolateBelowEnergy) return m->sfBrowning * browning_sigma(m, energy);
+   if (energy < m->extrapolateBelowEnergy[method]) {
+      if (method == 3) return m->mottXSatMin[method] * energy / m->extrapolateBelowEnergy[method];
+      return m->sfBrowning[method] * browning_sigma(m, energy);
+   }
    if (energy < MAX_NISTMOTT_()) return (BOHR * BOHR) * cmo_ulagrange_d1(m->spwem, 61, dl50(), param(), 3, log(energy));
    return rutherford_sigma(m->Z, energy);
 }
 
-/* NISTMottRS.cu:121-154 */
-static double nistmott_angle(const mott_elem* m, double energy, cmo_rng* r, int fixes)
+/* NISTMottRS.cu:121-154 (Browning's angle below extrapolateBelowEnergy for every method) */
+static double nistmott_angle(const mott_elem* m, double energy, int method, cmo_rng* r, int fixes)
 {
-   if (energy < m->extrapolateBelowEnergy) return browning_angle(m, energy, r, fixes);
+   if (energy < m->extrapolateBelowEnergy[method]) return browning_angle(m, energy, r, fixes);
    if (energy < MAX_NISTMOTT_()) {
       const double x0[] = { dl50(), 0. };
       const double xinc[] = { param(), 0.005 };
@@ -353,10 +357,13 @@ static void mott_setup(mott_elem* m)
    m->zp17 = pow(m->Z, 1.7);
    m->zp2 = pow(m->Z, 2.0);
    m->zp3 = pow(m->Z, 3.0);
-   m->extrapolateBelowEnergy = TOSI_EV * 50.;
-   m->sfBrowning = 1.0; /* unused for E >= extrapolateBelowEnergy */
-   m->mottXSatMin = nistmott_sigma(m, m->extrapolateBelowEnergy);
-   m->sfBrowning = m->mottXSatMin / browning_sigma(m, m->extrapolateBelowEnergy);
+   /* NISTMottRS.cu:82,86-87: 50 eV for method 1, 100 eV for methods 2 and 3; the cross section at the
+    * extrapolation energy itself comes from the table branch */
+   for (int method = 0; method < 4; ++method) {
+      m->extrapolateBelowEnergy[method] = TOSI_EV * (method <= 1 ? 50. : 100.);
+      m->mottXSatMin[method] = nistmott_sigma(m, m->extrapolateBelowEnergy[method], method);
+      m->sfBrowning[method] = m->mottXSatMin[method] / browning_sigma(m, m->extrapolateBelowEnergy[method]);
+   }
 }
 
 /* ---------------------------------------------------------------- scene */
@@ -379,8 +386,8 @@ typedef struct {
 
 typedef struct {
    int kind;
-   /* elastic: SelectableElasticSM.cu:69-89 */
-   int nel;
+   /* elastic: SelectableElasticSM.cu:69-89, NISTMottRS method */
+   int nel, method;
    int elem[MAXEL];         /* index into scene mott table */
    double scalefactor[MAXEL];
    double densityNa;
@@ -564,11 +571,12 @@ int cmo_msm_set_min_e(cmo_scene* s, int msm, double minE)
 int cmo_msm_add_nistmott(cmo_scene* s, int msm, int method)
 {
    msm_t* m = &s->msms[msm];
-   if (m->nmech >= MAXMECH || method != 1) return -1;
+   if (m->nmech >= MAXMECH || method < 1 || method > 3) return -1;
    const material* mt = &s->mats[m->material];
    mechanism* k = &m->mech[m->nmech];
    memset(k, 0, sizeof(*k));
    k->kind = M_NISTMOTT;
+   k->method = method;
    k->nel = mt->nel;
    k->densityNa = mt->density * AVOGADRO;
    for (int i = 0; i < mt->nel; ++i) {
@@ -1416,7 +1424,7 @@ static double elastic_set_cache(const cmo_scene* s, const mechanism* k, double k
 {
    double total = 0.;
    for (int i = 0; i < k->nel; i++) {
-      total += nistmott_sigma(&s->mott[k->elem[i]], kE) * k->scalefactor[i];
+      total += nistmott_sigma(&s->mott[k->elem[i]], kE, k->method) * k->scalefactor[i];
       cum[i] = total;
    }
    return total;
@@ -1605,7 +1613,7 @@ static int elastic_scatter(const cmo_scene* s, const mechanism* k, electron* pe,
    double rr = cmo_uniform(r) * total;
    int index = 0;
    while (cum[index] < rr) index++;
-   double alpha = nistmott_angle(&s->mott[k->elem[index]], kE, r, s->options & 1);
+   double alpha = nistmott_angle(&s->mott[k->elem[index]], kE, k->method, r, s->options & 1);
    double beta = 2 * PI * cmo_uniform(r);
    update_direction(&pe->theta, &pe->phi, alpha, beta);
    if (Zout) *Zout = k->elem[index];
@@ -1933,16 +1941,22 @@ int cmo_run(cmo_scene* s, int chamber, double beam_width, double beam_energy, co
 }
 
 /* ---------------------------------------------------------------- per-function entry points */
-void cmo_eval_nistmott(cmo_scene* s, int Z, int n, const double* E, const double* u, double* sigma, double* theta,
-                       int* ndev)
+void cmo_eval_nistmott_method(cmo_scene* s, int Z, int method, int n, const double* E, const double* u, double* sigma,
+                              double* theta, int* ndev)
 {
    const mott_elem* m = &s->mott[Z];
    for (int i = 0; i < n; ++i) {
       cmo_rng r = { u + 2 * i, 2, 0, { 0 } };
-      sigma[i] = nistmott_sigma(m, E[i]);
-      theta[i] = nistmott_angle(m, E[i], &r, s->options & 1);
+      sigma[i] = nistmott_sigma(m, E[i], method);
+      theta[i] = nistmott_angle(m, E[i], method, &r, s->options & 1);
       ndev[i] = r.used;
    }
+}
+
+void cmo_eval_nistmott(cmo_scene* s, int Z, int n, const double* E, const double* u, double* sigma, double* theta,
+                       int* ndev)
+{
+   cmo_eval_nistmott_method(s, Z, 1, n, E, u, sigma, theta, ndev);
 }
 
 void cmo_eval_table(cmo_scene* s, int table, int n, const double* x3, int order, double* out)

@@ -73,6 +73,9 @@ int cmo_region(cmo_scene* s, int parent, int msm, int shape);
 /* ---- per-function evaluation on arrays, deviates injected (u arrays are row-major) */
 void cmo_eval_nistmott(cmo_scene* s, int Z, int n, const double* E, const double* u, double* sigma, double* theta,
                        int* ndev);
+/* the same for NISTMottRS method 1, 2 or 3 (JMONSEL/NISTMottRS.cu:76-91 sets each method's constants) */
+void cmo_eval_nistmott_method(cmo_scene* s, int Z, int method, int n, const double* E, const double* u, double* sigma,
+                              double* theta, int* ndev);
 void cmo_eval_table(cmo_scene* s, int table, int n, const double* x3, int order, double* out);
 void cmo_eval_tabulated(cmo_scene* s, int msm, int mech, int n, const double* in /* E th ph u0..u5 */,
                         double* out /* rate E th ph hasSE ESE thSE phSE ndev */);

@@ -59,6 +59,7 @@ def lib():
         L.cmo_shape_union.argtypes = [C.c_void_p, C.c_int, C.c_int]
         L.cmo_region.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int]
         L.cmo_eval_nistmott.argtypes = [C.c_void_p, C.c_int, C.c_int, d, d, d, d, i]
+        L.cmo_eval_nistmott_method.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, d, d, d, d, i]
         L.cmo_eval_table.argtypes = [C.c_void_p, C.c_int, C.c_int, d, C.c_int, d]
         L.cmo_eval_tabulated.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, d, d]
         L.cmo_eval_tabulated_stride.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, d, d, C.c_int]

@@ -226,6 +226,37 @@ static void golden_nistmott(const std::string& out)
    fclose(f);
 }
 
+// NISTMottRS methods 2 (Factory100: Browning below 100 eV) and 3 (Factory100Lin: linear below 100 eV)
+static void golden_nistmott23(const std::string& out)
+{
+   FILE* f = openw(out, "nistmott23.txt");
+   fprintf(f, "# NISTMottRS methods 2 and 3 totalCrossSection and randomScatteringAngle; energies in J, sigma in m^2\n");
+   fprintf(f, "# method Z E u1 u2 sigma theta ndeviates\n");
+   const int Zs[] = { 1, 6, 8, 14, 29, 79 };
+   std::vector<double> Es;
+   for (int i = 0; i < 300; ++i) Es.push_back(ToSI::eV(::exp(::log(1.0) + (::log(30000.0) - ::log(1.0)) * uin())));
+   for (int i = 0; i < 100; ++i) Es.push_back(ToSI::eV(40.0 + 80.0 * uin()));
+   Es.push_back(ToSI::eV(100.)); Es.push_back(ToSI::eV(99.999)); Es.push_back(ToSI::eV(50.)); Es.push_back(ToSI::eV(49.999));
+   Es.push_back(ToSI::keV(20.)); Es.push_back(ToSI::eV(1.)); Es.push_back(ToSI::eV(3.75));
+   for (int method = 2; method <= 3; ++method) {
+      const RandomizedScatterFactoryT& fac = method == 2 ? NISTMottRS::Factory100 : NISTMottRS::Factory100Lin;
+      for (int z : Zs) {
+         const RandomizedScatterT& rs = fac.get(Element::byAtomicNumber(z));
+         for (size_t i = 0; i < Es.size(); ++i) {
+            double E = Es[i];
+            double u1 = uin(), u2 = uin();
+            if (i % 37 == 0) u1 = 0.0;
+            if (i % 43 == 0) u2 = 1.0;
+            double sigma = rs.totalCrossSection(E);
+            push({ u1, u2 });
+            double th = rs.randomScatteringAngle(E);
+            fprintf(f, "%d %d " G " " G " " G " " G " " G " %lld\n", method, z, E, u1, u2, sigma, th, g_drawn);
+         }
+      }
+   }
+   fclose(f);
+}
+
 static void golden_nutable(const std::string& out, const SiModel& si)
 {
    FILE* f = openw(out, "nutable.txt");
@@ -675,6 +706,7 @@ int main(int argc, char** argv)
       golden_misc(out, si);
       golden_barrier(out, si);
       golden_shapes2(out);
+      golden_nistmott23(out);  // last, so the earlier sets keep their input streams
       return 0;
    }
    if (mode == "run1" && argc >= 5) {

@@ -91,6 +91,37 @@ def test_nistmott_fp64(lines_engine, Z):
     assert d.max() < 1e-9
 
 
+@pytest.mark.parametrize("prec", [FP64, FP32], ids=["fp64", "fp32"])
+@pytest.mark.parametrize("method", [2, 3])
+def test_nistmott_methods_2_3(lines_engine, oracle_lines, method, prec):
+    """NISTMottRS methods 2 and 3 (extrapolation below 100 eV, JMONSEL/NISTMottRS.cu:76-119): FP64 against the
+    reference's golden vectors, FP32 against the oracle on float-rounded energies and deviates."""
+    import ctypes as C
+    import pyoracle as po
+    e, h = lines_engine
+    b, _, _ = oracle_lines
+    g = golden("nistmott23")
+    for Z in (1, 6, 8, 14):
+        rows = g[(g[:, 0] == method) & (g[:, 1] == Z)]
+        n = len(rows)
+        if prec == FP64:
+            E, u = rows[:, 2], np.ascontiguousarray(rows[:, 3:5])
+            rs, rt = rows[:, 5], rows[:, 6]
+        else:
+            E, u = f32_energy(rows[:, 2]), np.ascontiguousarray(f32(rows[:, 3:5]))
+            rs, rt = np.zeros(n), np.zeros(n)
+            nd = np.zeros(n, dtype=np.int32)
+            b.L.cmo_eval_nistmott_method(b.h, Z, method, n, po.dp(np.ascontiguousarray(E)), po.dp(u),
+                                         rs.ctypes.data_as(C.POINTER(C.c_double)),
+                                         rt.ctypes.data_as(C.POINTER(C.c_double)), nd.ctypes.data_as(C.POINTER(C.c_int)))
+        sig, th = e.eval_nistmott(Z, np.ascontiguousarray(E), u, prec, method)
+        tol = 1e-9 if prec == FP64 else 1e-6
+        r = rel(sig, rs)
+        d = np.abs(th - rt) / np.maximum(rt, 1e-6) if prec == FP32 else np.abs(th - rt)
+        print("method %d Z=%d sigma max rel %.3g theta max %.3g" % (method, Z, r.max(), d.max()))
+        assert r.max() < tol and d.max() < tol
+
+
 def test_nistmott_sweep(lines_engine, oracle_lines):
     """Sampled Mott angle over a fine grid of deviates and energies (FP64 vs the oracle)."""
     e, h = lines_engine

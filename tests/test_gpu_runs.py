@@ -203,6 +203,49 @@ def test_rough_lines_match_oracle(rough_oracle_runs, prec):
         assert abs(zb) < 3.5 and abs(zs) < 3.5
 
 
+@pytest.fixture(scope="module")
+def mott_method_oracle_runs():
+    import pyoracle
+    from cudamonsel_b200 import scenes
+    out = {}
+    for mat in ("si", "pmma"):
+        for method in (2, 3):
+            sc = scenes.halfspace(material=mat, mott_method=method)
+            ob, _, _ = pyoracle.run_scene(sc, np.tile([0.0, 0.0, -20e-9], (8, 1)), 0.0, scenes.eV(300.0), 2000, 31, 30)
+            out[mat, method] = ob
+    return out
+
+
+@pytest.mark.parametrize("prec", [FP64, FP32], ids=["fp64", "fp32"])
+@pytest.mark.parametrize("method", [2, 3])
+@pytest.mark.parametrize("mat", ["si", "pmma"])
+def test_nistmott_methods_match_oracle(mott_method_oracle_runs, mat, method, prec):
+    """Flat Si and PMMA at 300 eV with NISTMottRS method 2 (Factory100) or 3 (Factory100Lin): most of the
+    secondaries scatter elastically below 100 eV, where the methods differ (method 3 raises the SE yield by
+    a quarter), so the yields test the per-mechanism method choice.  Engine 64 x 500 primaries vs the
+    oracle's 8 x 2000; the same seed with method 1 must give different tallies."""
+    from cudamonsel_b200 import capi, scenes
+    e = capi.Engine(0)
+    h = scenes.build_engine(scenes.halfspace(material=mat, mott_method=method), e)
+    centers = np.tile([0.0, 0.0, -20e-9], (64, 1))
+    back, _, st = e.run(h["chamber"], centers, scenes.eV(300.0), 500, 30, 0.0, seed=41, precision=prec)
+    e.reset()
+    h1 = scenes.build_engine(scenes.halfspace(material=mat, mott_method=1), e)
+    back1, _, _ = e.run(h1["chamber"], centers, scenes.eV(300.0), 500, 30, 0.0, seed=41, precision=prec)
+    e.close()
+    assert st.primaries == 64 * 500
+    assert not np.array_equal(back, back1)
+    eb, es = batch_yields(back, 500, 300.0, 30)
+    ob = mott_method_oracle_runs[mat, method]
+    rb, rs = batch_yields(ob, 2000, 300.0, 30)
+    for name, a, r in (("BSE", eb, rb), ("SE", es, rs)):
+        # oracle batches are 4x larger: scale their spread to the engine's batch size
+        se = a.std(ddof=1) * np.sqrt(1.0 / len(a) + 1.0 / (4 * len(r)))
+        z = (a.mean() - r.mean()) / max(se, 1e-12)
+        print("%s method %d %s engine %.4f oracle %.4f z=%.2f" % (mat, method, name, a.mean(), r.mean(), z))
+        assert abs(z) < 3.5
+
+
 @pytest.mark.parametrize("prec", [FP64, FP32], ids=["fp64", "fp32"])
 def test_child_grid_finds_what_the_scan_finds(prec):
     """The rough-line chamber (385 children) searched through its x-y grid and by the in-order scan

@@ -44,6 +44,30 @@ def test_nistmott_sigma_and_angle(oracle_lines, Z):
     assert (nd == rows[:, 6]).all()
 
 
+@pytest.mark.parametrize("method", [2, 3])
+@pytest.mark.parametrize("Z", [1, 6, 8, 14])
+def test_nistmott_methods_2_3(oracle_lines, method, Z):
+    """NISTMottRS::Factory100 (method 2: Browning below 100 eV) and Factory100Lin (method 3: cross section
+    linear in energy below 100 eV, Browning angles), JMONSEL/NISTMottRS.cu:76-119 and :484-512."""
+    import pyoracle as po
+    b, h, _ = oracle_lines
+    g = golden("nistmott23")
+    rows = g[(g[:, 0] == method) & (g[:, 1] == Z)]
+    n = len(rows)
+    assert n > 400
+    sig, th = np.zeros(n), np.zeros(n)
+    nd = np.zeros(n, dtype=np.int32)
+    u = np.ascontiguousarray(rows[:, 3:5])
+    E = np.ascontiguousarray(rows[:, 2])
+    b.L.cmo_eval_nistmott_method(b.h, Z, method, n, po.dp(E), po.dp(u), D(sig), D(th),
+                                 nd.ctypes.data_as(C.POINTER(C.c_int)))
+    ok, bad = exact(sig, rows[:, 5])
+    assert ok, bad
+    ok, bad = exact(th, rows[:, 6])
+    assert ok, bad
+    assert (nd == rows[:, 7]).all()
+
+
 def test_nu_table_interpolation(oracle_halfspace):
     """NUTableInterpolation::interpolate on all four Si tables, inside and outside the domain."""
     import pyoracle as po
