@@ -253,6 +253,7 @@ def main():
     # FP64 plain form on the same workload: throughput and the yield error of FP32 against it
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    step(capi.PREC_FP64)  # untimed: builds the FP64 scene and wave buffers
     flush.zero_()
     e0.record(stream)
     st64 = step(capi.PREC_FP64)
@@ -281,9 +282,11 @@ def main():
     d2h = 2 * NPIX * stride * 4
 
     steps_total = sum(s.steps for s in stats)
-    launches = sum(6 * int(s.kernel_launches[0]) for s in stats)
+    launches = sum(sum(int(x) for x in s.kernel_launches) + int(s.step_launches) for s in stats)
     # roofline of the dominant kernel: one more step of the same workload with CUDA events
-    # between the kernels of every iteration (event nodes inside the captured graph)
+    # between the kernels of every iteration (event nodes inside the captured graph); a profiled
+    # run keeps the queue kernels to the end (no several-steps-per-thread tail), so its shares
+    # are those of the queue kernels
     flush.zero_()
     prof = [step(prec, profile=1)]
     torch.cuda.synchronize()

@@ -48,7 +48,7 @@ class RunStats(C.Structure):
     _fields_ = [("primaries", C.c_int64), ("steps", C.c_int64), ("scatter_events", C.c_int64),
                 ("barrier_events", C.c_int64), ("escapes", C.c_int64), ("secondaries", C.c_int64),
                 ("iterations", C.c_int64), ("device_ms", C.c_double), ("kernel_ms", C.c_double * 6),
-                ("kernel_launches", C.c_int64 * 6), ("units", C.c_int64 * 4)]
+                ("kernel_launches", C.c_int64 * 6), ("units", C.c_int64 * 4), ("step_launches", C.c_int64)]
 
     KERNELS = ("flight", "elastic", "inelastic", "misc", "spawn", "tail")
 
@@ -57,6 +57,7 @@ class RunStats(C.Structure):
         d["kernel_ms"] = dict(zip(self.KERNELS, list(self.kernel_ms)))
         d["kernel_launches"] = dict(zip(self.KERNELS, list(self.kernel_launches)))
         d["units"] = dict(zip(self.KERNELS[:4], list(self.units)))
+        d["step_launches"] = self.step_launches
         return d
 
 

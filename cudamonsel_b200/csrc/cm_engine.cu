@@ -742,20 +742,43 @@ template <typename R, int D> __global__ void __launch_bounds__(256) k_flight(Run
   flight_loop<R, D>(v, cur);
 }
 
-// FP32 flight over leaf shapes compiled for 4 resident CTAs per SM (64 registers): the kernel is
-// latency-bound and the extra warps hide more than the spills cost (linescan -3 %, rough image -14 %
-// against 2 CTAs per SM).  Tree walks (D > 0) spill too much at 64 registers and keep k_flight.
-__global__ void __launch_bounds__(256, 4) k_flight32_leaf(RunView<float> v, int cur) { flight_loop<float, 0>(v, cur); }
+// Resident CTAs per SM the kernels are compiled for (register caps 65536 / (256 x n)); a build may set
+// them with -DCM_MINB_FLIGHT32=n and so on.  CM_MINB_INELASTIC unset: the compiler chooses.
+#ifndef CM_MINB_FLIGHT32
+#define CM_MINB_FLIGHT32 3
+#endif
+#ifndef CM_MINB_ELASTIC
+#define CM_MINB_ELASTIC 4
+#endif
+#if defined(CM_MINB_ELASTIC)
+#define CM_LB_ELASTIC __launch_bounds__(256, CM_MINB_ELASTIC)
+#else
+#define CM_LB_ELASTIC __launch_bounds__(256)
+#endif
+#if defined(CM_MINB_INELASTIC)
+#define CM_LB_INELASTIC __launch_bounds__(256, CM_MINB_INELASTIC)
+#else
+#define CM_LB_INELASTIC __launch_bounds__(256)
+#endif
+
+// FP32 flight over leaf shapes compiled for 3 resident CTAs per SM (80 registers): the kernel is
+// latency-bound and the extra warps hide more than the spills cost (linescan +5 %, rough image +3 %
+// against 2 CTAs per SM; 4 CTAs spill twice as much and lose 7 % on the rough image).  Tree walks
+// (D > 0) spill too much under a cap and keep k_flight.  k_elastic runs at 4 CTAs per SM (64
+// registers, a few spills): linescan +2 %.
+__global__ void __launch_bounds__(256, CM_MINB_FLIGHT32) k_flight32_leaf(RunView<float> v, int cur) {
+  flight_loop<float, 0>(v, cur);
+}
 
 template <typename R>
-__global__ void __launch_bounds__(256) k_elastic(RunView<R> v, int cur) {
+__global__ void CM_LB_ELASTIC k_elastic(RunView<R> v, int cur) {
   DeviceSink sink;
   const int n = v.c->q[Q_EL];
   for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) elastic_one(v, cur, j, sink);
 }
 
 template <typename R>
-__global__ void __launch_bounds__(256) k_inelastic(RunView<R> v, int cur) {
+__global__ void CM_LB_INELASTIC k_inelastic(RunView<R> v, int cur) {
   DeviceSink sink;
   StepCounts sc;
   const int n = v.c->q[Q_TAB];
@@ -784,6 +807,36 @@ static void launch_flight(const RunView<float>& v, int cur, int grid, cudaStream
   if (v.s.depth == 0) k_flight32_leaf<<<grid, 256, 0, s>>>(v, cur);
   else if (v.s.depth <= 2) k_flight<float, 2><<<grid, 256, 0, s>>>(v, cur);
   else k_flight<float, kMaxShapeDepth><<<grid, 256, 0, s>>>(v, cur);
+}
+
+// The tail of a run: once fewer electrons are left than fill the GPU, each thread takes one electron
+// through CM_TAIL_STEPS whole steps per iteration (k_steps) instead of one step through the queue
+// kernels, whose launches and queue traffic then cost more than the steps themselves.
+#ifndef CM_TAIL_BELOW
+#define CM_TAIL_BELOW 65536
+#endif
+#ifndef CM_TAIL_STEPS
+#define CM_TAIL_STEPS 8
+#endif
+
+template <typename R, int D> __global__ void __launch_bounds__(256) k_steps(RunView<R> v, int cur, int nsteps) {
+  DeviceSink sink;
+  StepCounts sc;
+  const int n = v.c->n[cur];
+  int cnt[kClasses];
+  for (int k = 0; k < kClasses; ++k) cnt[k] = v.c->nc[cur][k];
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    int k = 0, j = i;
+    while (k < kClasses - 1 && j >= cnt[k]) j -= cnt[k++];
+    steps_one<R, D>(v, cur, k * v.W + j, nsteps, sink, sc);
+  }
+  flush_counts(v.c, sc);
+}
+
+template <typename R> static void launch_steps(const RunView<R>& v, int cur, int grid, cudaStream_t s) {
+  if (v.s.depth == 0) k_steps<R, 0><<<grid, 256, 0, s>>>(v, cur, CM_TAIL_STEPS);
+  else if (v.s.depth <= 2) k_steps<R, 2><<<grid, 256, 0, s>>>(v, cur, CM_TAIL_STEPS);
+  else k_steps<R, kMaxShapeDepth><<<grid, 256, 0, s>>>(v, cur, CM_TAIL_STEPS);
 }
 
 template <typename R> static void launch_misc(const RunView<R>& v, int cur, int grid, cudaStream_t s) {
@@ -940,12 +993,18 @@ static int run_device_once(cm_context* ctx, const cm_run_desc* d, uint32_t* back
   }
   CM_CUDA(cudaStreamEndCapture(stream, &graph));
   CM_CUDA(cudaGraphInstantiate(&exec, graph, 0));
+  // the tail graph (k_steps, spawn, tail per iteration), captured when first wanted
+  cudaGraph_t tgraph = nullptr;
+  cudaGraphExec_t texec = nullptr;
+  bool tail = false;
+  int titers = 0;
   CM_CUDA(cudaEventRecord(e0, stream));
   int iters = 0;
   int status = 0;
   for (;;) {
-    CM_CUDA(cudaGraphLaunch(exec, stream));
+    CM_CUDA(cudaGraphLaunch(tail ? texec : exec, stream));
     iters += 2 * K;
+    if (tail) titers += 2 * K;
     CM_CUDA(cudaMemcpyAsync(ctx->counters_host, ctx->counters, sizeof(Counters), cudaMemcpyDeviceToHost, stream));
     CM_CUDA(cudaStreamSynchronize(stream));
     if (d->profile) {
@@ -964,6 +1023,24 @@ static int run_device_once(cm_context* ctx, const cm_run_desc* d, uint32_t* back
     if (ctx->cancel && ctx->cancel->load()) {
       status = fail(CM_ECANCELED, "cancelled");
       break;
+    }
+    {
+      // all primaries started and fewer electrons left (waves and pool) than CM_TAIL_BELOW: tail graph.
+      // Profiled runs keep the queue kernels throughout, so that each kernel's time is measured.
+      const Counters& hc = *ctx->counters_host;
+      const long long left = (long long)hc.n[0] + hc.n[1] + std::min(hc.pool, v.poolCap);
+      tail = !d->profile && hc.next_primary == hc.total_primaries && left < CM_TAIL_BELOW;
+      if (tail && !texec) {
+        CM_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+        for (int it = 0; it < 2 * K; ++it) {
+          const int cur = it & 1;
+          launch_steps(v, cur, grid, stream);
+          launch_spawn<R>(v, cur, grid, stream);
+          k_tail<R><<<1, 32, 0, stream>>>(v, cur);
+        }
+        CM_CUDA(cudaStreamEndCapture(stream, &tgraph));
+        CM_CUDA(cudaGraphInstantiate(&texec, tgraph, 0));
+      }
     }
     if (iters >= maxIt) {
       const Counters& hc = *ctx->counters_host;
@@ -998,6 +1075,8 @@ static int run_device_once(cm_context* ctx, const cm_run_desc* d, uint32_t* back
   cudaEventElapsedTime(&ms, e0, e1);
   cudaGraphExecDestroy(exec);
   cudaGraphDestroy(graph);
+  if (texec) cudaGraphExecDestroy(texec);
+  if (tgraph) cudaGraphDestroy(tgraph);
   for (auto& ev : pev) cudaEventDestroy(ev);
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
@@ -1014,9 +1093,10 @@ static int run_device_once(cm_context* ctx, const cm_run_desc* d, uint32_t* back
     st->device_ms = ms;
     for (int k = 0; k < 6; ++k) {
       st->kernel_ms[k] = kms[k];
-      st->kernel_launches[k] = (int64_t)iters;
+      st->kernel_launches[k] = (int64_t)(k < 4 ? iters - titers : iters);
     }
     for (int k = 0; k < 4; ++k) st->units[k] = (int64_t)c.units[k];
+    st->step_launches = titers;
   }
   return status;
 }

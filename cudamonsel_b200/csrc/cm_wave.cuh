@@ -158,37 +158,46 @@ template <typename R, typename Sink> CM_D void cm_trace(const RunView<R>& v, con
 // region check, MONSEL_MaterialScatterModel::randomMeanPathLength, the
 // candidate point, RegionBase::findEndOfStep, the slowing-down loss, the
 // tracking cut; the step's end is queued for its event kernel, escapes are tallied.
+// One step's flight on a record held in registers (p, d, E, step, region, key and pixel valid): the
+// event queue of its end, or -1 when the electron ended here (escaped and tallied, stopped, trapped).
 template <typename R, int D, typename Sink>
-CM_D void flight_one(const RunView<R>& v, int cur, int i, Sink& sink, StepCounts& sc) {
+CM_D int flight_apply(const RunView<R>& v, El<R>& e, Sink& sink, StepCounts& sc) {
   const SceneView<R>& s = v.s;
-  const Wave<R>& W = v.w[cur];
-  El<R> e = load(W, i);
   int reg = e.region;
   if (reg < 0 || !shape_contains<R, D>(s, s.regions[reg].shape, e.p)) reg = containing_subregion<R, D>(s, s.chamber, e.p);
-  if (reg < 0) return;
+  if (reg < 0) return -1;
   const Msm& m = s.msms[s.regions[reg].msm];
-  Rng<R> g(e.key, e.step, 0);
-  R cum[kMaxMech];
-  R total = 0;
-  const R logE = mlog(e.E);
-  for (int k = 0; k < m.nmech; ++k) {
-    total += mech_rate(s, s.mechs[m.mech0 + k], e.E, logE);
-    cum[k] = total;
-  }
   bool complete = false;
   double fp = 2.0 * kChamberRadiusNm;
-  if (total != R(0)) {
-    const R f = -mlog(g.next()) / total;
-    if ((double)f < fp) fp = (double)f;
-  } else if (e.step > 1000000u) {  // MONSEL_MaterialScatterModel::randomMeanPathLength (:86-90)
-    complete = true;
-  } else if (!(e.E > R(0)) && e.step > 4096u) {
-    // With no energy and no mechanism an electron only flies straight and is reflected by every
-    // barrier it meets (ExpQMBarrierSM: perpE = 0 never transmits); trapped between two walls it
-    // bounces until the 1e6-step limit above, one wave iteration per bounce.  It is ended here
-    // once it has taken 4096 steps (one that would have reached the chamber later, tallied at
-    // 0 eV, is lost; that needs more than 4096 steps and never occurred in the tests).
-    complete = true;
+  R total = 0;
+  int idx = 0, kind = 0;
+  {
+    Rng<R> g(e.key, e.step, 0);
+    R cum[kMaxMech];
+    const R logE = mlog(e.E);
+    for (int k = 0; k < m.nmech; ++k) {
+      total += mech_rate(s, s.mechs[m.mech0 + k], e.E, logE);
+      cum[k] = total;
+    }
+    if (total != R(0)) {
+      const R f = -mlog(g.next()) / total;
+      if ((double)f < fp) fp = (double)f;
+      // MONSEL_MaterialScatterModel::scatter (:93-134) picks the mechanism from the rates at the
+      // step's starting energy with the stream's next deviate; it is drawn here, before the
+      // geometry, so that the rates need not stay live (nothing else draws from this stream)
+      const R r = g.next() * total;
+      while (idx < m.nmech - 1 && cum[idx] < r) ++idx;
+      kind = s.mechs[m.mech0 + idx].kind;
+    } else if (e.step > 1000000u) {  // MONSEL_MaterialScatterModel::randomMeanPathLength (:86-90)
+      complete = true;
+    } else if (!(e.E > R(0)) && e.step > 4096u) {
+      // With no energy and no mechanism an electron only flies straight and is reflected by every
+      // barrier it meets (ExpQMBarrierSM: perpE = 0 never transmits); trapped between two walls it
+      // bounces until the 1e6-step limit above, one wave iteration per bounce.  It is ended here
+      // once it has taken 4096 steps (one that would have reached the chamber later, tallied at
+      // 0 eV, is lost; that needs more than 4096 steps and never occurred in the tests).
+      complete = true;
+    }
   }
   double p1[3] = {e.p[0] + fp * (double)e.d[0], e.p[1] + fp * (double)e.d[1], e.p[2] + fp * (double)e.d[2]};
   double hn[3];
@@ -203,7 +212,7 @@ CM_D void flight_one(const RunView<R>& v, int cur, int i, Sink& sink, StepCounts
   e.step += 1;
   e.region = reg;
   ++sc.steps;
-  if ((e.E < (R)m.minE) || complete) return;
+  if ((e.E < (R)m.minE) || complete) return -1;
   int queue;
   if (next == reg) {
     ++sc.scat;
@@ -221,12 +230,7 @@ CM_D void flight_one(const RunView<R>& v, int cur, int i, Sink& sink, StepCounts
       queue = Q_MISC;
       e.aux = aux_pack(AUX_PASS, 0);
     } else {
-      // MONSEL_MaterialScatterModel::scatter (:93-134): the cache holds the step's starting energy
-      const R r = g.next() * total;
-      int idx = 0;
-      while (idx < m.nmech - 1 && cum[idx] < r) ++idx;
-      const int kind = s.mechs[m.mech0 + idx].kind;
-      if (kind == MECH_POLARON) return;  // GanachaudMokraniPolaronTrapSM::scatter: trapped, E = 0
+      if (kind == MECH_POLARON) return -1;  // GanachaudMokraniPolaronTrapSM::scatter: trapped, E = 0
       queue = kind == MECH_NISTMOTT ? Q_EL : kind == MECH_TABULATED ? Q_TAB : Q_MISC;
       e.aux = aux_pack(AUX_MECH, idx);
     }
@@ -239,15 +243,36 @@ CM_D void flight_one(const RunView<R>& v, int cur, int i, Sink& sink, StepCounts
     ++sc.esc;
     tally_escape(v, e, sink);
 #ifdef CM_TRACE
-    queue = 9;
-    cm_trace(v, e, next, queue, sink);
+    cm_trace(v, e, next, 9, sink);
 #endif
-    return;
+    return -1;
   }
 #ifdef CM_TRACE
   cm_trace(v, e, next, queue * 100 + aux_kind(e.aux) * 10 + aux_val(e.aux) % 10, sink);
 #endif
-  store(W, i, e);
+  return queue;
+}
+
+// The flight of wave slot i: reads what the step uses and writes back only what it changes
+// (direction, pixel and key stay in place for the event kernels), then queues the event.
+template <typename R, int D, typename Sink>
+CM_D void flight_one(const RunView<R>& v, int cur, int i, Sink& sink, StepCounts& sc) {
+  const Wave<R>& W = v.w[cur];
+  El<R> e;
+  e.p[0] = W.px[i]; e.p[1] = W.py[i]; e.p[2] = W.pz[i];
+  e.d[0] = W.dx[i]; e.d[1] = W.dy[i]; e.d[2] = W.dz[i];
+  e.E = W.E[i];
+  e.step = W.step[i];
+  e.region = W.region[i];
+  e.key = W.key[i];
+  e.pixel = W.pixel[i];
+  const int queue = flight_apply<R, D>(v, e, sink, sc);
+  if (queue < 0) return;
+  W.px[i] = e.p[0]; W.py[i] = e.p[1]; W.pz[i] = e.p[2];
+  W.E[i] = e.E; W.Ep[i] = e.Ep;
+  W.region[i] = e.region; W.aux[i] = e.aux;
+  W.step[i] = e.step;
+  if (aux_kind(e.aux) == AUX_BARRIER) { W.hx[i] = e.h[0]; W.hy[i] = e.h[1]; W.hz[i] = e.h[2]; }
   const int slot = sink.append_q(v.c->q, queue);
   v.q[queue][slot] = i;
 }
@@ -299,35 +324,34 @@ CM_D void push_secondary(const RunView<R>& v, const El<R>& pe, const R sd[3], R 
   ++sc.sec;
 }
 
+// The events of a step on a record in registers (after its flight: step already counted, so the
+// event's stream is (key, step - 1, 1)).  Each returns whether the electron lives on.
+
 // SelectableElasticSM events
-template <typename R, typename Sink> CM_D void elastic_one(const RunView<R>& v, int cur, int j, Sink& sink) {
+template <typename R> CM_D bool elastic_apply(const RunView<R>& v, El<R>& e) {
   const SceneView<R>& s = v.s;
-  El<R> e = load(v.w[cur], v.q[Q_EL][j]);
   const Msm& m = s.msms[s.regions[e.region].msm];
   const Mech& k = s.mechs[m.mech0 + aux_val(e.aux)];
   Rng<R> g(e.key, e.step - 1, 1);
   elastic_scatter(s, k, e.d, e.Ep, g);
-  if (!(e.E < (R)m.minE)) keep(v, cur ^ 1, e, sink);
+  return !(e.E < (R)m.minE);
 }
 
 // TabulatedInelasticSM events
-template <typename R, typename Sink> CM_D void inelastic_one(const RunView<R>& v, int cur, int j, Sink& sink, StepCounts& sc) {
+template <typename R, typename Sink> CM_D bool inelastic_apply(const RunView<R>& v, El<R>& e, Sink& sink, StepCounts& sc) {
   const SceneView<R>& s = v.s;
-  El<R> e = load(v.w[cur], v.q[Q_TAB][j]);
   const Msm& m = s.msms[s.regions[e.region].msm];
   const Mech& k = s.mechs[m.mech0 + aux_val(e.aux)];
   Rng<R> g(e.key, e.step - 1, 1);
   R sd[3], sE;
   const bool made = tabulated_scatter(s, k, e.d, e.E, sd, sE, g);
-  if (!(e.E < (R)m.minE)) keep(v, cur ^ 1, e, sink);
   if (made) push_secondary(v, e, sd, sE, sink, sc);
+  return !(e.E < (R)m.minE);
 }
 
 // barrier crossings, FittedInelSM, phonon, and steps that end without a mechanism
-template <typename R, int D, typename Sink>
-CM_D void misc_one(const RunView<R>& v, int cur, int j, Sink& sink, StepCounts& sc) {
+template <typename R, int D, typename Sink> CM_D bool misc_apply(const RunView<R>& v, El<R>& e, Sink& sink, StepCounts& sc) {
   const SceneView<R>& s = v.s;
-  El<R> e = load(v.w[cur], v.q[Q_MISC][j]);
   const Msm& m = s.msms[s.regions[e.region].msm];
   const int kind = aux_kind(e.aux);
   Rng<R> g(e.key, e.step - 1, 1);
@@ -339,8 +363,7 @@ CM_D void misc_one(const RunView<R>& v, int cur, int j, Sink& sink, StepCounts& 
     e.p[1] += kSmallDispNm * (double)e.d[1];
     e.p[2] += kSmallDispNm * (double)e.d[2];
     if (!shape_contains<R, D>(s, s.regions[e.region].shape, e.p)) e.region = containing_subregion<R, D>(s, s.chamber, e.p);
-    keep(v, cur ^ 1, e, sink);
-    return;
+    return true;
   }
   if (kind == AUX_MECH) {
     const Mech& k = s.mechs[m.mech0 + aux_val(e.aux)];
@@ -354,7 +377,40 @@ CM_D void misc_one(const RunView<R>& v, int cur, int j, Sink& sink, StepCounts& 
       phonon_scatter(k, e.d, e.E, e.Ep, g);
     }
   }
-  if (!(e.E < (R)m.minE)) keep(v, cur ^ 1, e, sink);
+  return !(e.E < (R)m.minE);
+}
+
+// the queue kernels' events: the record of queue entry j, its event, and the survivor kept
+template <typename R, typename Sink> CM_D void elastic_one(const RunView<R>& v, int cur, int j, Sink& sink) {
+  El<R> e = load(v.w[cur], v.q[Q_EL][j]);
+  if (elastic_apply(v, e)) keep(v, cur ^ 1, e, sink);
+}
+
+template <typename R, typename Sink> CM_D void inelastic_one(const RunView<R>& v, int cur, int j, Sink& sink, StepCounts& sc) {
+  El<R> e = load(v.w[cur], v.q[Q_TAB][j]);
+  if (inelastic_apply(v, e, sink, sc)) keep(v, cur ^ 1, e, sink);
+}
+
+template <typename R, int D, typename Sink>
+CM_D void misc_one(const RunView<R>& v, int cur, int j, Sink& sink, StepCounts& sc) {
+  El<R> e = load(v.w[cur], v.q[Q_MISC][j]);
+  if (misc_apply<R, D>(v, e, sink, sc)) keep(v, cur ^ 1, e, sink);
+}
+
+// Up to nsteps whole steps (flight and event) of wave slot i in one thread, the survivor kept.  The
+// tail of a run, when too few electrons are left to fill the GPU, goes this way: the same steps
+// with the same random streams as the queue kernels, without a launch and a queue per event.
+template <typename R, int D, typename Sink>
+CM_D void steps_one(const RunView<R>& v, int cur, int i, int nsteps, Sink& sink, StepCounts& sc) {
+  El<R> e = load(v.w[cur], i);
+  for (int k = 0; k < nsteps; ++k) {
+    const int q = flight_apply<R, D>(v, e, sink, sc);
+    if (q < 0) return;
+    const bool alive = q == Q_EL ? elastic_apply(v, e) : q == Q_TAB ? inelastic_apply(v, e, sink, sc)
+                                                                    : misc_apply<R, D>(v, e, sink, sc);
+    if (!alive) return;
+  }
+  keep(v, cur ^ 1, e, sink);
 }
 
 // refill plan of the next wave: secondaries from the pool first; new primaries

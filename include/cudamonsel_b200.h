@@ -154,6 +154,9 @@ typedef struct {
   double kernel_ms[6];         /* per kernel, summed over launches (profile != 0 only) */
   int64_t kernel_launches[6];
   int64_t units[4];            /* electrons handled by flight, elastic, inelastic, misc */
+  int64_t step_launches;       /* launches of the several-steps-per-thread kernel that runs the tail of a
+                                  run (when fewer electrons are left than fill the GPU); the queue kernels
+                                  flight .. misc do not run in those iterations */
 } cm_run_stats;
 
 /* back/fwd: [npix * hist_stride] counts, index = histogram bin + 1 (0 = underflow,
