@@ -284,22 +284,23 @@ def main():
     steps_total = sum(s.steps for s in stats)
     launches = sum(sum(int(x) for x in s.kernel_launches) + int(s.step_launches) for s in stats)
     # roofline of the dominant kernel: one more step of the same workload with CUDA events
-    # between the kernels of every iteration (event nodes inside the captured graph); a profiled
-    # run keeps the queue kernels to the end (no several-steps-per-thread tail), so its shares
-    # are those of the queue kernels
+    # between the kernels of every iteration (event nodes inside the captured graphs); the tail
+    # iterations run k_steps ("steps" in the shares), the others the six queue kernels
     flush.zero_()
     prof = [step(prec, profile=1)]
     torch.cuda.synchronize()
     kms = np.zeros(6)
     units = np.zeros(4)
+    step_ms = 0.0
     for s in prof:
         kms += np.array(list(s.kernel_ms))
         units += np.array(list(s.units))
+        step_ms += s.step_ms
     names = capi.RunStats.KERNELS
     dom = int(np.argmax(kms[:4]))
-    nlaunch = sum(int(s.iterations) for s in prof)
+    nlaunch = sum(int(s.kernel_launches[dom]) for s in prof)
     per_launch_units = units[dom] / max(1, nlaunch)
-    avg_ms = kms[dom] / max(1, sum(int(s.kernel_launches[dom]) for s in prof))
+    avg_ms = kms[dom] / max(1, nlaunch)
     achieved = units[dom] * BYTES_PER_STEP / (kms[dom] / 1000.0) / 1e9
     peak, peak_kind = peaks()
     traffic = None
@@ -417,7 +418,8 @@ def main():
                              "unit": "GB/s", "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
                              "bytes_per_unit": BYTES_PER_STEP, "units_per_launch": per_launch_units,
                              "avg_launch_ms": avg_ms},
-                "kernel_ms_share": {n: float(v / kms.sum()) for n, v in zip(names, kms)},
+                "kernel_ms_share": dict({n: float(v / (kms.sum() + step_ms)) for n, v in zip(names, kms)},
+                                        steps=float(step_ms / (kms.sum() + step_ms))),
                 "clocks": clk, "gpu_launches": launches,
                 "e2e": {"value": e2e_value, "unit": "primaries/s", "h2d_bytes_per_step": h2d,
                         "d2h_bytes_per_step": d2h},

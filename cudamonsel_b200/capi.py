@@ -15,6 +15,9 @@ LIBPATH = os.path.join(HERE, "libcudamonsel_b200.so")
 PREC_FP64 = 0
 PREC_FP32 = 1
 OPT_JMONSEL_FIXES = 1
+OPT_EXACT_CSG = 2
+OPT_SCAN_CHILDREN = 4
+OPT_QUEUE_STEPS = 8
 
 # every symbol include/cudamonsel_b200.h declares
 EXPORTS = (
@@ -48,7 +51,8 @@ class RunStats(C.Structure):
     _fields_ = [("primaries", C.c_int64), ("steps", C.c_int64), ("scatter_events", C.c_int64),
                 ("barrier_events", C.c_int64), ("escapes", C.c_int64), ("secondaries", C.c_int64),
                 ("iterations", C.c_int64), ("device_ms", C.c_double), ("kernel_ms", C.c_double * 6),
-                ("kernel_launches", C.c_int64 * 6), ("units", C.c_int64 * 4), ("step_launches", C.c_int64)]
+                ("kernel_launches", C.c_int64 * 6), ("units", C.c_int64 * 4), ("step_launches", C.c_int64),
+                ("step_units", C.c_int64), ("step_ms", C.c_double)]
 
     KERNELS = ("flight", "elastic", "inelastic", "misc", "spawn", "tail")
 
@@ -58,6 +62,8 @@ class RunStats(C.Structure):
         d["kernel_launches"] = dict(zip(self.KERNELS, list(self.kernel_launches)))
         d["units"] = dict(zip(self.KERNELS[:4], list(self.units)))
         d["step_launches"] = self.step_launches
+        d["step_units"] = self.step_units
+        d["step_ms"] = self.step_ms
         return d
 
 

@@ -813,13 +813,18 @@ static void launch_flight(const RunView<float>& v, int cur, int grid, cudaStream
 // through CM_TAIL_STEPS whole steps per iteration (k_steps) instead of one step through the queue
 // kernels, whose launches and queue traffic then cost more than the steps themselves.
 #ifndef CM_TAIL_BELOW
-#define CM_TAIL_BELOW 65536
+#define CM_TAIL_BELOW 262144
 #endif
 #ifndef CM_TAIL_STEPS
-#define CM_TAIL_STEPS 8
+#define CM_TAIL_STEPS 32
+#endif
+#if defined(CM_MINB_STEPS)
+#define CM_LB_STEPS __launch_bounds__(256, CM_MINB_STEPS)
+#else
+#define CM_LB_STEPS __launch_bounds__(256)
 #endif
 
-template <typename R, int D> __global__ void __launch_bounds__(256) k_steps(RunView<R> v, int cur, int nsteps) {
+template <typename R, int D> __global__ void CM_LB_STEPS k_steps(RunView<R> v, int cur, int nsteps) {
   DeviceSink sink;
   StepCounts sc;
   const int n = v.c->n[cur];
@@ -864,8 +869,8 @@ template <typename R> static void launch_spawn(const RunView<R>& v, int cur, int
 }
 
 template <typename R>
-__global__ void k_tail(RunView<R> v, int cur) {
-  if (blockIdx.x == 0 && threadIdx.x == 0) tail_update(v.c, cur, v.W, v.poolCap);
+__global__ void k_tail(RunView<R> v, int cur, int steps) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) tail_update(v.c, cur, v.W, v.poolCap, steps != 0);
 }
 
 #ifdef CM_TRACE
@@ -988,16 +993,19 @@ static int run_device_once(cm_context* ctx, const cm_run_desc* d, uint32_t* back
     if (ev) cudaEventRecordWithFlags(ev[3], stream, cudaEventRecordExternal);
     launch_spawn<R>(v, cur, grid, stream);
     if (ev) cudaEventRecordWithFlags(ev[4], stream, cudaEventRecordExternal);
-    k_tail<R><<<1, 32, 0, stream>>>(v, cur);
+    k_tail<R><<<1, 32, 0, stream>>>(v, cur, 0);
     if (ev) cudaEventRecordWithFlags(ev[5], stream, cudaEventRecordExternal);
   }
   CM_CUDA(cudaStreamEndCapture(stream, &graph));
   CM_CUDA(cudaGraphInstantiate(&exec, graph, 0));
-  // the tail graph (k_steps, spawn, tail per iteration), captured when first wanted
+  // the tail graph (k_steps, spawn, tail per iteration), captured when first wanted; profiled, with an
+  // event before the first kernel and after each kernel of every iteration
   cudaGraph_t tgraph = nullptr;
   cudaGraphExec_t texec = nullptr;
   bool tail = false;
   int titers = 0;
+  std::vector<cudaEvent_t> tev;
+  double step_ms = 0;
   CM_CUDA(cudaEventRecord(e0, stream));
   int iters = 0;
   int status = 0;
@@ -1007,13 +1015,21 @@ static int run_device_once(cm_context* ctx, const cm_run_desc* d, uint32_t* back
     if (tail) titers += 2 * K;
     CM_CUDA(cudaMemcpyAsync(ctx->counters_host, ctx->counters, sizeof(Counters), cudaMemcpyDeviceToHost, stream));
     CM_CUDA(cudaStreamSynchronize(stream));
-    if (d->profile) {
+    if (d->profile && !tail) {
       for (int it = 0; it < 2 * K; ++it)
         for (int k = 0; k < 6; ++k) {
           float t = 0;
           cudaEventElapsedTime(&t, pev[(size_t)it * 6 + k], pev[(size_t)it * 6 + k + 1]);
           kms[k] += t;
         }
+    } else if (d->profile) {
+      for (int it = 0; it < 2 * K; ++it) {
+        float t[3] = {0, 0, 0};
+        for (int k = 0; k < 3; ++k) cudaEventElapsedTime(&t[k], tev[(size_t)it * 3 + k], tev[(size_t)it * 3 + k + 1]);
+        step_ms += t[0];
+        kms[CM_K_SPAWN] += t[1];
+        kms[CM_K_TAIL] += t[2];
+      }
     }
     if (ctx->counters_host->error) {
       status = fail(ctx->counters_host->error, "secondary pool overflow; raise the wave size");
@@ -1025,18 +1041,27 @@ static int run_device_once(cm_context* ctx, const cm_run_desc* d, uint32_t* back
       break;
     }
     {
-      // all primaries started and fewer electrons left (waves and pool) than CM_TAIL_BELOW: tail graph.
-      // Profiled runs keep the queue kernels throughout, so that each kernel's time is measured.
+      // all primaries started and fewer electrons left (waves and pool) than CM_TAIL_BELOW: tail graph
+      // (unless CM_OPT_QUEUE_STEPS keeps the queue kernels to the end)
       const Counters& hc = *ctx->counters_host;
       const long long left = (long long)hc.n[0] + hc.n[1] + std::min(hc.pool, v.poolCap);
-      tail = !d->profile && hc.next_primary == hc.total_primaries && left < CM_TAIL_BELOW;
+      tail = !(ctx->options & CM_OPT_QUEUE_STEPS) && hc.next_primary == hc.total_primaries && left < CM_TAIL_BELOW;
       if (tail && !texec) {
+        if (d->profile) {
+          tev.resize((size_t)2 * K * 3 + 1);
+          for (auto& ev : tev) CM_CUDA(cudaEventCreate(&ev));
+        }
         CM_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+        if (d->profile) cudaEventRecordWithFlags(tev[0], stream, cudaEventRecordExternal);
         for (int it = 0; it < 2 * K; ++it) {
           const int cur = it & 1;
+          cudaEvent_t* ev = d->profile ? &tev[(size_t)it * 3 + 1] : nullptr;
           launch_steps(v, cur, grid, stream);
+          if (ev) cudaEventRecordWithFlags(ev[0], stream, cudaEventRecordExternal);
           launch_spawn<R>(v, cur, grid, stream);
-          k_tail<R><<<1, 32, 0, stream>>>(v, cur);
+          if (ev) cudaEventRecordWithFlags(ev[1], stream, cudaEventRecordExternal);
+          k_tail<R><<<1, 32, 0, stream>>>(v, cur, 1);
+          if (ev) cudaEventRecordWithFlags(ev[2], stream, cudaEventRecordExternal);
         }
         CM_CUDA(cudaStreamEndCapture(stream, &tgraph));
         CM_CUDA(cudaGraphInstantiate(&texec, tgraph, 0));
@@ -1078,6 +1103,7 @@ static int run_device_once(cm_context* ctx, const cm_run_desc* d, uint32_t* back
   if (texec) cudaGraphExecDestroy(texec);
   if (tgraph) cudaGraphDestroy(tgraph);
   for (auto& ev : pev) cudaEventDestroy(ev);
+  for (auto& ev : tev) cudaEventDestroy(ev);
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   CM_CUDA(cudaGetLastError());
@@ -1097,6 +1123,8 @@ static int run_device_once(cm_context* ctx, const cm_run_desc* d, uint32_t* back
     }
     for (int k = 0; k < 4; ++k) st->units[k] = (int64_t)c.units[k];
     st->step_launches = titers;
+    st->step_units = (int64_t)c.step_units;
+    st->step_ms = step_ms;
   }
   return status;
 }
@@ -2201,7 +2229,7 @@ static int run_noalloc(cm_context* ctx, const cm_run_desc* d, uint32_t* back, ui
       k_inelastic<R><<<grid, 256, 0, s>>>(v, cur);
       launch_misc<R>(v, cur, grid, s);
       launch_spawn<R>(v, cur, grid, s);
-      k_tail<R><<<1, 32, 0, s>>>(v, cur);
+      k_tail<R><<<1, 32, 0, s>>>(v, cur, 0);
     }
     CM_CUDA(cudaGetLastError());
     CM_CUDA(cudaMemcpyAsync(&hc, c, sizeof(Counters), cudaMemcpyDeviceToHost, s));

@@ -34,6 +34,7 @@ struct Counters {
   unsigned long long steps, scatters, barriers, escapes, secondaries;
   unsigned long long iterations;
   unsigned long long units[4];
+  unsigned long long step_units;  // electrons the several-steps kernel started with
 };
 
 template <typename R>
@@ -470,14 +471,15 @@ CM_D void spawn_one(const RunView<R>& v, int nxt, int j, int take_se, int poolTo
   store(v.w[nxt], seg * v.W + v.c->nc[nxt][seg] + sink.append_q(v.c->ns, seg), e);
 }
 
-// end of an iteration: counters of the next wave, reset of this one
-CM_D void tail_update(Counters* c, int cur, int W, int poolCap) {
+// end of an iteration: counters of the next wave, reset of this one (steps: the iteration ran k_steps)
+CM_D void tail_update(Counters* c, int cur, int W, int poolCap, bool steps) {
   const int nxt = cur ^ 1;
   int nn, take_se, take_p;
   refill_plan(c, nxt, W, poolCap, nn, take_se, take_p);
   if (c->pool > poolCap) c->pool = poolCap;
   if (!c->done) {
-    c->units[0] += (unsigned long long)c->n[cur];
+    if (steps) c->step_units += (unsigned long long)c->n[cur];
+    else c->units[0] += (unsigned long long)c->n[cur];
     c->units[1] += (unsigned long long)c->q[0];
     c->units[2] += (unsigned long long)c->q[1];
     c->units[3] += (unsigned long long)c->q[2];

@@ -46,6 +46,9 @@ extern "C" {
                                   FP32 merges intersections of plane sets into single plane sets */
 #define CM_OPT_SCAN_CHILDREN 4 /* test every child of a region in order, as RegionBase does; by default a region
                                   with many children finds them through an x-y grid (same results) */
+#define CM_OPT_QUEUE_STEPS 8   /* one step per iteration through the queue kernels to the end of a run; by default
+                                  the tail of a run (fewer electrons left than fill the GPU) takes several whole
+                                  steps per thread (same results) */
 
 typedef struct cm_context cm_context;
 
@@ -157,6 +160,8 @@ typedef struct {
   int64_t step_launches;       /* launches of the several-steps-per-thread kernel that runs the tail of a
                                   run (when fewer electrons are left than fill the GPU); the queue kernels
                                   flight .. misc do not run in those iterations */
+  int64_t step_units;          /* electrons those launches started with */
+  double step_ms;              /* their time (profile != 0 only) */
 } cm_run_stats;
 
 /* back/fwd: [npix * hist_stride] counts, index = histogram bin + 1 (0 = underflow,

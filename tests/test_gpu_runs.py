@@ -296,18 +296,24 @@ def test_deep_features_match_oracle(prec):
 @pytest.mark.parametrize("prec", [FP64, FP32], ids=["fp64", "fp32"])
 def test_tail_steps_give_the_same_tallies(prec):
     """The tail of a run (fewer electrons left than fill the GPU) runs several whole steps per thread
-    (k_steps); a profiled run keeps the queue kernels to the end.  Same seed: identical tallies."""
+    (k_steps); CM_OPT_QUEUE_STEPS keeps the queue kernels to the end, and a profiled run times each
+    kernel.  Same seed: identical tallies all three ways."""
     from cudamonsel_b200 import capi, scenes
     e = capi.Engine(0)
     h = scenes.build_engine(scenes.lines(), e)
     c = scenes.linescan_pixels(64)
     b0, f0, s0 = e.run(h["chamber"], c, scenes.eV(500.0), 300, 50, 1e-9, seed=9, precision=prec)
-    b1, f1, s1 = e.run(h["chamber"], c, scenes.eV(500.0), 300, 50, 1e-9, seed=9, precision=prec, profile=1)
+    b2, f2, s2 = e.run(h["chamber"], c, scenes.eV(500.0), 300, 50, 1e-9, seed=9, precision=prec, profile=1)
+    e.set_options(capi.OPT_QUEUE_STEPS)
+    b1, f1, s1 = e.run(h["chamber"], c, scenes.eV(500.0), 300, 50, 1e-9, seed=9, precision=prec)
     e.close()
-    print("steps %d, tail launches %d of %d iterations" % (s0.steps, s0.step_launches, s0.iterations))
-    assert s0.step_launches > 0 and s1.step_launches == 0
-    assert s0.steps == s1.steps and s0.secondaries == s1.secondaries
-    assert np.array_equal(b0, b1) and np.array_equal(f0, f1)
+    print("steps %d, tail launches %d of %d iterations, %d electrons started in k_steps" % (
+        s0.steps, s0.step_launches, s0.iterations, s0.step_units))
+    assert s0.step_launches > 0 and s1.step_launches == 0 and s2.step_launches > 0
+    assert s2.step_ms > 0 and s2.kernel_ms[0] > 0 and s1.step_units == 0
+    for b, f, s in ((b1, f1, s1), (b2, f2, s2)):
+        assert s0.steps == s.steps and s0.secondaries == s.secondaries
+        assert np.array_equal(b0, b) and np.array_equal(f0, f)
 
 
 def test_deterministic_and_independent_of_batch(half):
