@@ -39,7 +39,15 @@ class RunDesc(C.Structure):
                 ("pixel_center", C.POINTER(C.c_double)), ("pixel_energy", C.POINTER(C.c_double)),
                 ("pixel_nprim", C.POINTER(C.c_int)), ("pixel_nbins", C.POINTER(C.c_int)), ("seed", C.c_uint64),
                 ("hist_stride", C.c_int), ("wave", C.c_int), ("max_iterations", C.c_int),
-                ("pixel_key", C.POINTER(C.c_uint64)), ("profile", C.c_int)]
+                ("pixel_key", C.POINTER(C.c_uint64)), ("profile", C.c_int),
+                ("elevation", C.POINTER(C.c_uint32)), ("azimuth", C.POINTER(C.c_uint32)),
+                ("escape_log", C.c_void_p), ("escape_log_cap", C.c_int64)]
+
+
+ELEVATION_COUNTS, AZIMUTH_COUNTS = 182, 362
+# cm_escape_record
+ESCAPE_RECORD = np.dtype([("electron", np.uint64), ("pixel", np.int32), ("step", np.int32), ("energy_eV", np.float64),
+                          ("position", np.float64, 3), ("theta", np.float64), ("phi", np.float64)])
 
 
 class JobInfo(C.Structure):
@@ -265,7 +273,9 @@ class Engine:
 
     # ---- runs
     def run(self, chamber, centers, energies, nprim, nbins, beam_width, seed, precision=PREC_FP64, wave=0,
-            max_iterations=0, pixel_keys=None, profile=0):
+            max_iterations=0, pixel_keys=None, profile=0, angles=False, escape_log_cap=0):
+        """cm_run: (back, fwd, stats); with angles or an escape log also a dict of BackscatterStats'
+        elevation [npix, 182] and azimuthal [npix, 362] histograms and the escape records."""
         centers = np.ascontiguousarray(centers, dtype=np.float64).reshape(-1, 3)
         npix = len(centers)
         e, pe = _d(np.broadcast_to(np.asarray(energies, dtype=np.float64), (npix,)).copy())
@@ -278,12 +288,28 @@ class Engine:
             keys = np.ascontiguousarray(pixel_keys, dtype=np.uint64)
         desc = RunDesc(chamber, precision, npix, beam_width, pc, pe, pn, pb, seed, stride, wave, max_iterations,
                        keys.ctypes.data_as(C.POINTER(C.c_uint64)) if keys is not None else None, profile)
+        extra = None
+        if angles or escape_log_cap:
+            extra = {}
+            if angles:
+                extra["elevation"] = np.zeros((npix, ELEVATION_COUNTS), dtype=np.uint32)
+                extra["azimuth"] = np.zeros((npix, AZIMUTH_COUNTS), dtype=np.uint32)
+                desc.elevation = extra["elevation"].ctypes.data_as(C.POINTER(C.c_uint32))
+                desc.azimuth = extra["azimuth"].ctypes.data_as(C.POINTER(C.c_uint32))
+            if escape_log_cap:
+                log = np.zeros(int(escape_log_cap), dtype=ESCAPE_RECORD)
+                desc.escape_log = log.ctypes.data
+                desc.escape_log_cap = int(escape_log_cap)
         back = np.zeros((npix, stride), dtype=np.uint32)
         fwd = np.zeros((npix, stride), dtype=np.uint32)
         st = RunStats()
         self._check(self.L.cm_run(self.h, C.byref(desc), back.ctypes.data_as(C.POINTER(C.c_uint32)),
                                   fwd.ctypes.data_as(C.POINTER(C.c_uint32)), C.byref(st)))
-        return back, fwd, st
+        if extra is None:
+            return back, fwd, st
+        if escape_log_cap:
+            extra["escape_log"] = log[:min(int(escape_log_cap), int(st.escapes))]
+        return back, fwd, st, extra
 
     def run_device(self, desc, back_ptr, fwd_ptr, stream_ptr=None):
         st = RunStats()

@@ -703,6 +703,7 @@ struct DeviceSink {
     return base + (int)part.thread_rank();
   }
   __device__ __forceinline__ void count(uint32_t* h) { atomicAdd(h, 1u); }
+  __device__ __forceinline__ unsigned long long ticket(unsigned long long* c) { return atomicAdd(c, 1ull); }
   __device__ __forceinline__ void error(int* e, int code) { atomicExch(e, code); }
 };
 
@@ -957,6 +958,10 @@ static int run_device_once(cm_context* ctx, const cm_run_desc* d, uint32_t* back
   v.back = back;
   v.fwd = fwd;
   v.stride = d->hist_stride;
+  v.elev = d->elevation && d->azimuth ? d->elevation : nullptr;
+  v.azim = v.elev ? d->azimuth : nullptr;
+  v.log = d->escape_log && d->escape_log_cap > 0 ? d->escape_log : nullptr;
+  v.logCap = v.log ? d->escape_log_cap : 0;
 
   Counters c0;
   memset(&c0, 0, sizeof(c0));
@@ -1129,6 +1134,14 @@ static int run_device_once(cm_context* ctx, const cm_run_desc* d, uint32_t* back
   return status;
 }
 
+// zero the angle histograms a run tallies into (device arrays)
+static int clear_angles(const cm_run_desc* d, cudaStream_t s) {
+  if (!d->elevation || !d->azimuth) return 0;
+  CM_CUDA(cudaMemsetAsync(d->elevation, 0, (size_t)d->npix * CM_ELEVATION_COUNTS * sizeof(uint32_t), s));
+  CM_CUDA(cudaMemsetAsync(d->azimuth, 0, (size_t)d->npix * CM_AZIMUTH_COUNTS * sizeof(uint32_t), s));
+  return 0;
+}
+
 // Every electron's random stream is keyed by its lineage, so a run that
 // overflowed the secondary pool is repeated with a larger pool and gives the
 // same tallies it would have given the first time.
@@ -1137,6 +1150,7 @@ static int run_device(cm_context* ctx, const cm_run_desc* d, uint32_t* back, uin
                       cudaStream_t stream, const unsigned long long* prefix_dev, const double* e0ref_dev,
                       const unsigned long long* pkey_dev, unsigned long long total) {
   const size_t hbytes = (size_t)d->npix * d->hist_stride * sizeof(uint32_t);
+  int rc_clear;
   for (int attempt = 0; attempt < 4; ++attempt) {
     const int rc = run_device_once<R>(ctx, d, back, fwd, st, stream, prefix_dev, e0ref_dev, pkey_dev, total);
     if (rc != CM_EOVERFLOW) return rc;
@@ -1148,6 +1162,7 @@ static int run_device(cm_context* ctx, const cm_run_desc* d, uint32_t* back, uin
     if ((e = ensure_buffers<R>(ctx, W, (int)want))) return e;
     CM_CUDA(cudaMemsetAsync(back, 0, hbytes, stream));
     CM_CUDA(cudaMemsetAsync(fwd, 0, hbytes, stream));
+    if ((rc_clear = clear_angles(d, stream))) return rc_clear;
   }
   return fail(CM_EOVERFLOW, "secondary pool overflow");
 }
@@ -1827,23 +1842,46 @@ int cm_run(cm_context* ctx, const cm_run_desc* d, uint32_t* back, uint32_t* fwd,
     return fail(CM_EINVAL, "null array");
   CM_CUDA(cudaSetDevice(ctx->device));
   const size_t hbytes = (size_t)d->npix * d->hist_stride * sizeof(uint32_t);
-  uint32_t *bdev = nullptr, *fdev = nullptr;
-  CM_CUDA(cudaMalloc(&bdev, hbytes));
-  if (cudaMalloc(&fdev, hbytes) != cudaSuccess) {
-    cudaFree(bdev);
-    return fail(CM_ENOMEM, "histogram allocation failed");
+  const bool angles = d->elevation && d->azimuth;
+  const bool logged = d->escape_log && d->escape_log_cap > 0;
+  const size_t ebytes = angles ? (size_t)d->npix * CM_ELEVATION_COUNTS * sizeof(uint32_t) : 0;
+  const size_t abytes = angles ? (size_t)d->npix * CM_AZIMUTH_COUNTS * sizeof(uint32_t) : 0;
+  const size_t lbytes = logged ? (size_t)d->escape_log_cap * sizeof(cm_escape_record) : 0;
+  // device copies of the tallies: back, fwd, and when asked the angle histograms and the escape log
+  std::vector<void*> bufs;
+  void* dev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+  const size_t sizes[5] = {hbytes, hbytes, ebytes, abytes, lbytes};
+  for (int k = 0; k < 5; ++k) {
+    if (!sizes[k]) continue;
+    if (cudaMalloc(&dev[k], sizes[k]) != cudaSuccess) {
+      for (void* p : bufs) cudaFree(p);
+      return fail(CM_ENOMEM, "tally allocation failed");
+    }
+    bufs.push_back(dev[k]);
+    cudaMemsetAsync(dev[k], 0, sizes[k], ctx->stream);
   }
-  cudaMemsetAsync(bdev, 0, hbytes, ctx->stream);
-  cudaMemsetAsync(fdev, 0, hbytes, ctx->stream);
-  rc = run_common(ctx, d, d->pixel_center, d->pixel_energy, d->pixel_nprim, d->pixel_nbins, nullptr, bdev, fdev, st,
-                  ctx->stream);
+  cm_run_desc dl = *d;
+  dl.elevation = (uint32_t*)dev[2];
+  dl.azimuth = (uint32_t*)dev[3];
+  dl.escape_log = (cm_escape_record*)dev[4];
+  rc = run_common(ctx, &dl, d->pixel_center, d->pixel_energy, d->pixel_nprim, d->pixel_nbins, nullptr, (uint32_t*)dev[0],
+                  (uint32_t*)dev[1], st, ctx->stream);
   if (!rc) {
-    cudaMemcpyAsync(back, bdev, hbytes, cudaMemcpyDeviceToHost, ctx->stream);
-    cudaMemcpyAsync(fwd, fdev, hbytes, cudaMemcpyDeviceToHost, ctx->stream);
+    cudaMemcpyAsync(back, dev[0], hbytes, cudaMemcpyDeviceToHost, ctx->stream);
+    cudaMemcpyAsync(fwd, dev[1], hbytes, cudaMemcpyDeviceToHost, ctx->stream);
+    if (angles) {
+      cudaMemcpyAsync(d->elevation, dev[2], ebytes, cudaMemcpyDeviceToHost, ctx->stream);
+      cudaMemcpyAsync(d->azimuth, dev[3], abytes, cudaMemcpyDeviceToHost, ctx->stream);
+    }
+    if (logged && st) {
+      const int64_t n = std::min<int64_t>(d->escape_log_cap, st->escapes);
+      cudaMemcpyAsync(d->escape_log, dev[4], (size_t)n * sizeof(cm_escape_record), cudaMemcpyDeviceToHost, ctx->stream);
+    } else if (logged) {
+      cudaMemcpyAsync(d->escape_log, dev[4], lbytes, cudaMemcpyDeviceToHost, ctx->stream);
+    }
     cudaStreamSynchronize(ctx->stream);
   }
-  cudaFree(bdev);
-  cudaFree(fdev);
+  for (void* p : bufs) cudaFree(p);
   if (!rc) CM_CUDA(cudaGetLastError());
   return rc;
 }
@@ -1883,6 +1921,7 @@ int cm_run_device(cm_context* ctx, const cm_run_desc* d, uint32_t* back, uint32_
   const size_t hbytes = (size_t)d->npix * d->hist_stride * sizeof(uint32_t);
   CM_CUDA(cudaMemsetAsync(back, 0, hbytes, s));
   CM_CUDA(cudaMemsetAsync(fwd, 0, hbytes, s));
+  if ((rc = clear_angles(d, s))) return rc;
   rc = run_common(ctx, d, c.data(), e.data(), np.data(), nb.data(), (int*)d->pixel_nbins, back, fwd, st, s);
   cudaEventRecord(eout, s);
   cudaStreamWaitEvent(caller, eout, 0);
@@ -2197,6 +2236,9 @@ static int run_noalloc(cm_context* ctx, const cm_run_desc* d, uint32_t* back, ui
   v.back = back;
   v.fwd = fwd;
   v.stride = d->hist_stride;
+  v.elev = v.azim = nullptr;  // not taken here (no room in the fixed scratch)
+  v.log = nullptr;
+  v.logCap = 0;
   // the array keeps the previous call's contents: the counters, the bad-input
   // flag and the caller's tallies start at zero; waves, queues and pool are
   // only read below the counts, so they need no clearing
@@ -2268,6 +2310,8 @@ extern "C" int cm_run_noalloc(cm_context* ctx, const cm_run_desc* d, uint32_t* b
                               cm_run_stats* stats, void* stream) {
   using namespace cm;
   int rc = check_desc(ctx, d);
+  if (!rc && (d->elevation || d->azimuth || d->escape_log))
+    rc = fail(CM_EINVAL, "cm_run_noalloc tallies the energy histograms only (no angle histograms or escape log)");
   if (rc) return rc;
   if (!d->pixel_center || !d->pixel_energy || !d->pixel_nprim || !d->pixel_nbins || !back || !fwd)
     return fail(CM_EINVAL, "null array");

@@ -260,6 +260,8 @@ int cm_job_submit(cm_server* srv, const cm_context* scene, const cm_run_desc* d,
     return fail(CM_EINVAL, "bad chamber handle");
   if (d->hist_stride < 3 || d->hist_stride > 1026) return fail(CM_EINVAL, "hist_stride out of range");
   if (!d->pixel_center || !d->pixel_energy || !d->pixel_nprim || !d->pixel_nbins) return fail(CM_EINVAL, "null array");
+  if (d->elevation || d->azimuth || d->escape_log)
+    return fail(CM_EINVAL, "jobs tally the energy histograms only (no angle histograms or escape log)");
   std::unique_ptr<JobRecord> j(new JobRecord());
   j->options = scene->options;
   j->mott = scene->mott;

@@ -35,6 +35,7 @@ struct Counters {
   unsigned long long iterations;
   unsigned long long units[4];
   unsigned long long step_units;  // electrons the several-steps kernel started with
+  unsigned long long logged;      // escapes offered to the escape log
 };
 
 template <typename R>
@@ -107,6 +108,9 @@ struct RunView {
   double width;          // nm
   uint32_t *back, *fwd;
   int stride;
+  uint32_t *elev, *azim;       // per-pixel angle histograms (182 and 362 counts), or null
+  cm_escape_record* log;       // escape log, or null
+  long long logCap;
 };
 
 // per-thread event counts, reduced once per warp by the kernels
@@ -130,13 +134,34 @@ CM_D int hist_bin(double max, int nbins, double val) {
   return l;
 }
 
-// BackscatterStats::actionPerformed for a BackscatterEvent (NISTMonte/BackscatterStats.cu:147-170)
+// BackscatterStats::actionPerformed for a BackscatterEvent (NISTMonte/BackscatterStats.cu:147-170):
+// elevation and azimuth histograms, the log, then the forward or back energy histogram
 template <typename R, typename Sink> CM_D void tally_escape(const RunView<R>& v, const El<R>& e, Sink& sink) {
   const int px = e.pixel;
   const double E0ref = v.pe0ref[px];
   double val = (double)e.E;
   if (e.E == (R)v.pe0[px]) val = E0ref;  // electrons that never lost energy carry E0 exactly, as in the reference
   const double elevation = (kPi / 2) - atan2(e.p[2], sqrt((e.p[0] * e.p[0]) + (e.p[1] * e.p[1])));
+  if (v.elev) {
+    double azimuth = atan2(e.p[1], e.p[0]);
+    if (azimuth < 0.0) azimuth = (2.0 * kPi) + azimuth;
+    const int be = hist_bin(kPi, 180, elevation) + 1, ba = hist_bin(2.0 * kPi, 360, azimuth) + 1;
+    if (be <= 181) sink.count(v.elev + (size_t)px * 182 + be);  // past the overflow slot: never counted
+    if (ba <= 361) sink.count(v.azim + (size_t)px * 362 + ba);
+  }
+  if (v.log) {
+    const unsigned long long k = sink.ticket(&v.c->logged);
+    if (k < (unsigned long long)v.logCap) {
+      cm_escape_record& r = v.log[k];
+      r.electron = e.key;
+      r.pixel = px;
+      r.step = (int)e.step;
+      r.energy_eV = val;
+      for (int j = 0; j < 3; ++j) r.position[j] = e.p[j] * 1e-9;
+      r.theta = atan2(sqrt((double)e.d[0] * (double)e.d[0] + (double)e.d[1] * (double)e.d[1]), (double)e.d[2]);
+      r.phi = atan2((double)e.d[1], (double)e.d[0]);
+    }
+  }
   const int nb = v.pnbins[px];
   const int b = hist_bin(E0ref, nb, val) + 1;
   if (b > nb + 1) return;  // past the overflow slot: the reference writes out of bounds and never counts it

@@ -141,7 +141,34 @@ typedef struct {
                                   A pixel's result depends only on its key, its beam and primary count,
                                   not on the other pixels of the run. */
   int profile;                 /* nonzero: time each kernel with CUDA events inside the loop */
+  /* BackscatterStats' elevation and azimuthal histograms (NISTMonte/BackscatterStats.cu:105-106,147-165:
+   * Histogram(0, pi, 180) of pi/2 - atan2(z, r) and Histogram(0, 2 pi, 360) of atan2(y, x) at the escape
+   * point), per pixel, or NULL: [npix * CM_ELEVATION_COUNTS] and [npix * CM_AZIMUTH_COUNTS] counts, index =
+   * bin + 1 as for back/fwd.  Every escape is counted, also those past the energy histogram's overflow slot.
+   * Host arrays for cm_run, device arrays for cm_run_device; not taken by cm_run_noalloc or the job server. */
+  uint32_t* elevation;
+  uint32_t* azimuth;
+  /* BackscatterStats' detected-electron log (setLogDetected, BackscatterStats.cu:166-168), or NULL: the first
+   * escape_log_cap escapes in arrival order (which varies from run to run); the run's stats.escapes says how
+   * many there were.  Host array for cm_run, device array for cm_run_device. */
+  struct cm_escape_record* escape_log;
+  int64_t escape_log_cap;
 } cm_run_desc;
+
+#define CM_ELEVATION_COUNTS 182 /* 180 bins + underflow + overflow */
+#define CM_AZIMUTH_COUNTS 362   /* 360 bins + underflow + overflow */
+
+/* BackscatterStats::Datum (BackscatterStats.cu:10-57): the electron, its step count, kinetic energy, position
+ * and direction angles when it left the chamber.  The electron is named by its random-stream key (the
+ * reference numbers electrons in creation order, which a parallel run does not have). */
+typedef struct cm_escape_record {
+  uint64_t electron;
+  int32_t pixel;
+  int32_t step;
+  double energy_eV;
+  double position[3];          /* m */
+  double theta, phi;           /* direction (cos phi sin theta, sin phi sin theta, cos theta) */
+} cm_escape_record;
 
 /* kernels of one wavefront iteration, in launch order */
 #define CM_K_FLIGHT 0

@@ -1822,13 +1822,19 @@ typedef struct {
    histo h;
    cmo_tally* t;
    cmo_rng* r;
+   histo h_el, h_az; /* BackscatterStats.cu:105-106 */
 } run_ctx;
 
-/* BackscatterStats.cu:140-181 */
+/* BackscatterStats.cu:140-181: elevation and azimuth first, then the energy histogram */
 static void tally_escape(run_ctx* c, const electron* e)
 {
    const double* pos = e->pos;
    const double elevation = (PI / 2) - atan2(pos[2], sqrt((pos[0] * pos[0]) + (pos[1] * pos[1])));
+   double azimuth = atan2(pos[1], pos[0]);
+   if (azimuth < 0.0) azimuth = (2.0 * PI) + azimuth;
+   const int be = histo_bin(&c->h_el, elevation) + 1, ba = histo_bin(&c->h_az, azimuth) + 1;
+   if (be <= 181) c->t->elevation[be]++; /* past the overflow slot the reference writes out of bounds */
+   if (ba <= 361) c->t->azimuth[ba]++;
    const double kEeV = e->E * FROMSI_EV;
    int b = histo_bin(&c->h, kEeV) + 1;
    if (b > c->h.nbins + 1) { c->t->dropped_overrange++; return; }
@@ -1907,6 +1913,8 @@ int cmo_run(cmo_scene* s, int chamber, double beam_width, double beam_energy, co
    memset(out, 0, sizeof(*out));
    /* BackscatterStats(monte, nbins): energy histogram over [0, beam energy in eV] */
    histo_init(&c.h, 0.0, beam_energy * FROMSI_EV, nbins);
+   histo_init(&c.h_el, 0.0, PI, 180);
+   histo_init(&c.h_az, 0.0, 2.0 * PI, 360);
    electron* stack = (electron*)malloc(sizeof(electron) * STACKMAX);
    for (int i = 0; i < nprim; ++i) {
       /* GaussianBeam::createElectron (GaussianBeam.cu:52-65) + initializeTrajectory (MonteCarloSS.cu:99-105) */

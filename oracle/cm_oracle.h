@@ -103,6 +103,8 @@ typedef struct {
    int64_t trajectories;
    int64_t scatter_events, barrier_events, secondaries;
    int64_t dropped_overrange; /* escapes whose bin index falls past the overflow slot (reference writes out of bounds) */
+   int64_t elevation[182];    /* BackscatterStats elevation histogram, Histogram(0, pi, 180), index = bin + 1 */
+   int64_t azimuth[362];      /* BackscatterStats azimuthal histogram, Histogram(0, 2 pi, 360), index = bin + 1 */
 } cmo_tally;
 
 int cmo_run(cmo_scene* s, int chamber_region, double beam_width, double beam_energy, const double center[3],

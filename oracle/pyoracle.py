@@ -88,7 +88,7 @@ def ip(a):
 class Tally(C.Structure):
     _fields_ = [("back", C.c_int64 * 1026), ("fwd", C.c_int64 * 1026), ("trajectories", C.c_int64),
                 ("scatter_events", C.c_int64), ("barrier_events", C.c_int64), ("secondaries", C.c_int64),
-                ("dropped_overrange", C.c_int64)]
+                ("dropped_overrange", C.c_int64), ("elevation", C.c_int64 * 182), ("azimuth", C.c_int64 * 362)]
 
 
 class Scene:

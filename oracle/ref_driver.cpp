@@ -667,6 +667,12 @@ static int run_scene(bool lines, int nprim, unsigned long long seed, const std::
       for (int j = -1; j <= hist.binCount(); ++j) printf(" %d", hist.counts(j));
       printf("\nfwd");
       for (int j = -1; j <= fwd.binCount(); ++j) printf(" %d", fwd.counts(j));
+      const HistogramT& elev = back.elevationHistogram();
+      const HistogramT& azim = back.azimuthalHistogram();
+      printf("\nelev");
+      for (int j = -1; j <= elev.binCount(); ++j) printf(" %d", elev.counts(j));
+      printf("\nazim");
+      for (int j = -1; j <= azim.binCount(); ++j) printf(" %d", azim.counts(j));
       printf("\n");
       monte.removeActionListener(back);
    }

@@ -36,7 +36,8 @@ def main():
         r = subprocess.run([os.path.join(ref, "ref_driver"), "run1", "10000", str(seed), tables, "1000"], cwd=ref,
                            capture_output=True, text=True, check=True)
         out.append("# seed %d\n" % seed + "\n".join(l for l in r.stdout.splitlines()
-                                                    if l.startswith(("pixel", "back", "fwd", "steps", "seconds", "#"))))
+                                                    if l.startswith(("pixel", "back", "fwd", "elev", "azim", "steps",
+                                                                       "seconds", "#"))))
     with open(os.path.join(HERE, "run_halfspace_1keV.txt"), "w") as f:
         f.write("\n".join(out) + "\n")
     print("wrote run_halfspace_1keV.txt")

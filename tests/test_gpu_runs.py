@@ -316,6 +316,84 @@ def test_tail_steps_give_the_same_tallies(prec):
         assert np.array_equal(b0, b) and np.array_equal(f0, f)
 
 
+def ref_angles(kind):
+    runs = []
+    for line in open(os.path.join(GOLDEN, "run_halfspace_1keV.txt")):
+        w = line.split()
+        if w and w[0] == kind:
+            runs.append([int(x) for x in w[1:]])
+    return np.array(runs)
+
+
+@pytest.mark.parametrize("prec", [FP64, FP32], ids=["fp64", "fp32"])
+def test_angle_histograms_match_reference(half, prec):
+    """BackscatterStats' elevation and azimuthal histograms (BackscatterStats.cu:105-106,147-165), 1 keV
+    pencil beam on flat Si: engine 40 x 1000 primaries vs the reference's 4 x 10 000 (chi-squared)."""
+    from cudamonsel_b200 import stats
+    e, h = half
+    centers = np.tile([0.0, 0.0, -20e-9], (40, 1))
+    back, fwd, st, ex = e.run(h["chamber"], centers, scenes_eV(1000.0), 1000, 100, 0.0, seed=21, precision=prec,
+                              angles=True)
+    el, az = ex["elevation"], ex["azimuth"]
+    assert el.shape == (40, 182) and az.shape == (40, 362)
+    assert el.sum() == az.sum() == st.escapes
+    assert el.sum() >= back.sum() + fwd.sum() and el[:, :92].sum() == 0
+    for name, mine in (("elev", el), ("azim", az)):
+        ref = ref_angles(name)
+        chi, dof, p = stats.chi2_two_sample(mine.sum(0), 40000, ref.sum(0), 40000)
+        print("%s chi2 %.1f dof %d p %.3g" % (name, chi, dof, p))
+        assert p > 1e-3
+
+
+def scenes_eV(x):
+    from cudamonsel_b200 import scenes
+    return scenes.eV(x)
+
+
+def ref_bin(maxv, nbins, vals):
+    """Histogram(0, max, nbins).bin + 1 with Algorithm::binarySearch's insertion point (the tallies' rule)."""
+    delta = maxv / nbins
+    edges = np.array([0.0] + [0.0 + i * delta for i in range(1, nbins + 1)])
+    return np.searchsorted(edges, vals, side="left") + 1
+
+
+@pytest.mark.parametrize("prec", [FP64, FP32], ids=["fp64", "fp32"])
+def test_escape_log_rebuilds_the_tallies(prec):
+    """BackscatterStats' detected-electron log: one record per escape; binning the logged energies and
+    escape points again gives the run's energy histograms exactly and its angle histograms up to the
+    rounding of the logged position; a smaller log keeps the first records and the count."""
+    from cudamonsel_b200 import capi, scenes
+    e = capi.Engine(0)
+    h = scenes.build_engine(scenes.lines(), e)
+    c = scenes.linescan_pixels(16)
+    back, fwd, st, ex = e.run(h["chamber"], c, scenes.eV(500.0), 200, 50, 1e-9, seed=4, precision=prec, angles=True,
+                              escape_log_cap=200000)
+    log = ex["escape_log"]
+    assert len(log) == st.escapes > 0
+    assert len(np.unique(log["pixel"])) == 16 and (log["step"] > 0).all()
+    pos = log["position"]
+    elev = np.pi / 2 - np.arctan2(pos[:, 2], np.sqrt(pos[:, 0] ** 2 + pos[:, 1] ** 2))
+    e0ref = scenes.eV(500.0) * (1.0 / 1.60217653e-19)  # the histogram top as the engine computes it (FromSI::eV)
+    be = ref_bin(e0ref, 50, log["energy_eV"])
+    for px in range(16):
+        m = log["pixel"] == px
+        for hist, sel in ((back, elev[m] >= np.pi / 2), (fwd, elev[m] < np.pi / 2)):
+            b = be[m][sel]
+            counts = np.bincount(b[b <= 51], minlength=52)
+            assert np.array_equal(counts, hist[px].astype(np.int64)), px
+    el_counts = np.bincount(ref_bin(np.pi, 180, elev), minlength=182)
+    diff = np.abs(el_counts - ex["elevation"].sum(0).astype(np.int64)).sum()
+    print("escapes %d, elevation histogram from the log differs by %d counts" % (st.escapes, diff))
+    assert diff <= 4
+    d = np.stack([np.cos(log["phi"]) * np.sin(log["theta"]), np.sin(log["phi"]) * np.sin(log["theta"]),
+                  np.cos(log["theta"])], axis=1)
+    assert np.allclose((d * d).sum(1), 1.0)
+    _, _, st2, ex2 = e.run(h["chamber"], c, scenes.eV(500.0), 200, 50, 1e-9, seed=4, precision=prec,
+                           escape_log_cap=100)
+    e.close()
+    assert st2.escapes == st.escapes and len(ex2["escape_log"]) == 100
+
+
 def test_deterministic_and_independent_of_batch(half):
     """Same seed -> identical tallies; a pixel's tally is the same alone and inside a larger
     batch of other pixels when it carries the same stream key (the serving guarantee)."""
