@@ -173,6 +173,7 @@ def main():
     ap.add_argument("--no-serving", action="store_true", help="skip the served-stream latency measurement")
     ap.add_argument("--no-image", action="store_true", help="skip the rough-line image (FP32 vs FP64)")
     ap.add_argument("--no-deep", action="store_true", help="skip the 10 keV deep-penetration layout")
+    ap.add_argument("--no-autotune", action="store_true", help="run with the default launch settings")
     ap.add_argument("--profile-run", action="store_true",
                     help="run one FP32 step of the workload and exit (the case for ncu captures)")
     a = ap.parse_args()
@@ -223,6 +224,13 @@ def main():
         print("profile run: %d primaries, %d electron-steps, %d iterations" % (st.primaries, st.steps, st.iterations))
         eng.close()
         return 0
+    # launch settings picked by the engine's autotuner on this workload (outside the timed region)
+    tuned = {}
+    if not a.no_autotune:
+        for name, pr in (("fp32", capi.PREC_FP32), ("fp64", capi.PREC_FP64)):
+            tt = eng.autotune(h["chamber"], centers, scenes.eV(BEAM_EV), NPRIM, NBINS, 1e-9, 0, precision=pr,
+                              pixel_keys=keys)
+            tuned[name] = {k: v for k, v in tt.as_dict().items() if k != "ms"}
     for _ in range(a.warmup):
         step(prec)
     torch.cuda.synchronize()
@@ -410,7 +418,8 @@ def main():
                 "vs_baseline": None, "dtype": "f32", "data": "synthetic",
                 "config": {"workload": WORKLOAD, "pixels": NPIX, "primaries_per_pixel": NPRIM, "beam_eV": BEAM_EV,
                            "precision": "f32 transport, f64 positions and plane solves",
-                           "l2": "flushed between steps (256 MB write)", "parallelism": "replicas x%d" % world},
+                           "l2": "flushed between steps (256 MB write)", "parallelism": "replicas x%d" % world,
+                           "tuning": tuned or "defaults"},
                 "electron_steps_per_s": world * steps_total / (ms / 1000.0),
                 "fp64": {"value": prim_per_rank / (ms64 / 1000.0), "unit": "primaries/s", "steps": int(st64.steps)},
                 "yield_error_vs_fp64": yerr,

@@ -28,7 +28,7 @@ EXPORTS = (
     "cm_shape_union", "cm_shape_cylinder", "cm_shape_translate", "cm_shape_line", "cm_region_add", "cm_run", "cm_run_device", "cm_run_noalloc",
     "cm_eval_nistmott", "cm_eval_table", "cm_eval_tabulated", "cm_eval_elastic", "cm_eval_csd", "cm_eval_phonon",
     "cm_eval_shape", "cm_eval_barrier", "cm_eval_freepath", "cm_server_create", "cm_server_destroy", "cm_job_submit",
-    "cm_job_poll", "cm_job_wait", "cm_job_cancel", "cm_job_result",
+    "cm_job_poll", "cm_job_wait", "cm_job_cancel", "cm_job_result", "cm_get_tuning", "cm_set_tuning", "cm_autotune",
 )
 
 JOB_QUEUED, JOB_RUNNING, JOB_DONE, JOB_FAILED, JOB_CANCELLED = 0, 1, 2, 3, 4
@@ -48,6 +48,14 @@ ELEVATION_COUNTS, AZIMUTH_COUNTS = 182, 362
 # cm_escape_record
 ESCAPE_RECORD = np.dtype([("electron", np.uint64), ("pixel", np.int32), ("step", np.int32), ("energy_eV", np.float64),
                           ("position", np.float64, 3), ("theta", np.float64), ("phi", np.float64)])
+
+
+class Tuning(C.Structure):
+    _fields_ = [("wave", C.c_int), ("tail_below", C.c_int), ("tail_steps", C.c_int), ("blocks_per_sm", C.c_int),
+                ("ms", C.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
 
 
 class JobInfo(C.Structure):
@@ -97,6 +105,9 @@ def load(path=LIBPATH):
         "cm_context_destroy": [ctx],
         "cm_context_reset": [ctx],
         "cm_set_options": [ctx, C.c_int],
+        "cm_get_tuning": [ctx, C.c_int, C.POINTER(Tuning)],
+        "cm_set_tuning": [ctx, C.c_int, C.POINTER(Tuning)],
+        "cm_autotune": [ctx, C.POINTER(RunDesc), C.POINTER(Tuning)],
         "cm_add_mott_element": [ctx, C.c_int, d, d],
         "cm_add_table": [ctx, C.c_int, i, d, d, i],
         "cm_add_material": [ctx, C.c_int, i, d, d, C.c_double, C.c_double, C.c_double, C.c_double, C.c_int, d, i],
@@ -194,6 +205,23 @@ class Engine:
     # ---- scene (same method names as oracle/pyoracle.Scene via scene.SceneSpec)
     def set_options(self, opt):
         self._check(self.L.cm_set_options(self.h, opt))
+
+    def tuning(self, precision=PREC_FP64):
+        t = Tuning()
+        self._check(self.L.cm_get_tuning(self.h, precision, C.byref(t)))
+        return t
+
+    def set_tuning(self, precision=PREC_FP64, wave=0, tail_below=0, tail_steps=0, blocks_per_sm=0):
+        t = Tuning(wave, tail_below, tail_steps, blocks_per_sm, 0.0)
+        self._check(self.L.cm_set_tuning(self.h, precision, C.byref(t)))
+
+    def autotune(self, chamber, centers, energies, nprim, nbins, beam_width, seed, precision=PREC_FP64,
+                 pixel_keys=None):
+        """cm_autotune on this workload (host arrays); returns the Tuning kept for later runs."""
+        desc, keep, _, _ = _run_desc(chamber, centers, energies, nprim, nbins, beam_width, seed, precision, pixel_keys)
+        t = Tuning()
+        self._check(self.L.cm_autotune(self.h, C.byref(desc), C.byref(t)))
+        return t
 
     def mott(self, Z, spwem, x1):
         a, pa = _d(spwem)

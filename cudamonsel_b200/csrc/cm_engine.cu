@@ -166,6 +166,7 @@ struct cm_context {
   Counters* counters_host = nullptr;
   cudaStream_t stream = nullptr;
   const std::atomic<int>* cancel = nullptr;  // set by a job server: checked between graph launches
+  cm_tuning tune[2] = {{0, 0, 0, 0, 0.0}, {0, 0, 0, 0, 0.0}};  // launch settings per precision (0: default)
   void dirty() {
     d64.release();
     d32.release();
@@ -839,10 +840,20 @@ template <typename R, int D> __global__ void CM_LB_STEPS k_steps(RunView<R> v, i
   flush_counts(v.c, sc);
 }
 
-template <typename R> static void launch_steps(const RunView<R>& v, int cur, int grid, cudaStream_t s) {
-  if (v.s.depth == 0) k_steps<R, 0><<<grid, 256, 0, s>>>(v, cur, CM_TAIL_STEPS);
-  else if (v.s.depth <= 2) k_steps<R, 2><<<grid, 256, 0, s>>>(v, cur, CM_TAIL_STEPS);
-  else k_steps<R, kMaxShapeDepth><<<grid, 256, 0, s>>>(v, cur, CM_TAIL_STEPS);
+template <typename R> static void launch_steps(const RunView<R>& v, int cur, int grid, int nsteps, cudaStream_t s) {
+  if (v.s.depth == 0) k_steps<R, 0><<<grid, 256, 0, s>>>(v, cur, nsteps);
+  else if (v.s.depth <= 2) k_steps<R, 2><<<grid, 256, 0, s>>>(v, cur, nsteps);
+  else k_steps<R, kMaxShapeDepth><<<grid, 256, 0, s>>>(v, cur, nsteps);
+}
+
+// the launch settings a run uses: the context's tuning, built-in defaults where it holds 0
+template <typename R> static cm_tuning resolved_tuning(const cm_context* ctx) {
+  cm_tuning t = ctx->tune[sizeof(R) == 8 ? CM_PREC_FP64 : CM_PREC_FP32];
+  if (t.wave <= 0) t.wave = sizeof(R) == 8 ? (1 << 20) : (1 << 21);
+  if (t.tail_below <= 0) t.tail_below = CM_TAIL_BELOW;
+  if (t.tail_steps <= 0) t.tail_steps = CM_TAIL_STEPS;
+  if (t.blocks_per_sm <= 0) t.blocks_per_sm = 8;
+  return t;
 }
 
 template <typename R> static void launch_misc(const RunView<R>& v, int cur, int grid, cudaStream_t s) {
@@ -927,7 +938,8 @@ static int run_device_once(cm_context* ctx, const cm_run_desc* d, uint32_t* back
                       const unsigned long long* pkey_dev, unsigned long long total) {
   int rc;
   if ((rc = build_scene<R>(ctx, scene_of<R>(ctx)))) return rc;
-  const int W = d->wave > 0 ? d->wave : (sizeof(R) == 8 ? (1 << 20) : (1 << 21));
+  const cm_tuning tu = resolved_tuning<R>(ctx);
+  const int W = d->wave > 0 ? d->wave : tu.wave;
   RunBuffers<R>& rb0 = buffers_of<R>(ctx);
   const int poolWant = rb0.cap == W && rb0.poolCap > 8 * W ? rb0.poolCap : 8 * W;
   if ((rc = ensure_buffers<R>(ctx, W, poolWant))) return rc;
@@ -967,7 +979,7 @@ static int run_device_once(cm_context* ctx, const cm_run_desc* d, uint32_t* back
   memset(&c0, 0, sizeof(c0));
   c0.total_primaries = total;
   CM_CUDA(cudaMemcpyAsync(ctx->counters, &c0, sizeof(c0), cudaMemcpyHostToDevice, stream));
-  const int grid = ctx->nsm * 8;
+  const int grid = ctx->nsm * tu.blocks_per_sm;
   const int maxIt = d->max_iterations > 0 ? d->max_iterations : 500000;
   cudaEvent_t e0, e1;
   CM_CUDA(cudaEventCreate(&e0));
@@ -1050,7 +1062,7 @@ static int run_device_once(cm_context* ctx, const cm_run_desc* d, uint32_t* back
       // (unless CM_OPT_QUEUE_STEPS keeps the queue kernels to the end)
       const Counters& hc = *ctx->counters_host;
       const long long left = (long long)hc.n[0] + hc.n[1] + std::min(hc.pool, v.poolCap);
-      tail = !(ctx->options & CM_OPT_QUEUE_STEPS) && hc.next_primary == hc.total_primaries && left < CM_TAIL_BELOW;
+      tail = !(ctx->options & CM_OPT_QUEUE_STEPS) && hc.next_primary == hc.total_primaries && left < tu.tail_below;
       if (tail && !texec) {
         if (d->profile) {
           tev.resize((size_t)2 * K * 3 + 1);
@@ -1061,7 +1073,7 @@ static int run_device_once(cm_context* ctx, const cm_run_desc* d, uint32_t* back
         for (int it = 0; it < 2 * K; ++it) {
           const int cur = it & 1;
           cudaEvent_t* ev = d->profile ? &tev[(size_t)it * 3 + 1] : nullptr;
-          launch_steps(v, cur, grid, stream);
+          launch_steps(v, cur, grid, tu.tail_steps, stream);
           if (ev) cudaEventRecordWithFlags(ev[0], stream, cudaEventRecordExternal);
           launch_spawn<R>(v, cur, grid, stream);
           if (ev) cudaEventRecordWithFlags(ev[1], stream, cudaEventRecordExternal);
@@ -1365,6 +1377,24 @@ int cm_context_destroy(cm_context* ctx) {
   cudaFreeHost(ctx->counters_host);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
+  return 0;
+}
+
+int cm_get_tuning(cm_context* ctx, int precision, cm_tuning* out) {
+  if (!ctx || !out) return fail(CM_EINVAL, "null argument");
+  if (precision != CM_PREC_FP64 && precision != CM_PREC_FP32) return fail(CM_EINVAL, "bad precision");
+  *out = ctx->tune[precision];
+  return 0;
+}
+
+int cm_set_tuning(cm_context* ctx, int precision, const cm_tuning* t) {
+  if (!ctx || !t) return fail(CM_EINVAL, "null argument");
+  if (precision != CM_PREC_FP64 && precision != CM_PREC_FP32) return fail(CM_EINVAL, "bad precision");
+  if (t->wave < 0 || (t->wave > 0 && (t->wave < 1024 || t->wave > (1 << 24)))) return fail(CM_EINVAL, "wave out of range");
+  if (t->tail_below < 0) return fail(CM_EINVAL, "tail_below < 0");
+  if (t->tail_steps < 0 || t->tail_steps > 4096) return fail(CM_EINVAL, "tail_steps out of range");
+  if (t->blocks_per_sm < 0 || t->blocks_per_sm > 32) return fail(CM_EINVAL, "blocks_per_sm out of range");
+  ctx->tune[precision] = *t;
   return 0;
 }
 
@@ -1928,6 +1958,64 @@ int cm_run_device(cm_context* ctx, const cm_run_desc* d, uint32_t* back, uint32_
   cudaEventDestroy(ein);
   cudaEventDestroy(eout);
   return rc;
+}
+
+// Coordinate descent over the launch settings from the defaults, one cm_run per candidate.
+int cm_autotune(cm_context* ctx, const cm_run_desc* d, cm_tuning* best) {
+  int rc = check_desc(ctx, d);
+  if (rc) return rc;
+  if (!d->pixel_center || !d->pixel_energy || !d->pixel_nprim || !d->pixel_nbins) return fail(CM_EINVAL, "null array");
+  cm_run_desc dd = *d;
+  dd.wave = 0;
+  dd.profile = 0;
+  dd.elevation = dd.azimuth = nullptr;
+  dd.escape_log = nullptr;
+  dd.escape_log_cap = 0;
+  std::vector<uint32_t> back((size_t)d->npix * d->hist_stride), fwd(back.size());
+  cm_tuning& slot = ctx->tune[d->precision];
+  const cm_tuning saved = slot;
+  auto trial = [&](const cm_tuning& t, double& ms) -> int {
+    slot = t;
+    cm_run_stats st;
+    memset(&st, 0, sizeof(st));
+    const int r = cm_run(ctx, &dd, back.data(), fwd.data(), &st);
+    ms = st.device_ms;
+    return r;
+  };
+  cm_tuning cur = d->precision == CM_PREC_FP64 ? cm::resolved_tuning<double>(ctx) : cm::resolved_tuning<float>(ctx);
+  double cur_ms = 0, ms = 0;
+  if ((rc = trial(cur, cur_ms)) || (rc = trial(cur, cur_ms))) {  // the first run also builds the scene
+    slot = saved;
+    return rc;
+  }
+  const int w = cur.wave;
+  const int waves[] = {w / 2, w * 2};
+  const int belows[] = {65536, 131072, 524288};
+  const int steps[] = {16, 64};
+  const int blocks[] = {4, 16};
+  auto sweep = [&](int cm_tuning::*field, const int* vals, int n) -> int {
+    for (int k = 0; k < n; ++k) {
+      if (vals[k] == cur.*field) continue;
+      cm_tuning t = cur;
+      t.*field = vals[k];
+      const int r = trial(t, ms);
+      if (r) return r;
+      if (ms < 0.99 * cur_ms) {
+        cur = t;
+        cur_ms = ms;
+      }
+    }
+    return 0;
+  };
+  if ((rc = sweep(&cm_tuning::wave, waves, 2)) || (rc = sweep(&cm_tuning::tail_below, belows, 3)) ||
+      (rc = sweep(&cm_tuning::tail_steps, steps, 2)) || (rc = sweep(&cm_tuning::blocks_per_sm, blocks, 2))) {
+    slot = saved;
+    return rc;
+  }
+  cur.ms = cur_ms;
+  slot = cur;
+  if (best) *best = cur;
+  return 0;
 }
 
 // ---- per-function entry points

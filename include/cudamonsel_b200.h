@@ -59,6 +59,19 @@ int cm_context_destroy(cm_context* ctx);
 int cm_context_reset(cm_context* ctx);
 const char* cm_last_error(void);
 int cm_set_options(cm_context* ctx, int options);
+
+/* Launch settings of the transport loop (no reference counterpart: the reference runs one trajectory at a
+ * time), one set per precision.  0 = the built-in default.  Every setting gives the same tallies, because
+ * each electron's random stream is keyed by its lineage, so they change only the speed. */
+typedef struct {
+  int wave;                    /* electrons per wave segment (default 2^21 in FP32, 2^20 in FP64) */
+  int tail_below;              /* k_steps runs the tail once fewer electrons are left (default 262144) */
+  int tail_steps;              /* whole steps per thread and launch in the tail (default 32) */
+  int blocks_per_sm;           /* grid = SMs x blocks_per_sm blocks of 256 threads (default 8) */
+  double ms;                   /* cm_autotune: device time of the transport loop under these settings */
+} cm_tuning;
+int cm_get_tuning(cm_context* ctx, int precision, cm_tuning* out);
+int cm_set_tuning(cm_context* ctx, int precision, const cm_tuning* tuning);
 int cm_version(void);
 
 /* ---- data ------------------------------------------------------------------- */
@@ -198,6 +211,14 @@ int cm_run(cm_context* ctx, const cm_run_desc* desc, uint32_t* back, uint32_t* f
 /* Same with inputs (pixel arrays) and outputs (back, fwd) already in device memory. */
 int cm_run_device(cm_context* ctx, const cm_run_desc* desc_device_arrays, uint32_t* back_device, uint32_t* fwd_device,
                   cm_run_stats* stats, void* stream);
+
+/* Autotuner: times the transport loop of desc (host arrays as for cm_run; its tallies are discarded)
+ * under candidate settings, one setting at a time from the defaults (coordinate descent; a change is
+ * kept when it is at least 1 % faster), and keeps the fastest for this context's later runs.  desc
+ * should hold at least a wave's worth of primaries so that the trial sees the full and the tail phases
+ * of a run.  The settings are kept for desc->precision; *best (may be NULL) receives them. */
+int cm_autotune(cm_context* ctx, const cm_run_desc* desc, cm_tuning* best);
+
 /* No counterpart in the reference.  cm_run_device for callers that cannot
  * allocate device memory while they run: a service whose device memory belongs
  * to another allocator (a caching pool, a reservation fixed at start-up), where

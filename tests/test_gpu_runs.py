@@ -394,6 +394,34 @@ def test_escape_log_rebuilds_the_tallies(prec):
     assert st2.escapes == st.escapes and len(ex2["escape_log"]) == 100
 
 
+@pytest.mark.parametrize("prec", [FP64, FP32], ids=["fp64", "fp32"])
+def test_autotune_and_settings_keep_the_tallies(prec):
+    """cm_autotune keeps the fastest launch settings for the precision it tuned; runs under the tuned,
+    the default and deliberately odd settings (small waves, short tail steps, few blocks) give the
+    same tallies.  Out-of-range settings are refused."""
+    from cudamonsel_b200 import capi, scenes
+    e = capi.Engine(0)
+    h = scenes.build_engine(scenes.lines(), e)
+    c = scenes.linescan_pixels(32)
+    args = (h["chamber"], c, scenes.eV(500.0), 300, 50, 1e-9, 9)
+    with pytest.raises(capi.CMError):
+        e.set_tuning(prec, blocks_per_sm=64)
+    b0, f0, s0 = e.run(*args, precision=prec)
+    t = e.autotune(*args, precision=prec)
+    print("tuned", t.as_dict())
+    got = e.tuning(prec)
+    assert t.ms > 0 and (got.wave, got.tail_below, got.tail_steps, got.blocks_per_sm) == (
+        t.wave, t.tail_below, t.tail_steps, t.blocks_per_sm)
+    other = e.tuning(FP32 if prec == FP64 else FP64)
+    assert (other.wave, other.tail_below, other.tail_steps, other.blocks_per_sm) == (0, 0, 0, 0)
+    b1, f1, s1 = e.run(*args, precision=prec)
+    e.set_tuning(prec, wave=65536, tail_below=3000, tail_steps=3, blocks_per_sm=2)
+    b2, f2, s2 = e.run(*args, precision=prec)
+    e.close()
+    for b, f, s in ((b1, f1, s1), (b2, f2, s2)):
+        assert s.steps == s0.steps and np.array_equal(b, b0) and np.array_equal(f, f0)
+
+
 def test_deterministic_and_independent_of_batch(half):
     """Same seed -> identical tallies; a pixel's tally is the same alone and inside a larger
     batch of other pixels when it carries the same stream key (the serving guarantee)."""
