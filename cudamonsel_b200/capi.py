@@ -18,6 +18,7 @@ OPT_JMONSEL_FIXES = 1
 OPT_EXACT_CSG = 2
 OPT_SCAN_CHILDREN = 4
 OPT_QUEUE_STEPS = 8
+OPT_GLOBAL_TABLES = 16
 
 # every symbol include/cudamonsel_b200.h declares
 EXPORTS = (

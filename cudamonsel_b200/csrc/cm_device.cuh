@@ -364,22 +364,33 @@ template <typename R> CM_D R nu_d3(const R* f, const R* xs0, int n0, const R* xs
   return dot4(w0, y);
 }
 
+// the staged prefix of the table blob (kernels launched with it hold s.nstaged elements here)
+extern __shared__ __align__(16) unsigned char cm_stage_smem[];
+
+// an array of the table blob: from shared memory when the kernel staged it, else from global memory
+template <typename R> CM_D const R* blob_at(const SceneView<R>& s, int off) {
+#ifdef __CUDA_ARCH__
+  if (off < s.nstaged) return reinterpret_cast<const R*>(cm_stage_smem) + off;
+#endif
+  return s.blob + off;
+}
+
 // NUTableInterpolation::interpolate (JMONSEL/NUTableInterpolation.cu:98-115)
 template <typename R> CM_D R table_interp(const SceneView<R>& s, int t, R x0, R x1, R x2, int order) {
   const Table& tb = s.tables[t];
-  const R* v = s.blob + tb.off_v;
+  const R* v = blob_at(s, tb.off_v);
   if (tb.dim == 1) {
-    if (order == 1) return nu_d1_order1(v, s.blob + tb.off_x[0], tb.n[0], x0);
+    if (order == 1) return nu_d1_order1(v, blob_at(s, tb.off_x[0]), tb.n[0], x0);
     int first, nearest;
-    const R* xs = s.blob + tb.off_x[0];
+    const R* xs = blob_at(s, tb.off_x[0]);
     nu_locate(x0, xs, tb.n[0], 3, first, nearest);
     R fv[4] = {v[first], v[first + 1], v[first + 2], v[first + 3]};
     R xv[4] = {xs[first], xs[first + 1], xs[first + 2], xs[first + 3]};
     return nu_neville3(fv, xv, nearest - first, x0);
   }
-  if (tb.dim == 2) return nu_d2(v, s.blob + tb.off_x[0], tb.n[0], s.blob + tb.off_x[1], tb.n[1], x0, x1);
-  return nu_d3(v, s.blob + tb.off_x[0], tb.n[0], s.blob + tb.off_x[1], tb.n[1], s.blob + tb.off_x[2], tb.n[2], x0, x1, x2,
-               (s.options & 1) != 0);
+  if (tb.dim == 2) return nu_d2(v, blob_at(s, tb.off_x[0]), tb.n[0], blob_at(s, tb.off_x[1]), tb.n[1], x0, x1);
+  return nu_d3(v, blob_at(s, tb.off_x[0]), tb.n[0], blob_at(s, tb.off_x[1]), tb.n[1], blob_at(s, tb.off_x[2]), tb.n[2], x0,
+               x1, x2, (s.options & 1) != 0);
 }
 
 // ------------------------------------------------------------ elastic scattering
@@ -417,7 +428,7 @@ template <typename R> CM_D R nistmott_rate(const SceneView<R>& s, const Mott& m,
     return (R)m.sfBrowning[method] * browning_sigma(m, E) * kbrown;
   }
   if (E < (R)s.maxMott) {
-    return kel * ulagrange_d1(s.blob + m.off_spwem, 61, s.dl50, s.param, (double)logE);
+    return kel * ulagrange_d1(blob_at(s, m.off_spwem), 61, s.dl50, s.param, (double)logE);
   }
   // ScreenedRutherfordScatteringAngle.cu:24-30
   return (R)m.rutherfordA / (E + (R)m.rutherfordB) * kbrown;

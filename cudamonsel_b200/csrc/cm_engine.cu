@@ -43,6 +43,8 @@ namespace cm {
 // ------------------------------------------------------------------ units
 static const double kEV = 1.60217653e-19;          // PhysicalConstants::ElectronCharge
 static const double kFromSIeV = 1.0 / 1.60217653e-19;  // FromSI::EV
+// the small tables (prefix of the table blob) the event kernels stage into shared memory
+static const size_t kStageBytes = 48 * 1024;
 static const double kToSIkeV = 1.60217653e-19 * 1.0e3;
 static const double kBohr = 5.291772083e-11;
 static const double kAvogadro = 6.0221415e23;
@@ -386,42 +388,84 @@ static int build_scene(cm_context* ctx, DevScene<R>& ds) {
   ds.release();
   std::vector<R> blob;
   std::vector<double> mott64;
+  // The blob holds every table's abscissae and values and the NIST Mott cross sections.  Pieces are
+  // built apart and laid out small first: the prefix that fits kStageBytes is what the event kernels
+  // copy into shared memory (the rest, such as a large 3-D angle table, is read through L1/L2).
+  struct Piece {
+    std::vector<R> data;
+    std::vector<int*> offs;   // offsets to patch
+    std::vector<int> rel;     // relative offsets of those fields in data
+  };
+  std::vector<Piece> pieces;
   // tables, converted by role to eV / nm units
-  std::vector<Table> tabs;
-  for (auto& t : ctx->tables) {
-    Table d;
+  std::vector<Table> tabs(ctx->tables.size());
+  for (size_t ti = 0; ti < ctx->tables.size(); ++ti) {
+    const auto& t = ctx->tables[ti];
+    Table& d = tabs[ti];
     memset(&d, 0, sizeof(d));
     d.dim = t.dim;
+    Piece pc;
     const double ax0 = (t.role >= 1) ? kFromSIeV : 1.0;
     const double vf = t.role == 1 ? 1e-9 : t.role == 4 ? kFromSIeV : 1.0;
     for (int k = 0; k < t.dim; ++k) {
       d.n[k] = t.n[k];
-      d.off_x[k] = (int)blob.size();
+      pc.offs.push_back(&d.off_x[k]);
+      pc.rel.push_back((int)pc.data.size());
       const double f = k == 0 ? ax0 : 1.0;
-      for (double v : t.x[k]) blob.push_back((R)(v * f));
+      for (double v : t.x[k]) pc.data.push_back((R)(v * f));
       d.domain[k][0] = t.domain[k][0] * f;
       d.domain[k][1] = t.domain[k][1] * f;
     }
-    d.off_v = (int)blob.size();
-    for (double v : t.v) blob.push_back((R)(v * vf));
+    pc.offs.push_back(&d.off_v);
+    pc.rel.push_back((int)pc.data.size());
+    for (double v : t.v) pc.data.push_back((R)(v * vf));
     d.range[0] = t.range[0] * vf;
     d.range[1] = t.range[1] * vf;
-    tabs.push_back(d);
+    pieces.push_back(std::move(pc));
   }
   // NIST Mott elements
-  std::vector<Mott> motts;
+  std::vector<Mott> motts(ctx->mott.size());
   std::map<int, int> mottIndex;
-  for (auto& kv : ctx->mott) {
-    Mott m;
-    memset(&m, 0, sizeof(m));
-    mott_constants(kv.first, kv.second, m);
-    m.off_spwem = (int)blob.size();
-    for (double v : kv.second.spwem) blob.push_back((R)v);
-    m.off_x1 = -1;
-    m.off_x1d = (int)mott64.size();  // the quantile table in double as well (the angle's cubic needs it)
-    for (double v : kv.second.x1) mott64.push_back(v);
-    mottIndex[kv.first] = (int)motts.size();
-    motts.push_back(m);
+  {
+    size_t mi = 0;
+    for (auto& kv : ctx->mott) {
+      Mott& m = motts[mi];
+      memset(&m, 0, sizeof(m));
+      mott_constants(kv.first, kv.second, m);
+      Piece pc;
+      pc.offs.push_back(&m.off_spwem);
+      pc.rel.push_back(0);
+      for (double v : kv.second.spwem) pc.data.push_back((R)v);
+      pieces.push_back(std::move(pc));
+      m.off_x1 = -1;
+      m.off_x1d = (int)mott64.size();  // the quantile table in double as well (the angle's cubic needs it)
+      for (double v : kv.second.x1) mott64.push_back(v);
+      mottIndex[kv.first] = (int)mi++;
+    }
+  }
+  int nstage = 0;
+  {
+    std::vector<size_t> order(pieces.size());
+    for (size_t k = 0; k < order.size(); ++k) order[k] = k;
+    std::stable_sort(order.begin(), order.end(),
+                     [&](size_t a, size_t b) { return pieces[a].data.size() < pieces[b].data.size(); });
+    const size_t align = 16 / sizeof(R);
+    bool staging = true;
+    for (size_t k : order) {
+      Piece& pc = pieces[k];
+      if (staging && (blob.size() + pc.data.size()) * sizeof(R) > kStageBytes) {
+        staging = false;
+        while (blob.size() % align) blob.push_back(R(0));
+        nstage = (int)blob.size();
+      }
+      const int base = (int)blob.size();
+      for (size_t f = 0; f < pc.offs.size(); ++f) *pc.offs[f] = base + pc.rel[f];
+      blob.insert(blob.end(), pc.data.begin(), pc.data.end());
+    }
+    if (staging) {
+      while (blob.size() % align) blob.push_back(R(0));
+      nstage = (int)blob.size();
+    }
   }
   // scatter models
   std::vector<Msm> msms;
@@ -672,6 +716,8 @@ static int build_scene(cm_context* ctx, DevScene<R>& ds) {
   v.dl50 = log(0.050 * kToSIkeV * kFromSIeV);
   v.param = (log(20.0 * kToSIkeV) - log(0.050 * kToSIkeV)) / 60.0;
   v.maxMott = 20.0 * kToSIkeV * kFromSIeV;
+  v.nstaged = 0;
+  v.nstage = nstage;
   ds.valid = true;
   return 0;
 }
@@ -708,6 +754,44 @@ struct DeviceSink {
   __device__ __forceinline__ void error(int* e, int code) { atomicExch(e, code); }
 };
 
+// The staged prefix of the table blob (v.s.nstaged elements, a multiple of 16 bytes, 16-byte aligned at
+// both ends) into this block's shared memory: one bulk copy by the tensor memory accelerator completing on
+// an mbarrier.  The wait is bounded; a copy that has not landed by then sets CM_ETIMEOUT and the block
+// does no work (the host ends the run with that error).  Every thread of the block must call it.
+template <typename R> __device__ __forceinline__ bool stage_tables(const RunView<R>& v) {
+  const int n = v.s.nstaged;
+  if (n <= 0) return true;
+  __shared__ __align__(8) unsigned long long bar;
+  const unsigned bar_a = (unsigned)__cvta_generic_to_shared(&bar);
+  const unsigned dst = (unsigned)__cvta_generic_to_shared(cm_stage_smem);
+  const unsigned bytes = (unsigned)n * (unsigned)sizeof(R);
+  if (threadIdx.x == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar_a) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar_a), "r"(bytes) : "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+                 "l"(v.s.blob), "r"(bytes), "r"(bar_a)
+                 : "memory");
+  }
+  unsigned done = 0;
+  for (int it = 0; it < (1 << 20) && !done; ++it) {
+    asm volatile(
+        "{\n"
+        ".reg .pred p;\n"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n"
+        "selp.u32 %0, 1, 0, p;\n"
+        "}\n"
+        : "=r"(done)
+        : "r"(bar_a)
+        : "memory");
+  }
+  if (!done) atomicExch(&v.c->error, CM_ETIMEOUT);
+  return __syncthreads_and(done) != 0;
+}
+
 __device__ __forceinline__ void flush_counts(Counters* c, StepCounts& sc) {
   for (int off = 16; off > 0; off >>= 1) {
     sc.steps += __shfl_down_sync(0xffffffffu, sc.steps, off);
@@ -729,6 +813,7 @@ template <typename R, int D> __device__ __forceinline__ void flight_loop(const R
   DeviceSink sink;
   StepCounts sc;
   const int n = v.c->n[cur];
+  if ((int)(blockIdx.x * blockDim.x) >= n || !stage_tables(v)) return;  // blocks without work stage nothing
   int cnt[kClasses];
   for (int k = 0; k < kClasses; ++k) cnt[k] = v.c->nc[cur][k];
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -743,6 +828,18 @@ template <typename R, int D> __device__ __forceinline__ void flight_loop(const R
 template <typename R, int D> __global__ void __launch_bounds__(256) k_flight(RunView<R> v, int cur) {
   flight_loop<R, D>(v, cur);
 }
+
+// Kernels that stage the small tables into shared memory (1 flight, 2 elastic, 4 inelastic, 8 steps) and
+// the inelastic grid in blocks per SM when it stages.  k_inelastic gathers ~130 table values per event
+// (cubic interpolation in the 2-D energy-loss and SE tables and the 3-D angle table); staged into the
+// shared memory of a grid of 2 resident blocks per SM it gains 1 % on the linescan.  Staging in the
+// other kernels, whose few small-table reads hit L1, loses 4 % (a copy per block, less L1).
+#ifndef CM_STAGE_KERNELS
+#define CM_STAGE_KERNELS 4
+#endif
+#ifndef CM_INEL_BLOCKS_PER_SM
+#define CM_INEL_BLOCKS_PER_SM 2
+#endif
 
 // Resident CTAs per SM the kernels are compiled for (register caps 65536 / (256 x n)); a build may set
 // them with -DCM_MINB_FLIGHT32=n and so on.  CM_MINB_INELASTIC unset: the compiler chooses.
@@ -776,6 +873,7 @@ template <typename R>
 __global__ void CM_LB_ELASTIC k_elastic(RunView<R> v, int cur) {
   DeviceSink sink;
   const int n = v.c->q[Q_EL];
+  if ((int)(blockIdx.x * blockDim.x) >= n || !stage_tables(v)) return;
   for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) elastic_one(v, cur, j, sink);
 }
 
@@ -784,6 +882,7 @@ __global__ void CM_LB_INELASTIC k_inelastic(RunView<R> v, int cur) {
   DeviceSink sink;
   StepCounts sc;
   const int n = v.c->q[Q_TAB];
+  if ((int)(blockIdx.x * blockDim.x) >= n || !stage_tables(v)) return;
   for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) inelastic_one(v, cur, j, sink, sc);
   flush_counts(v.c, sc);
 }
@@ -799,16 +898,17 @@ __global__ void __launch_bounds__(256) k_misc(RunView<R> v, int cur) {
 }
 
 // the kernels are compiled for the intersection nestings 0 (leaf shapes only), 2 and 4
-static void launch_flight(const RunView<double>& v, int cur, int grid, cudaStream_t s) {
-  if (v.s.depth == 0) k_flight<double, 0><<<grid, 256, 0, s>>>(v, cur);
-  else if (v.s.depth <= 2) k_flight<double, 2><<<grid, 256, 0, s>>>(v, cur);
-  else k_flight<double, kMaxShapeDepth><<<grid, 256, 0, s>>>(v, cur);
+// smem: bytes of staged tables (v.s.nstaged elements), 0 when the view stages none
+static void launch_flight(const RunView<double>& v, int cur, int grid, cudaStream_t s, size_t smem = 0) {
+  if (v.s.depth == 0) k_flight<double, 0><<<grid, 256, smem, s>>>(v, cur);
+  else if (v.s.depth <= 2) k_flight<double, 2><<<grid, 256, smem, s>>>(v, cur);
+  else k_flight<double, kMaxShapeDepth><<<grid, 256, smem, s>>>(v, cur);
 }
 
-static void launch_flight(const RunView<float>& v, int cur, int grid, cudaStream_t s) {
-  if (v.s.depth == 0) k_flight32_leaf<<<grid, 256, 0, s>>>(v, cur);
-  else if (v.s.depth <= 2) k_flight<float, 2><<<grid, 256, 0, s>>>(v, cur);
-  else k_flight<float, kMaxShapeDepth><<<grid, 256, 0, s>>>(v, cur);
+static void launch_flight(const RunView<float>& v, int cur, int grid, cudaStream_t s, size_t smem = 0) {
+  if (v.s.depth == 0) k_flight32_leaf<<<grid, 256, smem, s>>>(v, cur);
+  else if (v.s.depth <= 2) k_flight<float, 2><<<grid, 256, smem, s>>>(v, cur);
+  else k_flight<float, kMaxShapeDepth><<<grid, 256, smem, s>>>(v, cur);
 }
 
 // The tail of a run: once fewer electrons are left than fill the GPU, each thread takes one electron
@@ -830,6 +930,7 @@ template <typename R, int D> __global__ void CM_LB_STEPS k_steps(RunView<R> v, i
   DeviceSink sink;
   StepCounts sc;
   const int n = v.c->n[cur];
+  if ((int)(blockIdx.x * blockDim.x) >= n || !stage_tables(v)) return;
   int cnt[kClasses];
   for (int k = 0; k < kClasses; ++k) cnt[k] = v.c->nc[cur][k];
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -840,10 +941,11 @@ template <typename R, int D> __global__ void CM_LB_STEPS k_steps(RunView<R> v, i
   flush_counts(v.c, sc);
 }
 
-template <typename R> static void launch_steps(const RunView<R>& v, int cur, int grid, int nsteps, cudaStream_t s) {
-  if (v.s.depth == 0) k_steps<R, 0><<<grid, 256, 0, s>>>(v, cur, nsteps);
-  else if (v.s.depth <= 2) k_steps<R, 2><<<grid, 256, 0, s>>>(v, cur, nsteps);
-  else k_steps<R, kMaxShapeDepth><<<grid, 256, 0, s>>>(v, cur, nsteps);
+template <typename R>
+static void launch_steps(const RunView<R>& v, int cur, int grid, int nsteps, cudaStream_t s, size_t smem) {
+  if (v.s.depth == 0) k_steps<R, 0><<<grid, 256, smem, s>>>(v, cur, nsteps);
+  else if (v.s.depth <= 2) k_steps<R, 2><<<grid, 256, smem, s>>>(v, cur, nsteps);
+  else k_steps<R, kMaxShapeDepth><<<grid, 256, smem, s>>>(v, cur, nsteps);
 }
 
 // the launch settings a run uses: the context's tuning, built-in defaults where it holds 0
@@ -980,6 +1082,12 @@ static int run_device_once(cm_context* ctx, const cm_run_desc* d, uint32_t* back
   c0.total_primaries = total;
   CM_CUDA(cudaMemcpyAsync(ctx->counters, &c0, sizeof(c0), cudaMemcpyHostToDevice, stream));
   const int grid = ctx->nsm * tu.blocks_per_sm;
+  // the kernels that read tables (flight, elastic, inelastic, steps) stage the blob's small-table prefix
+  // into shared memory unless CM_OPT_GLOBAL_TABLES; the others get a view without it
+  v.s.nstaged = 0;
+  RunView<R> vs = v;
+  if (!(ctx->options & CM_OPT_GLOBAL_TABLES)) vs.s.nstaged = v.s.nstage;
+  const size_t smem = (size_t)vs.s.nstaged * sizeof(R);
   const int maxIt = d->max_iterations > 0 ? d->max_iterations : 500000;
   cudaEvent_t e0, e1;
   CM_CUDA(cudaEventCreate(&e0));
@@ -1000,11 +1108,14 @@ static int run_device_once(cm_context* ctx, const cm_run_desc* d, uint32_t* back
   for (int it = 0; it < 2 * K; ++it) {
     const int cur = it & 1;
     cudaEvent_t* ev = d->profile ? &pev[(size_t)it * 6 + 1] : nullptr;
-    launch_flight(v, cur, grid, stream);
+    if (CM_STAGE_KERNELS & 1) launch_flight(vs, cur, grid, stream, smem);
+    else launch_flight(v, cur, grid, stream);
     if (ev) cudaEventRecordWithFlags(ev[0], stream, cudaEventRecordExternal);
-    k_elastic<R><<<grid, 256, 0, stream>>>(v, cur);
+    if (CM_STAGE_KERNELS & 2) k_elastic<R><<<grid, 256, smem, stream>>>(vs, cur);
+    else k_elastic<R><<<grid, 256, 0, stream>>>(v, cur);
     if (ev) cudaEventRecordWithFlags(ev[1], stream, cudaEventRecordExternal);
-    k_inelastic<R><<<grid, 256, 0, stream>>>(v, cur);
+    if (CM_STAGE_KERNELS & 4) k_inelastic<R><<<ctx->nsm * CM_INEL_BLOCKS_PER_SM, 256, smem, stream>>>(vs, cur);
+    else k_inelastic<R><<<grid, 256, 0, stream>>>(v, cur);
     if (ev) cudaEventRecordWithFlags(ev[2], stream, cudaEventRecordExternal);
     launch_misc<R>(v, cur, grid, stream);
     if (ev) cudaEventRecordWithFlags(ev[3], stream, cudaEventRecordExternal);
@@ -1049,7 +1160,9 @@ static int run_device_once(cm_context* ctx, const cm_run_desc* d, uint32_t* back
       }
     }
     if (ctx->counters_host->error) {
-      status = fail(ctx->counters_host->error, "secondary pool overflow; raise the wave size");
+      const int err = ctx->counters_host->error;
+      status = err == CM_ETIMEOUT ? fail(err, "a table copy into shared memory did not complete in time")
+                                  : fail(err, "secondary pool overflow; raise the wave size");
       break;
     }
     if (ctx->counters_host->done) break;
@@ -1073,7 +1186,8 @@ static int run_device_once(cm_context* ctx, const cm_run_desc* d, uint32_t* back
         for (int it = 0; it < 2 * K; ++it) {
           const int cur = it & 1;
           cudaEvent_t* ev = d->profile ? &tev[(size_t)it * 3 + 1] : nullptr;
-          launch_steps(v, cur, grid, tu.tail_steps, stream);
+          if (CM_STAGE_KERNELS & 8) launch_steps(vs, cur, grid, tu.tail_steps, stream, smem);
+          else launch_steps(v, cur, grid, tu.tail_steps, stream, 0);
           if (ev) cudaEventRecordWithFlags(ev[0], stream, cudaEventRecordExternal);
           launch_spawn<R>(v, cur, grid, stream);
           if (ev) cudaEventRecordWithFlags(ev[1], stream, cudaEventRecordExternal);

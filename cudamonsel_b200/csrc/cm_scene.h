@@ -151,6 +151,8 @@ struct SceneView {
   int depth;                 // deepest intersection nesting; 0 = every shape is a leaf (plane set or sphere)
   double dl50, param;        // NISTMott log-energy grid (eV)
   double maxMott;            // NISTMottRS MAX_NISTMOTT in eV
+  int nstaged;               // elements of blob's prefix this kernel holds in shared memory (0: none)
+  int nstage;                // elements of the prefix the scene places for staging (a multiple of 16 bytes)
 };
 
 }  // namespace cm

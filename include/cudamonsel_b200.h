@@ -37,6 +37,7 @@ extern "C" {
 #define CM_EOVERFLOW -5 /* a device queue overflowed (secondary pool too small) */
 #define CM_ELIMIT -6    /* iteration limit reached before all trajectories ended */
 #define CM_ECANCELED -7 /* the job was cancelled */
+#define CM_ETIMEOUT -8  /* a bounded wait on the device ran out (a table copy into shared memory did not land) */
 
 #define CM_PREC_FP64 0  /* plain form: all transport arithmetic in double */
 #define CM_PREC_FP32 1  /* batched form: float physics, double positions and plane solves */
@@ -46,6 +47,8 @@ extern "C" {
                                   FP32 merges intersections of plane sets into single plane sets */
 #define CM_OPT_SCAN_CHILDREN 4 /* test every child of a region in order, as RegionBase does; by default a region
                                   with many children finds them through an x-y grid (same results) */
+#define CM_OPT_GLOBAL_TABLES 16 /* kernels read every table from global memory (through L1/L2); by default the small
+                                   tables are staged into each block's shared memory by a bulk copy (same results) */
 #define CM_OPT_QUEUE_STEPS 8   /* one step per iteration through the queue kernels to the end of a run; by default
                                   the tail of a run (fewer electrons left than fill the GPU) takes several whole
                                   steps per thread (same results) */

@@ -422,6 +422,23 @@ def test_autotune_and_settings_keep_the_tallies(prec):
         assert s.steps == s0.steps and np.array_equal(b, b0) and np.array_equal(f, f0)
 
 
+@pytest.mark.parametrize("prec", [FP64, FP32], ids=["fp64", "fp32"])
+def test_staged_tables_give_the_same_tallies(prec):
+    """The event kernels read the small tables from shared memory (a bulk copy per block);
+    CM_OPT_GLOBAL_TABLES reads them from global memory.  Same seed: identical tallies, for the lines
+    (Si and PMMA tables) and for a run whose tail goes to k_steps."""
+    from cudamonsel_b200 import capi, scenes
+    e = capi.Engine(0)
+    h = scenes.build_engine(scenes.lines(), e)
+    c = scenes.linescan_pixels(48)
+    b0, f0, s0 = e.run(h["chamber"], c, scenes.eV(500.0), 300, 50, 1e-9, seed=12, precision=prec)
+    e.set_options(capi.OPT_GLOBAL_TABLES)
+    b1, f1, s1 = e.run(h["chamber"], c, scenes.eV(500.0), 300, 50, 1e-9, seed=12, precision=prec)
+    e.close()
+    assert s0.step_launches > 0
+    assert s0.steps == s1.steps and np.array_equal(b0, b1) and np.array_equal(f0, f1)
+
+
 def test_deterministic_and_independent_of_batch(half):
     """Same seed -> identical tallies; a pixel's tally is the same alone and inside a larger
     batch of other pixels when it carries the same stream key (the serving guarantee)."""
