@@ -84,10 +84,9 @@ class Clocks:
 
 
 def linescan_inputs(rank):
-    from cudamonsel_b200 import scenes
+    from cudamonsel_b200 import replicas, scenes
     centers = scenes.linescan_pixels(NPIX, 1e-9, 0.0, -120e-9)
-    keys = (np.arange(NPIX, dtype=np.uint64) + np.uint64(1_000_003 * (rank + 1)))
-    return centers, keys
+    return centers, replicas.pixel_keys(rank, NPIX)
 
 
 # ------------------------------------------------------------------ CPU arms
@@ -187,7 +186,7 @@ def main():
     import torch
     import torch.distributed as dist
     from datetime import timedelta
-    from cudamonsel_b200 import capi, scenes
+    from cudamonsel_b200 import capi, replicas, scenes
 
     torch.cuda.set_device(local)
     if world > 1:
@@ -249,14 +248,10 @@ def main():
     if world > 1:
         dist.barrier()
     clk = clocks.stop()
-    ms = sum(e0.elapsed_time(e1) for e0, e1 in ev)
-    t = torch.tensor([ms], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms = float(t.item())
+    ms = replicas.max_over_ranks(sum(e0.elapsed_time(e1) for e0, e1 in ev), dev)
     back32 = t_back.cpu().numpy().astype(np.int64)
     prim_per_rank = NPIX * NPRIM
-    value = world * prim_per_rank * a.steps / (ms / 1000.0)
+    value = replicas.job_rate(prim_per_rank * a.steps, world, ms)
 
     # FP64 plain form on the same workload: throughput and the yield error of FP32 against it
     torch.cuda.synchronize()
@@ -282,10 +277,7 @@ def main():
         t0 = time.perf_counter()
         eng.run(h["chamber"], centers, scenes.eV(BEAM_EV), NPRIM, NBINS, 1e-9, 0, precision=prec, pixel_keys=keys)
         e2e_ms += 1000 * (time.perf_counter() - t0)
-    te = torch.tensor([e2e_ms], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(te, op=dist.ReduceOp.MAX)
-    e2e_value = world * prim_per_rank * a.steps / (float(te.item()) / 1000.0)
+    e2e_value = replicas.job_rate(prim_per_rank * a.steps, world, replicas.max_over_ranks(e2e_ms, dev))
     h2d = NPIX * (3 * 8 + 8 + 4 + 4 + 8)
     d2h = 2 * NPIX * stride * 4
 
