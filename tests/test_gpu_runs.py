@@ -439,6 +439,42 @@ def test_staged_tables_give_the_same_tallies(prec):
     assert s0.steps == s1.steps and np.array_equal(b0, b1) and np.array_equal(f0, f1)
 
 
+@pytest.fixture(scope="module")
+def penn_runs(tmp_path_factory):
+    """Scattering tables from the dielectric model (small grids) and oracle runs on them."""
+    import pyoracle
+    from cudamonsel_b200 import scenes
+    from cudamonsel_b200.data import gen_penn_tables, gen_si_tables
+    d = str(tmp_path_factory.mktemp("penn"))
+    gen_penn_tables.build(d, n_iimfp=48, n_loss=24, n_theta=(16, 17, 17))
+    tables = [os.path.join(d, n) for n in gen_si_tables.NAMES]
+    ob, _, _ = pyoracle.run_scene(scenes.halfspace(tables=tables), np.tile([0.0, 0.0, -20e-9], (8, 1)), 0.0,
+                                  scenes.eV(1000.0), 1500, 51, 100)
+    return tables, ob
+
+
+@pytest.mark.parametrize("prec", [FP64, FP32], ids=["fp64", "fp32"])
+def test_penn_tables_match_oracle(penn_runs, prec):
+    """Tables generated from the dielectric model (Penn single-pole algorithm) run on the engine: flat Si,
+    1 keV, engine 32 x 500 primaries vs the oracle's 8 x 1500 on the same tables."""
+    from cudamonsel_b200 import capi, scenes, stats
+    tables, ob = penn_runs
+    e = capi.Engine(0)
+    h = scenes.build_engine(scenes.halfspace(tables=tables), e)
+    back, _, st = e.run(h["chamber"], np.tile([0.0, 0.0, -20e-9], (32, 1)), scenes.eV(1000.0), 500, 100, 0.0,
+                        seed=8, precision=prec)
+    e.close()
+    eb, es = batch_yields(back, 500, 1000.0, 100)
+    rb, rs = batch_yields(ob, 1500, 1000.0, 100)
+    for name, a, r in (("BSE", eb, rb), ("SE", es, rs)):
+        se = np.sqrt(a.var(ddof=1) / len(a) + r.var(ddof=1) / len(r))
+        z = (a.mean() - r.mean()) / max(se, 1e-12)
+        print("%s engine %.4f oracle %.4f z=%.2f" % (name, a.mean(), r.mean(), z))
+        assert abs(z) < 4
+    _, _, p = stats.chi2_two_sample(back.sum(0), 16000, ob.sum(0), 12000)
+    assert p > 1e-3
+
+
 def test_deterministic_and_independent_of_batch(half):
     """Same seed -> identical tallies; a pixel's tally is the same alone and inside a larger
     batch of other pixels when it carries the same stream key (the serving guarantee)."""
