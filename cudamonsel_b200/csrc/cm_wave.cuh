@@ -60,13 +60,33 @@ template <typename R> CM_D El<R> load(const Wave<R>& w, int i) {
   return e;
 }
 
-template <typename R> CM_D void store(const Wave<R>& w, int i, const El<R>& e) {
+// The fields a step starts from (position, direction, energy, region, pixel, step count, key).  Ep, aux
+// and the hit normal are written by the flight for its event and read only by that event, so records
+// moved between waves and the pool carry the live fields alone (60 of 80 bytes in FP32).
+template <typename R> CM_D El<R> load_live(const Wave<R>& w, int i) {
+  El<R> e;
+  e.p[0] = w.px[i]; e.p[1] = w.py[i]; e.p[2] = w.pz[i];
+  e.d[0] = w.dx[i]; e.d[1] = w.dy[i]; e.d[2] = w.dz[i];
+  e.E = w.E[i];
+  e.region = w.region[i]; e.pixel = w.pixel[i];
+  e.step = w.step[i]; e.key = w.key[i];
+  return e;
+}
+
+template <typename R> CM_D void store_live(const Wave<R>& w, int i, const El<R>& e) {
   w.px[i] = e.p[0]; w.py[i] = e.p[1]; w.pz[i] = e.p[2];
   w.dx[i] = e.d[0]; w.dy[i] = e.d[1]; w.dz[i] = e.d[2];
-  w.E[i] = e.E; w.Ep[i] = e.Ep;
-  w.region[i] = e.region; w.pixel[i] = e.pixel; w.aux[i] = e.aux;
+  w.E[i] = e.E;
+  w.region[i] = e.region; w.pixel[i] = e.pixel;
   w.step[i] = e.step; w.key[i] = e.key;
-  w.hx[i] = e.h[0]; w.hy[i] = e.h[1]; w.hz[i] = e.h[2];
+}
+
+// what an elastic or inelastic event reads: the live fields, the step's starting energy and the mechanism
+template <typename R> CM_D El<R> load_event(const Wave<R>& w, int i) {
+  El<R> e = load_live(w, i);
+  e.Ep = w.Ep[i];
+  e.aux = w.aux[i];
+  return e;
 }
 
 enum { Q_EL = 0, Q_TAB = 1, Q_MISC = 2 };
@@ -307,7 +327,7 @@ CM_D void flight_one(const RunView<R>& v, int cur, int i, Sink& sink, StepCounts
 template <typename R, typename Sink> CM_D void keep(const RunView<R>& v, int nxt, const El<R>& e, Sink& sink) {
   const int k = v.s.regions[e.region].cls;
   const int slot = sink.append_q(v.c->nc[nxt], k);
-  store(v.w[nxt], k * v.W + slot, e);
+  store_live(v.w[nxt], k * v.W + slot, e);
 }
 
 // wave index of the i-th electron of a wave counted over its class segments in order
@@ -346,7 +366,7 @@ CM_D void push_secondary(const RunView<R>& v, const El<R>& pe, const R sd[3], R 
     sink.error(&v.c->error, -5 /* CM_EOVERFLOW */);
     return;
   }
-  store(v.pool, slot, se);
+  store_live(v.pool, slot, se);
   ++sc.sec;
 }
 
@@ -408,12 +428,12 @@ template <typename R, int D, typename Sink> CM_D bool misc_apply(const RunView<R
 
 // the queue kernels' events: the record of queue entry j, its event, and the survivor kept
 template <typename R, typename Sink> CM_D void elastic_one(const RunView<R>& v, int cur, int j, Sink& sink) {
-  El<R> e = load(v.w[cur], v.q[Q_EL][j]);
+  El<R> e = load_event(v.w[cur], v.q[Q_EL][j]);
   if (elastic_apply(v, e)) keep(v, cur ^ 1, e, sink);
 }
 
 template <typename R, typename Sink> CM_D void inelastic_one(const RunView<R>& v, int cur, int j, Sink& sink, StepCounts& sc) {
-  El<R> e = load(v.w[cur], v.q[Q_TAB][j]);
+  El<R> e = load_event(v.w[cur], v.q[Q_TAB][j]);
   if (inelastic_apply(v, e, sink, sc)) keep(v, cur ^ 1, e, sink);
 }
 
@@ -428,7 +448,7 @@ CM_D void misc_one(const RunView<R>& v, int cur, int j, Sink& sink, StepCounts& 
 // with the same random streams as the queue kernels, without a launch and a queue per event.
 template <typename R, int D, typename Sink>
 CM_D void steps_one(const RunView<R>& v, int cur, int i, int nsteps, Sink& sink, StepCounts& sc) {
-  El<R> e = load(v.w[cur], i);
+  El<R> e = load_live(v.w[cur], i);
   for (int k = 0; k < nsteps; ++k) {
     const int q = flight_apply<R, D>(v, e, sink, sc);
     if (q < 0) return;
@@ -460,9 +480,9 @@ template <typename R, int D, typename Sink>
 CM_D void spawn_one(const RunView<R>& v, int nxt, int j, int take_se, int poolTop, unsigned long long first,
                     Sink& sink) {
   if (j < take_se) {
-    const El<R> se = load(v.pool, poolTop - 1 - j);
+    const El<R> se = load_live(v.pool, poolTop - 1 - j);
     const int seg = v.s.regions[se.region].cls;
-    store(v.w[nxt], seg * v.W + v.c->nc[nxt][seg] + sink.append_q(v.c->ns, seg), se);
+    store_live(v.w[nxt], seg * v.W + v.c->nc[nxt][seg] + sink.append_q(v.c->ns, seg), se);
     return;
   }
   // GaussianBeam::createElectron (NISTMonte/GaussianBeam.cu:52-65) + initializeTrajectory (MonteCarloSS.cu:99-105)
@@ -493,7 +513,7 @@ CM_D void spawn_one(const RunView<R>& v, int nxt, int j, int take_se, int poolTo
   e.step = 0;
   e.h[0] = e.h[1] = e.h[2] = 0;
   const int seg = e.region >= 0 ? v.s.regions[e.region].cls : 0;
-  store(v.w[nxt], seg * v.W + v.c->nc[nxt][seg] + sink.append_q(v.c->ns, seg), e);
+  store_live(v.w[nxt], seg * v.W + v.c->nc[nxt][seg] + sink.append_q(v.c->ns, seg), e);
 }
 
 // end of an iteration: counters of the next wave, reset of this one (steps: the iteration ran k_steps)
