@@ -317,6 +317,14 @@ def main():
         hi = scenes.build_engine(img, eimg)
         ic, ie, inp, inb = scenes.rough_image(seed=rank)
         ikeys = np.arange(len(ic), dtype=np.uint64) + np.uint64(7_000_003 * (rank + 1))
+        # both precisions autotuned on the first eighth of the pixel rows (outside the timed runs)
+        itune = {}
+        if not a.no_autotune:
+            band = slice(0, len(ic) // 8)
+            for name, pr in (("fp32", capi.PREC_FP32), ("fp64", capi.PREC_FP64)):
+                tt = eimg.autotune(hi["chamber"], ic[band], ie[band], inp[band], inb[band], 1e-9, 0, precision=pr,
+                                   pixel_keys=ikeys[band])
+                itune[name] = {k: v for k, v in tt.as_dict().items() if k != "ms"}
         runs = {}
         for name, pr in (("fp32", capi.PREC_FP32), ("fp64", capi.PREC_FP64)):
             t0 = time.perf_counter()
@@ -332,7 +340,7 @@ def main():
             err[nm + "_fp32"], err[nm + "_fp64"], err[nm + "_rel_err"] = a32, a64, abs(a32 - a64) / a64
         image_line = {"workload": "rough lines 3 x 128 segments (sidewall offsets N(0, 1.5 nm)), 256 x 256 px at "
                                   "2 nm, Poisson(300)/px, E per row in {300, 500, 1000} eV",
-                      "primaries": ntot,
+                      "primaries": ntot, "tuning": itune or "defaults",
                       "fp32_primaries_per_s": ntot / (runs["fp32"][1].device_ms / 1e3),
                       "fp64_primaries_per_s": ntot / (runs["fp64"][1].device_ms / 1e3),
                       "fp32_over_fp64": runs["fp64"][1].device_ms / runs["fp32"][1].device_ms,
