@@ -395,6 +395,51 @@ def test_escape_log_rebuilds_the_tallies(prec):
 
 
 @pytest.mark.parametrize("prec", [FP64, FP32], ids=["fp64", "fp32"])
+def test_angle_histograms_and_log_through_run_device(prec):
+    """cm_run_device with device arrays for the angle histograms and the escape log (filled with garbage
+    first: the run clears the histograms) gives what cm_run gives with host arrays for the same keys."""
+    import ctypes as C
+    import torch
+    from cudamonsel_b200 import capi, scenes
+    e = capi.Engine(0)
+    h = scenes.build_engine(scenes.lines(), e)
+    npix, nprim, nb = 24, 150, 50
+    c = scenes.linescan_pixels(npix)
+    keys = np.arange(npix, dtype=np.uint64) + np.uint64(777)
+    back, fwd, st, ex = e.run(h["chamber"], c, scenes.eV(500.0), nprim, nb, 1e-9, 0, precision=prec, angles=True,
+                              escape_log_cap=100000, pixel_keys=keys)
+    dev = torch.device("cuda", 0)
+    tc = torch.tensor(c.ravel(), dtype=torch.float64, device=dev)
+    te = torch.full((npix,), scenes.eV(500.0), dtype=torch.float64, device=dev)
+    tn = torch.full((npix,), nprim, dtype=torch.int32, device=dev)
+    tb = torch.full((npix,), nb, dtype=torch.int32, device=dev)
+    tk = torch.tensor(keys.astype(np.int64), device=dev)
+    tback = torch.zeros((npix, nb + 2), dtype=torch.int32, device=dev)
+    tfwd = torch.zeros_like(tback)
+    tel = torch.full((npix, capi.ELEVATION_COUNTS), 9, dtype=torch.int32, device=dev)
+    taz = torch.full((npix, capi.AZIMUTH_COUNTS), 9, dtype=torch.int32, device=dev)
+    tlog = torch.zeros((100000, capi.ESCAPE_RECORD.itemsize // 8), dtype=torch.int64, device=dev)
+    P = lambda x, ty: C.cast(C.c_void_p(x.data_ptr()), C.POINTER(ty))
+    d = capi.RunDesc(h["chamber"], prec, npix, 1e-9, P(tc, C.c_double), P(te, C.c_double), P(tn, C.c_int),
+                     P(tb, C.c_int), 0, nb + 2, 0, 0, P(tk, C.c_uint64), 0)
+    d.elevation = P(tel, C.c_uint32)
+    d.azimuth = P(taz, C.c_uint32)
+    d.escape_log = tlog.data_ptr()
+    d.escape_log_cap = 100000
+    st2 = e.run_device(d, tback.data_ptr(), tfwd.data_ptr())
+    torch.cuda.synchronize()
+    e.close()
+    assert st2.escapes == st.escapes
+    assert np.array_equal(tback.cpu().numpy().astype(np.uint32), back)
+    assert np.array_equal(tel.cpu().numpy().astype(np.uint32), ex["elevation"])
+    assert np.array_equal(taz.cpu().numpy().astype(np.uint32), ex["azimuth"])
+    log2 = tlog.cpu().numpy()[:st2.escapes].copy().view(capi.ESCAPE_RECORD).ravel()
+    order = lambda g: np.lexsort((g["step"], g["electron"]))
+    a, b = ex["escape_log"][order(ex["escape_log"])], log2[order(log2)]
+    assert np.array_equal(a["electron"], b["electron"]) and np.array_equal(a["energy_eV"], b["energy_eV"])
+
+
+@pytest.mark.parametrize("prec", [FP64, FP32], ids=["fp64", "fp32"])
 def test_autotune_and_settings_keep_the_tallies(prec):
     """cm_autotune keeps the fastest launch settings for the precision it tuned; runs under the tuned,
     the default and deliberately odd settings (small waves, short tail steps, few blocks) give the
