@@ -151,7 +151,7 @@ typedef struct {
   const int* pixel_nbins;      /* [npix], 1..1024 */
   uint64_t seed;
   int hist_stride;             /* >= max(pixel_nbins) + 2 */
-  int wave;                    /* electrons per wave; 0 = default */
+  int wave;                    /* electrons per wave; 0 = the context's cm_tuning.wave, else the default */
   int max_iterations;          /* 0 = default */
   const uint64_t* pixel_key;   /* [npix] random-stream key of each pixel, or NULL: derived from seed and index.
                                   A pixel's result depends only on its key, its beam and primary count,
