@@ -951,7 +951,7 @@ static void launch_steps(const RunView<R>& v, int cur, int grid, int nsteps, cud
 // the launch settings a run uses: the context's tuning, built-in defaults where it holds 0
 template <typename R> static cm_tuning resolved_tuning(const cm_context* ctx) {
   cm_tuning t = ctx->tune[sizeof(R) == 8 ? CM_PREC_FP64 : CM_PREC_FP32];
-  if (t.wave <= 0) t.wave = sizeof(R) == 8 ? (1 << 20) : (1 << 21);
+  if (t.wave <= 0) t.wave = 1 << 21;
   if (t.tail_below <= 0) t.tail_below = CM_TAIL_BELOW;
   if (t.tail_steps <= 0) t.tail_steps = CM_TAIL_STEPS;
   if (t.blocks_per_sm <= 0) t.blocks_per_sm = 8;
@@ -2113,6 +2113,7 @@ int cm_autotune(cm_context* ctx, const cm_run_desc* d, cm_tuning* best) {
       cm_tuning t = cur;
       t.*field = vals[k];
       const int r = trial(t, ms);
+      if (r == CM_ENOMEM) continue;  // a candidate wave that does not fit is skipped
       if (r) return r;
       if (ms < 0.99 * cur_ms) {
         cur = t;

@@ -204,10 +204,11 @@ template <typename R, typename Sink> CM_D void cm_trace(const RunView<R>& v, con
 // region check, MONSEL_MaterialScatterModel::randomMeanPathLength, the
 // candidate point, RegionBase::findEndOfStep, the slowing-down loss, the
 // tracking cut; the step's end is queued for its event kernel, escapes are tallied.
-// One step's flight on a record held in registers (p, d, E, step, region, key and pixel valid): the
-// event queue of its end, or -1 when the electron ended here (escaped and tallied, stopped, trapped).
+// One step's flight on a record held in registers (p, d, E, step, region and key valid; the pixel too,
+// or, when pixel_src is given, read from there if the electron escapes): the event queue of its end, or
+// -1 when the electron ended here (escaped and tallied, stopped, trapped).
 template <typename R, int D, typename Sink>
-CM_D int flight_apply(const RunView<R>& v, El<R>& e, Sink& sink, StepCounts& sc) {
+CM_D int flight_apply(const RunView<R>& v, El<R>& e, Sink& sink, StepCounts& sc, const int* pixel_src = nullptr) {
   const SceneView<R>& s = v.s;
   int reg = e.region;
   if (reg < 0 || !shape_contains<R, D>(s, s.regions[reg].shape, e.p)) reg = containing_subregion<R, D>(s, s.chamber, e.p);
@@ -287,6 +288,7 @@ CM_D int flight_apply(const RunView<R>& v, El<R>& e, Sink& sink, StepCounts& sc)
     e.h[0] = (R)hn[0]; e.h[1] = (R)hn[1]; e.h[2] = (R)hn[2];
   } else {
     ++sc.esc;
+    if (pixel_src) e.pixel = *pixel_src;
     tally_escape(v, e, sink);
 #ifdef CM_TRACE
     cm_trace(v, e, next, 9, sink);
@@ -311,8 +313,7 @@ CM_D void flight_one(const RunView<R>& v, int cur, int i, Sink& sink, StepCounts
   e.step = W.step[i];
   e.region = W.region[i];
   e.key = W.key[i];
-  e.pixel = W.pixel[i];
-  const int queue = flight_apply<R, D>(v, e, sink, sc);
+  const int queue = flight_apply<R, D>(v, e, sink, sc, W.pixel + i);  // the pixel is read only on escape
   if (queue < 0) return;
   W.px[i] = e.p[0]; W.py[i] = e.p[1]; W.pz[i] = e.p[2];
   W.E[i] = e.E; W.Ep[i] = e.Ep;

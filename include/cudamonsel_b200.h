@@ -67,7 +67,7 @@ int cm_set_options(cm_context* ctx, int options);
  * time), one set per precision.  0 = the built-in default.  Every setting gives the same tallies, because
  * each electron's random stream is keyed by its lineage, so they change only the speed. */
 typedef struct {
-  int wave;                    /* electrons per wave segment (default 2^21 in FP32, 2^20 in FP64) */
+  int wave;                    /* electrons per wave segment (default 2^21) */
   int tail_below;              /* k_steps runs the tail once fewer electrons are left (default 262144) */
   int tail_steps;              /* whole steps per thread and launch in the tail (default 32) */
   int blocks_per_sm;           /* grid = SMs x blocks_per_sm blocks of 256 threads (default 8) */
