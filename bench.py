@@ -8,9 +8,13 @@ Gaussian beam (sigma 1 nm) landing on 256 pixels 1 nm apart across the
 middle line, 2000 primaries per pixel (512 000 primaries), synthetic tables.
 Metric: primary electrons per second, FP32 transport (FP64 positions and
 plane solves), with the linescan yields checked against an FP64 run of the
-same workload.  Under torchrun each rank runs the full linescan with its own
-random streams (weak scaling, no collective on the data path); the time is
-the max over ranks.
+same workload.  Before the warm-up the engine's autotuner picks the launch
+settings of each precision on this workload (--no-autotune: defaults); they
+are printed in config.tuning.  Under torchrun each rank runs the full linescan
+with its own random streams (weak scaling, no collective on the data path);
+the time is the max over ranks.  Further lines: the rough-line image (both
+precisions autotuned on its first eighth of rows), the 10 keV deep layout and
+the served stream.
 """
 import argparse
 import json
