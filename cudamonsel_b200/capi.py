@@ -19,6 +19,8 @@ OPT_EXACT_CSG = 2
 OPT_SCAN_CHILDREN = 4
 OPT_QUEUE_STEPS = 8
 OPT_GLOBAL_TABLES = 16
+# CM_E* statuses (include/cudamonsel_b200.h)
+EINVAL, ECUDA, ENOMEM, ESTATE, EOVERFLOW, ELIMIT, ECANCELED, ETIMEOUT = -1, -2, -3, -4, -5, -6, -7, -8
 
 # every symbol include/cudamonsel_b200.h declares
 EXPORTS = (
@@ -27,7 +29,7 @@ EXPORTS = (
     "cm_msm_add_tabulated", "cm_msm_add_fitted", "cm_msm_add_phonon", "cm_msm_add_polaron", "cm_msm_set_csd_jln",
     "cm_msm_set_min_e", "cm_msm_set_barrier", "cm_shape_sphere", "cm_shape_planes", "cm_shape_intersection",
     "cm_shape_union", "cm_shape_cylinder", "cm_shape_translate", "cm_shape_line", "cm_region_add", "cm_run", "cm_run_device", "cm_run_noalloc",
-    "cm_eval_nistmott", "cm_eval_table", "cm_eval_tabulated", "cm_eval_elastic", "cm_eval_csd", "cm_eval_phonon",
+    "cm_eval_nistmott", "cm_eval_table", "cm_eval_locate", "cm_eval_pick", "cm_eval_tabulated", "cm_eval_elastic", "cm_eval_csd", "cm_eval_phonon",
     "cm_eval_shape", "cm_eval_barrier", "cm_eval_freepath", "cm_server_create", "cm_server_destroy", "cm_job_submit",
     "cm_job_poll", "cm_job_wait", "cm_job_cancel", "cm_job_result", "cm_get_tuning", "cm_set_tuning", "cm_autotune",
 )
@@ -85,7 +87,11 @@ class RunStats(C.Structure):
 
 
 class CMError(RuntimeError):
-    pass
+    """A CM_E* status from the library; .code is the status."""
+
+    def __init__(self, msg, code=0):
+        super().__init__(msg)
+        self.code = code
 
 
 _libs = {}
@@ -141,6 +147,8 @@ def load(path=LIBPATH):
         "cm_job_result": [C.c_void_p, C.c_int, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.POINTER(RunStats)],
         "cm_eval_nistmott": [ctx, C.c_int, C.c_int, C.c_int, d, d, d, d, C.c_int],
         "cm_eval_table": [ctx, C.c_int, C.c_int, d, C.c_int, d, C.c_int],
+        "cm_eval_locate": [ctx, C.c_int, C.c_int, d, C.c_int, i, C.c_int],
+        "cm_eval_pick": [ctx, C.c_int, C.c_int, d, d, C.c_int],
         "cm_eval_tabulated": [ctx, C.c_int, C.c_int, C.c_int, d, d, C.c_int],
         "cm_eval_elastic": [ctx, C.c_int, C.c_int, C.c_int, d, d, C.c_int],
         "cm_eval_csd": [ctx, C.c_int, C.c_int, d, d, C.c_int],
@@ -196,7 +204,7 @@ class Engine:
 
     def _check(self, rc):
         if rc != 0:
-            raise CMError("cudamonsel_b200 error %d: %s" % (rc, self.L.cm_last_error().decode()))
+            raise CMError("cudamonsel_b200 error %d: %s" % (rc, self.L.cm_last_error().decode()), rc)
 
     def _out(self, fn, *args):
         o = C.c_int(-1)
@@ -379,6 +387,18 @@ class Engine:
                                          out.ctypes.data_as(C.POINTER(C.c_double)), precision))
         return out
 
+    def eval_locate(self, table, x3, order, precision=PREC_FP64):
+        """cm_eval_locate: int array [n, 6] of (first, nearest) per axis (-1 for missing axes)."""
+        x3 = np.ascontiguousarray(x3, dtype=np.float64)
+        out = np.zeros((len(x3), 6), dtype=np.int32)
+        self._check(self.L.cm_eval_locate(self.h, table, len(x3), x3.ctypes.data_as(C.POINTER(C.c_double)), order,
+                                          out.ctypes.data_as(C.POINTER(C.c_int)), precision))
+        return out
+
+    def eval_pick(self, msm, inp, precision=PREC_FP64):
+        """cm_eval_pick: [n, 2] of (mechanism index, total rate in 1/m) for rows (E in J, deviate)."""
+        return self._eval(self.L.cm_eval_pick, (msm,), inp, 2, precision)
+
     def eval_tabulated(self, msm, mech, inp, precision=PREC_FP64):
         return self._eval(self.L.cm_eval_tabulated, (msm, mech), inp, 12, precision)
 
@@ -425,13 +445,13 @@ class Server:
         h = C.c_void_p()
         rc = self.L.cm_server_create(device, slots, budget_gb, C.byref(h))
         if rc:
-            raise CMError("cudamonsel_b200 error %d: %s" % (rc, self.L.cm_last_error().decode()))
+            raise CMError("cudamonsel_b200 error %d: %s" % (rc, self.L.cm_last_error().decode()), rc)
         self.h = h
         self.shape = {}
 
     def _check(self, rc):
         if rc != 0:
-            raise CMError("cudamonsel_b200 error %d: %s" % (rc, self.L.cm_last_error().decode()))
+            raise CMError("cudamonsel_b200 error %d: %s" % (rc, self.L.cm_last_error().decode()), rc)
 
     def close(self):
         if getattr(self, "h", None):

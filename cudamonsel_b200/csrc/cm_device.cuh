@@ -289,19 +289,18 @@ template <typename R> CM_D R nu_neville1(R f0, R f1, R x0, R x1, int ns, R x) {
   return ns == 0 ? f0 + ho * den : f1 + hp * den;
 }
 
-// NULagrangeInterpolation.cu:131-147 for a 1-D table, order 1 (TabulatedInelasticSM::scatterRate)
-template <typename R> CM_D R nu_d1_order1(const R* f, const R* xs, int n, R x) {
-  int first, nearest;
-  nu_locate(x, xs, n, 1, first, nearest);
-  return nu_neville1(f[first], f[first + 1], xs[first], xs[first + 1], nearest - first, x);
+// Window selection of every table lookup: NULagrangeInterpolation::locate on the axis's double copy with
+// the argument promoted to double, so FP32 picks exactly the window and nearest node the reference picks
+// for the same (float) argument; comparing with float-rounded abscissae would move the boundaries.
+CM_D void nu_window(double x, const double* xsd, int n, int order, int& first, int& nearest) {
+  nu_locate<double>(x, xsd, n, order, first, nearest);
 }
 
-// d1 of order 3 on a small 4-point array (the last step of d2/d3)
-template <typename R> CM_D R nu_d1_4(const R* fv, const R* xv, R x) {
+// NULagrangeInterpolation.cu:131-147 for a 1-D table, order 1 (TabulatedInelasticSM::scatterRate)
+template <typename R> CM_D R nu_d1_order1(const R* f, const R* xs, const double* xsd, int n, R x) {
   int first, nearest;
-  nu_locate(x, xv, 4, 3, first, nearest);
-  // first is always 0 for a 4-point array
-  return nu_neville3(fv, xv, nearest - first, x);
+  nu_window((double)x, xsd, n, 1, first, nearest);
+  return nu_neville1(f[first], f[first + 1], xs[first], xs[first + 1], nearest - first, x);
 }
 
 // Lagrange weights of the cubic through the 4 abscissae xv at x.  d2 and d3 evaluate many cubics on
@@ -318,11 +317,12 @@ template <typename R> CM_D void lag4(const R* xv, R x, R w[4]) {
 template <typename R> CM_D R dot4(const R w[4], const R* f) { return w[0] * f[0] + w[1] * f[1] + w[2] * f[2] + w[3] * f[3]; }
 
 // NULagrangeInterpolation.cu:169-192 on a 2-D table (order 3)
-template <typename R> CM_D R nu_d2(const R* f, const R* xs0, int n0, const R* xs1, int n1, R xa, R xb) {
+template <typename R>
+CM_D R nu_d2(const R* f, const R* xs0, const double* xs0d, int n0, const R* xs1, const double* xs1d, int n1, R xa, R xb) {
   int i0, near0;
-  nu_locate(xa, xs0, n0, 3, i0, near0);
+  nu_window((double)xa, xs0d, n0, 3, i0, near0);
   int j0, near1;
-  nu_locate(xb, xs1, n1, 3, j0, near1);
+  nu_window((double)xb, xs1d, n1, 3, j0, near1);
   R xv1[4] = {xs1[j0], xs1[j0 + 1], xs1[j0 + 2], xs1[j0 + 3]};
   R w1[4];
   lag4(xv1, xb, w1);
@@ -337,13 +337,14 @@ template <typename R> CM_D R nu_d2(const R* f, const R* xs0, int n0, const R* xs
 
 // NULagrangeInterpolation.cu:215-240 on a 3-D table (order 3).  The reference's
 // final 1-D step uses xsamp[0][0..3] (line 236) whatever the window; `fixes`
-// uses the window's own abscissae.
-template <typename R> CM_D R nu_d3(const R* f, const R* xs0, int n0, const R* xs1, int n1, const R* xs2, int n2, R xa, R xb,
-                                   R xc, bool fixes) {
+// uses the window's own abscissae.  Evaluated in double in both precisions (see Table).
+CM_D double nu_d3(const double* f, const double* xs0, int n0, const double* xs1, int n1, const double* xs2, int n2,
+                  double xa, double xb, double xc, bool fixes) {
+  using R = double;
   int i0, near0, j0, near1, k0, near2;
-  nu_locate(xa, xs0, n0, 3, i0, near0);
-  nu_locate(xb, xs1, n1, 3, j0, near1);
-  nu_locate(xc, xs2, n2, 3, k0, near2);
+  nu_window((double)xa, xs0, n0, 3, i0, near0);
+  nu_window((double)xb, xs1, n1, 3, j0, near1);
+  nu_window((double)xc, xs2, n2, 3, k0, near2);
   R xv1[4] = {xs1[j0], xs1[j0 + 1], xs1[j0 + 2], xs1[j0 + 3]};
   R xv2[4] = {xs2[k0], xs2[k0 + 1], xs2[k0 + 2], xs2[k0 + 3]};
   R w1[4], w2[4];
@@ -380,17 +381,32 @@ template <typename R> CM_D R table_interp(const SceneView<R>& s, int t, R x0, R 
   const Table& tb = s.tables[t];
   const R* v = blob_at(s, tb.off_v);
   if (tb.dim == 1) {
-    if (order == 1) return nu_d1_order1(v, blob_at(s, tb.off_x[0]), tb.n[0], x0);
+    const double* xsd = s.dbl + tb.off_x64[0];
+    if (order == 1) return nu_d1_order1(v, blob_at(s, tb.off_x[0]), xsd, tb.n[0], x0);
     int first, nearest;
     const R* xs = blob_at(s, tb.off_x[0]);
-    nu_locate(x0, xs, tb.n[0], 3, first, nearest);
+    nu_window((double)x0, xsd, tb.n[0], 3, first, nearest);
     R fv[4] = {v[first], v[first + 1], v[first + 2], v[first + 3]};
     R xv[4] = {xs[first], xs[first + 1], xs[first + 2], xs[first + 3]};
     return nu_neville3(fv, xv, nearest - first, x0);
   }
-  if (tb.dim == 2) return nu_d2(v, blob_at(s, tb.off_x[0]), tb.n[0], blob_at(s, tb.off_x[1]), tb.n[1], x0, x1);
-  return nu_d3(v, blob_at(s, tb.off_x[0]), tb.n[0], blob_at(s, tb.off_x[1]), tb.n[1], blob_at(s, tb.off_x[2]), tb.n[2], x0,
-               x1, x2, (s.options & 1) != 0);
+  if (tb.dim == 2)
+    return nu_d2(v, blob_at(s, tb.off_x[0]), s.dbl + tb.off_x64[0], tb.n[0], blob_at(s, tb.off_x[1]),
+                 s.dbl + tb.off_x64[1], tb.n[1], x0, x1);
+  return (R)nu_d3(s.dbl + tb.off_v64, s.dbl + tb.off_x64[0], tb.n[0], s.dbl + tb.off_x64[1], tb.n[1],
+                          s.dbl + tb.off_x64[2], tb.n[2], (double)x0, (double)x1, (double)x2, (s.options & 1) != 0);
+}
+
+// The windows NUTableInterpolation::interpolate selects for (x0, x1, x2): (first, nearest) per axis,
+// order 1 on a 1-D table as scatterRate uses it, else 3; unused axes give -1.
+template <typename R> CM_D void table_windows(const SceneView<R>& s, int t, R x0, R x1, R x2, int order, int out[6]) {
+  const Table& tb = s.tables[t];
+  const R xs[3] = {x0, x1, x2};
+  for (int k = 0; k < 3; ++k) {
+    out[2 * k] = out[2 * k + 1] = -1;
+    if (k < tb.dim) nu_window((double)xs[k], s.dbl + tb.off_x64[k], tb.n[k], tb.dim == 1 ? order : 3, out[2 * k],
+                              out[2 * k + 1]);
+  }
 }
 
 // ------------------------------------------------------------ elastic scattering
@@ -440,7 +456,7 @@ template <typename R, typename G> CM_D R nistmott_angle(const SceneView<R>& s, c
   if (E < (R)s.maxMott) {
     const double lg = log((double)E);  // double in both precisions: see ulagrange_d1
     const R u = g.next();
-    const double q = ulagrange_d2(s.mott64 + m.off_x1d, 61, 201, s.dl50, 0.0, s.param, 0.005, lg, (double)u);
+    const double q = ulagrange_d2(s.dbl + m.off_x1d, 61, 201, s.dl50, 0.0, s.param, 0.005, lg, (double)u);
     if (sizeof(R) == 4) {  // theta near pi: asin is ill-conditioned near 1, so q is not rounded to float first
       const double a = fabs(q);
       return a >= 1.0 ? (R)kPi : (R)(2.0 * asin(a));
@@ -547,13 +563,19 @@ template <typename R> CM_D R tabulated_rate(const SceneView<R>& s, const Mech& k
 
 // GanachaudMokraniPhononInelasticSM.cu:46-72
 template <typename R> CM_D R phonon_rate(const Mech& k, R kE) {
-  const R pe = (R)k.phononE;
-  if (kE < pe) return 0;
-  const R x = pe / kE;
-  if (x < R(0.1)) return (R)k.prefactor * x * mlog(R(4) / x);
-  if (x >= R(1)) return 0;
-  const R t = msqrt(R(1) - x);
-  return (R)k.prefactor * x * mlog((R(1) + t) / (R(1) - t));
+  // GanachaudMokraniPhononInelasticSM::scatterRate (GanachaudMokraniPhononInelasticSM.cu:46-72).  The energy
+  // ratio and the branch decisions are taken in double in both precisions (kE is exact in either), so a
+  // float phonon energy never moves an energy near threshold to the other branch; the common small-x
+  // form then runs in the compute precision, the rare x >= 0.1 form (E < 10 hbar omega) in double.
+  if ((double)kE < k.phononE) return 0;
+  const double xd = k.phononE / (double)kE;
+  if (xd < 0.1) {
+    const R x = (R)xd;
+    return (R)k.prefactor * x * mlog(R(4) / x);
+  }
+  if (xd >= 1.0) return 0;
+  const double t = sqrt(1.0 - xd);
+  return (R)(k.prefactor * xd * log((1.0 + t) / (1.0 - t)));
 }
 
 // ------------------------------------------------------------ geometry (double)

@@ -387,7 +387,7 @@ static int build_scene(cm_context* ctx, DevScene<R>& ds) {
   if (ds.valid) return 0;
   ds.release();
   std::vector<R> blob;
-  std::vector<double> mott64;
+  std::vector<double> dbl;  // SceneView::dbl
   // The blob holds every table's abscissae and values and the NIST Mott cross sections.  Pieces are
   // built apart and laid out small first: the prefix that fits kStageBytes is what the event kernels
   // copy into shared memory (the rest, such as a large 3-D angle table, is read through L1/L2).
@@ -413,8 +413,15 @@ static int build_scene(cm_context* ctx, DevScene<R>& ds) {
       pc.rel.push_back((int)pc.data.size());
       const double f = k == 0 ? ax0 : 1.0;
       for (double v : t.x[k]) pc.data.push_back((R)(v * f));
+      d.off_x64[k] = (int)dbl.size();
+      for (double v : t.x[k]) dbl.push_back(v * f);
       d.domain[k][0] = t.domain[k][0] * f;
       d.domain[k][1] = t.domain[k][1] * f;
+    }
+    d.off_v64 = -1;
+    if (t.dim == 3) {
+      d.off_v64 = (int)dbl.size();
+      for (double v : t.v) dbl.push_back(v * vf);
     }
     pc.offs.push_back(&d.off_v);
     pc.rel.push_back((int)pc.data.size());
@@ -438,8 +445,8 @@ static int build_scene(cm_context* ctx, DevScene<R>& ds) {
       for (double v : kv.second.spwem) pc.data.push_back((R)v);
       pieces.push_back(std::move(pc));
       m.off_x1 = -1;
-      m.off_x1d = (int)mott64.size();  // the quantile table in double as well (the angle's cubic needs it)
-      for (double v : kv.second.x1) mott64.push_back(v);
+      m.off_x1d = (int)dbl.size();  // the quantile table in double as well (the angle's cubic needs it)
+      for (double v : kv.second.x1) dbl.push_back(v);
       mottIndex[kv.first] = (int)mi++;
     }
   }
@@ -706,7 +713,7 @@ static int build_scene(cm_context* ctx, DevScene<R>& ds) {
       (rc = dev_copy(ds.allocs, regions, &v.regions, h)) || (rc = dev_copy(ds.allocs, children, &v.children, h)) ||
       (rc = dev_copy(ds.allocs, msms, &v.msms, h)) || (rc = dev_copy(ds.allocs, mechs, &v.mechs, h)) ||
       (rc = dev_copy(ds.allocs, motts, &v.mott, h)) || (rc = dev_copy(ds.allocs, tabs, &v.tables, h)) ||
-      (rc = dev_copy(ds.allocs, blob, &v.blob, h)) || (rc = dev_copy(ds.allocs, mott64, &v.mott64, h)) ||
+      (rc = dev_copy(ds.allocs, blob, &v.blob, h)) || (rc = dev_copy(ds.allocs, dbl, &v.dbl, h)) ||
       (rc = dev_copy(ds.allocs, grids, &v.grids, h)) || (rc = dev_copy(ds.allocs, cell_start, &v.cell_start, h)) ||
       (rc = dev_copy(ds.allocs, grid_items, &v.grid_items, h)))
     return rc;
@@ -993,13 +1000,24 @@ static int* g_ntrace = nullptr;
 static int g_tracecap = 0;
 #endif
 
+// One device buffer of the run: CM_ENOMEM when the device has no room (the runtime's error state is
+// cleared, so the context stays usable and a smaller request can follow), CM_ECUDA for other failures.
+static int run_alloc(std::vector<void*>& allocs, void** p, size_t bytes) {
+  const cudaError_t e = cudaMalloc(p, bytes);
+  if (e == cudaErrorMemoryAllocation) {
+    (void)cudaGetLastError();
+    char msg[128];
+    snprintf(msg, sizeof(msg), "device memory exhausted allocating %zu bytes of run buffers", bytes);
+    return fail(CM_ENOMEM, msg);
+  }
+  if (e != cudaSuccess) return fail(CM_ECUDA, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+  allocs.push_back(*p);
+  return 0;
+}
+
 template <typename R>
 static int alloc_wave(std::vector<void*>& allocs, Wave<R>& w, int cap) {
-  auto A = [&](void** p, size_t bytes) -> int {
-    CM_CUDA(cudaMalloc(p, bytes));
-    allocs.push_back(*p);
-    return 0;
-  };
+  auto A = [&](void** p, size_t bytes) -> int { return run_alloc(allocs, p, bytes); };
   int rc = 0;
   size_t n = (size_t)cap;
   if ((rc = A((void**)&w.px, n * 8)) || (rc = A((void**)&w.py, n * 8)) || (rc = A((void**)&w.pz, n * 8)) ||
@@ -1013,19 +1031,37 @@ static int alloc_wave(std::vector<void*>& allocs, Wave<R>& w, int cap) {
   return 0;
 }
 
+// bytes of one electron record (Wave<R>): position 3 x f64, 8 fields of R, 4 int32, the u64 key
+template <typename R> constexpr size_t record_bytes() { return 3 * 8 + 8 * sizeof(R) + 4 * 4 + 8; }
+
 template <typename R>
 static int ensure_buffers(cm_context* ctx, int W, int poolCap) {
   RunBuffers<R>& rb = buffers_of<R>(ctx);
   if (rb.cap == W && rb.poolCap >= poolCap) return 0;
   rb.release();
+  // two waves of kClasses segments, the pool, three queues: refused before any allocation when the
+  // device has not that much free memory (less a reserve for the run's other buffers)
+  const size_t need = ((size_t)2 * kClasses * W + (size_t)poolCap) * record_bytes<R>() + (size_t)3 * W * 4;
+  size_t freeb = 0, totalb = 0;
+  CM_CUDA(cudaMemGetInfo(&freeb, &totalb));
+  if (need + ((size_t)256 << 20) > freeb) {
+    char msg[160];
+    snprintf(msg, sizeof(msg), "a wave of %d electrons needs %.1f GB of run buffers, %.1f GB are free", W,
+             need / 1e9, freeb / 1e9);
+    return fail(CM_ENOMEM, msg);
+  }
   int rc;
   if ((rc = alloc_wave(rb.allocs, rb.w[0], kClasses * W)) || (rc = alloc_wave(rb.allocs, rb.w[1], kClasses * W)) ||
-      (rc = alloc_wave(rb.allocs, rb.pool, poolCap)))
+      (rc = alloc_wave(rb.allocs, rb.pool, poolCap))) {
+    rb.release();  // nothing half-built stays behind: the next run allocates afresh
     return rc;
+  }
   for (int k = 0; k < 3; ++k) {
     void* p;
-    CM_CUDA(cudaMalloc(&p, (size_t)W * 4));
-    rb.allocs.push_back(p);
+    if ((rc = run_alloc(rb.allocs, &p, (size_t)W * 4))) {
+      rb.release();
+      return rc;
+    }
     rb.q[k] = (int*)p;
   }
   rb.cap = W;
@@ -1311,6 +1347,26 @@ template <typename R> __global__ void k_eval_table(SceneView<R> s, int t, int n,
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   out[i] = (double)table_interp(s, t, (R)(x[3 * i] * f0), (R)x[3 * i + 1], (R)x[3 * i + 2], order) / vf;
+}
+
+template <typename R> __global__ void k_eval_locate(SceneView<R> s, int t, int n, const double* x, double f0, int order,
+                                                    double* out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  int w[6];
+  table_windows(s, t, (R)(x[3 * i] * f0), (R)x[3 * i + 1], (R)x[3 * i + 2], order, w);
+  for (int k = 0; k < 6; ++k) out[6 * i + k] = w[k];
+}
+
+template <typename R> __global__ void k_eval_pick(SceneView<R> s, int msm, int n, const double* in, double* out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const Msm& m = s.msms[msm];
+  const R E = (R)(in[2 * i] * kFromSIeV);
+  R cum[kMaxMech];
+  const R total = msm_cumulative_rates(s, m, E, cum);
+  out[2 * i] = total != R(0) ? mech_pick(cum, m.nmech, (R)in[2 * i + 1] * total) : -1;
+  out[2 * i + 1] = (double)total * 1e9;
 }
 
 template <typename R> __global__ void k_eval_tabulated(SceneView<R> s, int mech, int n, const double* in, double* out) {
@@ -1905,6 +1961,7 @@ static int check_desc(cm_context* ctx, const cm_run_desc* d) {
   if (ctx->regions[d->chamber].parent != -1) return fail(CM_EINVAL, "the chamber must be a root region");
   if (d->hist_stride < 3 || d->hist_stride > 1026) return fail(CM_EINVAL, "hist_stride out of range");
   if (!(d->beam_width >= 0)) return fail(CM_EINVAL, "negative beam width");
+  if (d->wave < 0 || d->wave > kMaxWave) return fail(CM_EINVAL, "wave out of range (0 .. 2^27 electrons)");
   return 0;
 }
 
@@ -1998,6 +2055,7 @@ int cm_run(cm_context* ctx, const cm_run_desc* d, uint32_t* back, uint32_t* fwd,
   for (int k = 0; k < 5; ++k) {
     if (!sizes[k]) continue;
     if (cudaMalloc(&dev[k], sizes[k]) != cudaSuccess) {
+      (void)cudaGetLastError();
       for (void* p : bufs) cudaFree(p);
       return fail(CM_ENOMEM, "tally allocation failed");
     }
@@ -2217,6 +2275,32 @@ int cm_eval_table(cm_context* ctx, int table, int n, const double* x, int order,
       k_eval_table<double><<<g, 128>>>(ctx->d64.view, table, n, din, f0, vf, order, dout);
     else
       k_eval_table<float><<<g, 128>>>(ctx->d32.view, table, n, din, f0, vf, order, dout);
+  });
+}
+
+int cm_eval_locate(cm_context* ctx, int table, int n, const double* x, int order, int* out, int precision) {
+  int rc = scene_for(ctx, precision);
+  if (rc) return rc;
+  if (table < 0 || table >= (int)ctx->tables.size()) return fail(CM_EINVAL, "bad table handle");
+  if (!out) return fail(CM_EINVAL, "null output");
+  const double f0 = ctx->tables[table].role >= 1 ? kFromSIeV : 1.0;
+  std::vector<double> w((size_t)std::max(n, 0) * 6);
+  rc = eval_launch(ctx, n, x, 3, w.data(), 6, [&](double* din, double* dout, int g) {
+    if (precision == CM_PREC_FP64) k_eval_locate<double><<<g, 128>>>(ctx->d64.view, table, n, din, f0, order, dout);
+    else k_eval_locate<float><<<g, 128>>>(ctx->d32.view, table, n, din, f0, order, dout);
+  });
+  if (rc) return rc;
+  for (size_t k = 0; k < w.size(); ++k) out[k] = (int)w[k];
+  return 0;
+}
+
+int cm_eval_pick(cm_context* ctx, int msm, int n, const double* in, double* out, int precision) {
+  int rc = scene_for(ctx, precision);
+  if (rc) return rc;
+  if (msm < 0 || msm >= (int)ctx->msms.size()) return fail(CM_EINVAL, "bad material model handle");
+  return eval_launch(ctx, n, in, 2, out, 2, [&](double* din, double* dout, int g) {
+    if (precision == CM_PREC_FP64) k_eval_pick<double><<<g, 128>>>(ctx->d64.view, msm, n, din, dout);
+    else k_eval_pick<float><<<g, 128>>>(ctx->d32.view, msm, n, din, dout);
   });
 }
 
@@ -2480,11 +2564,17 @@ static int run_noalloc(cm_context* ctx, const cm_run_desc* d, uint32_t* back, ui
     CM_CUDA(cudaMemcpyAsync(&hc, c, sizeof(Counters), cudaMemcpyDeviceToHost, s));
     CM_CUDA(cudaStreamSynchronize(s));
     if (hc.error) {
-      status = fail(CM_EOVERFLOW, "cm_run_noalloc: the secondary pool in the fixed scratch overflowed; pass "
-                                  "fewer primaries per call or use cm_run_device");
+      status = hc.error == CM_EOVERFLOW
+                   ? fail(CM_EOVERFLOW, "cm_run_noalloc: the secondary pool in the fixed scratch overflowed; pass "
+                                        "fewer primaries per call or use cm_run_device")
+                   : fail(hc.error, "cm_run_noalloc: the transport kernels reported error " + std::to_string(hc.error));
       break;
     }
     if (hc.done) break;
+    if (ctx->cancel && ctx->cancel->load()) {
+      status = fail(CM_ECANCELED, "cancelled");
+      break;
+    }
     if (it >= maxIt) {
       status = fail(CM_ELIMIT, "cm_run_noalloc: iteration limit reached");
       break;

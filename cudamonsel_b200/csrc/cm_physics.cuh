@@ -178,23 +178,37 @@ template <typename R, typename G> CM_D int elastic_scatter(const SceneView<R>& s
   return el;
 }
 
+// The deflection of GanachaudMokraniPhononInelasticSM::scatter (GanachaudMokraniPhononInelasticSM.cu:19-44)
+// for x = hbar omega / E (with omx = 1 - x, both formed in double) and the deviate r0.  Double: the
+// reference's cos(theta) as written.
+template <typename R> CM_D R phonon_theta(double x, double omx, R r0);
+template <> CM_D double phonon_theta(double x, double, double r0) {
+  double costheta;
+  if (x < 0.1) costheta = 1 + (((x * x) - (pow(16.0, r0) * pow(x, 2.0 - (2.0 * r0)))) / 8.0);
+  else {
+    const double root = sqrt(1.0 - x);
+    const double temp = pow(((-2.0 * (1 + root)) + x) / ((-2.0 * (1 - root)) + x), r0);
+    costheta = temp + (((x - 2.0) * (temp - 1)) / 2.0 / root);
+  }
+  return acos(costheta);
+}
+// Float: the angle in double as well.  Its exponent r0 ln(16/x^2) reaches ~20 for low-loss events, where
+// the rounding of a float argument alone moves the angle by ~1e-6; phonon events are a small share of the
+// steps, so the double evaluation costs little.
+template <> CM_D float phonon_theta(double xd, double omxd, float r0) {
+  return (float)phonon_theta<double>(xd, omxd, (double)r0);
+}
+
 // GanachaudMokraniPhononInelasticSM::scatter (GanachaudMokraniPhononInelasticSM.cu:19-44)
 template <typename R, typename G> CM_D void phonon_scatter(const Mech& k, R d[3], R& E, R& Ep, G& g) {
   const R kE0 = E;
-  const R pe = (R)k.phononE;
-  if (kE0 < pe) return;
-  const R x = pe / kE0;
+  // the threshold and the energy ratio in double, as in phonon_rate
+  if ((double)kE0 < k.phononE) return;
+  const double xd = k.phononE / (double)kE0;
   const R r0 = g.next(), r1 = g.next();
-  R costheta;
-  if (x < R(0.1)) costheta = 1 + (((x * x) - (mpow(R(16), r0) * mpow(x, R(2) - (R(2) * r0)))) / R(8));
-  else {
-    const R root = msqrt(R(1) - x);
-    const R temp = mpow(((R(-2) * (1 + root)) + x) / ((R(-2) * (1 - root)) + x), r0);
-    costheta = temp + (((x - R(2)) * (temp - 1)) / R(2) / root);
-  }
   const R phi = R(2) * R(kPi) * r1;
-  update_dir(d, macos(costheta), phi);
-  E = kE0 - pe;
+  update_dir(d, phonon_theta<R>(xd, ((double)kE0 - k.phononE) / (double)kE0, r0), phi);
+  E = (R)((double)kE0 - k.phononE);
   Ep = kE0;
 }
 

@@ -61,6 +61,7 @@ struct ChildGrid {
 // electrons are kept in one wave segment per material class, so that the
 // threads of a warp mostly run the same material's code
 constexpr int kClasses = 4;
+constexpr int kMaxWave = 1 << 27;  // electrons per wave segment: kClasses x and 8 x (the pool) stay within int
 
 // JoyLuoNieminenCSD (JMONSEL/JoyLuoNieminenCSD.cu:42-121) in eV/nm units
 struct Jln {
@@ -111,7 +112,7 @@ struct Msm {
 struct Mott {
   int Z;
   int off_spwem, off_x1;     // offsets of the cross sections in the table blob (off_x1 unused: -1)
-  int off_x1d;               // offset of the 61 x 201 quantile table in the double copy (mott64)
+  int off_x1d;               // offset of the 61 x 201 quantile table in the double copies (dbl)
   double extrapolateBelowEnergy[4];  // eV
   double sfBrowning[4];
   double mottXSatMin[4];             // table value (units of a0^2) at extrapolateBelowEnergy
@@ -120,12 +121,17 @@ struct Mott {
   double rutherfordAlpha;           // alpha = rutherfordAlpha / E
 };
 
-// NUTableInterpolation (dims 1..3) in the precision blob
+// NUTableInterpolation (dims 1..3) in the precision blob, with double copies in SceneView::dbl of every
+// axis (window selection compares the argument with the reference's abscissae in double in both
+// precisions) and of a 3-D table's values (its reference d3 step extrapolates from the first energy
+// window, which amplifies rounding by orders of magnitude, so FP32 evaluates it in double too)
 struct Table {
   int dim;
   int n[3];
   int off_x[3];
   int off_v;
+  int off_x64[3];            // axes in dbl
+  int off_v64;               // values in dbl (3-D tables), else -1
   double domain[3][2];
   double range[2];
 };
@@ -145,7 +151,8 @@ struct SceneView {
   const int* cell_start;
   const int* grid_items;
   const R* blob;             // table data in compute precision
-  const double* mott64;      // NISTMott quantile tables in double (sampled angles within 1e-6 in FP32 too)
+  const double* dbl;         // double copies: NISTMott quantile tables (sampled angles within 1e-6 in FP32
+                             // too), NU-table axes and 3-D table values
   int chamber;
   int options;               // bit 0: JMONSEL fixes, bit 1: exact CSG in FP32
   int depth;                 // deepest intersection nesting; 0 = every shape is a leaf (plane set or sphere)

@@ -199,6 +199,25 @@ template <typename R, typename Sink> CM_D void cm_trace(const RunView<R>& v, con
 }
 #endif
 
+// MONSEL_MaterialScatterModel::setCache (MONSEL_MaterialScatterModel.cu:44-62): the cumulative scatter rates
+// of the model's mechanisms at E (1/nm) into cum[0..nmech); returns the total
+template <typename R> CM_D R msm_cumulative_rates(const SceneView<R>& s, const Msm& m, R E, R* cum) {
+  R total = 0;
+  const R logE = mlog(E);
+  for (int k = 0; k < m.nmech; ++k) {
+    total += mech_rate(s, s.mechs[m.mech0 + k], E, logE);
+    cum[k] = total;
+  }
+  return total;
+}
+
+// MONSEL_MaterialScatterModel::scatter (:93-134): the first mechanism whose cumulative rate reaches r
+template <typename R> CM_D int mech_pick(const R* cum, int n, R r) {
+  int idx = 0;
+  while (idx < n - 1 && cum[idx] < r) ++idx;
+  return idx;
+}
+
 // ---------------------------------------------------------------- flight
 // MonteCarloSS::takeStep (NISTMonte/MonteCarloSS.cu:107-163) up to the event:
 // region check, MONSEL_MaterialScatterModel::randomMeanPathLength, the
@@ -221,19 +240,14 @@ CM_D int flight_apply(const RunView<R>& v, El<R>& e, Sink& sink, StepCounts& sc,
   {
     Rng<R> g(e.key, e.step, 0);
     R cum[kMaxMech];
-    const R logE = mlog(e.E);
-    for (int k = 0; k < m.nmech; ++k) {
-      total += mech_rate(s, s.mechs[m.mech0 + k], e.E, logE);
-      cum[k] = total;
-    }
+    total = msm_cumulative_rates(s, m, e.E, cum);
     if (total != R(0)) {
       const R f = -mlog(g.next()) / total;
       if ((double)f < fp) fp = (double)f;
       // MONSEL_MaterialScatterModel::scatter (:93-134) picks the mechanism from the rates at the
       // step's starting energy with the stream's next deviate; it is drawn here, before the
       // geometry, so that the rates need not stay live (nothing else draws from this stream)
-      const R r = g.next() * total;
-      while (idx < m.nmech - 1 && cum[idx] < r) ++idx;
+      idx = mech_pick(cum, m.nmech, g.next() * total);
       kind = s.mechs[m.mech0 + idx].kind;
     } else if (e.step > 1000000u) {  // MONSEL_MaterialScatterModel::randomMeanPathLength (:86-90)
       complete = true;

@@ -102,8 +102,60 @@ class SceneSpec:
     def line(self, topz, width, length, thetal, thetar, radl=0.0, radr=0.0):
         return self._op("line", topz, width, length, thetal, thetar, radl, radr)
 
+    def rotate(self, shape, pivot, phi, theta, psi):
+        """ITransform::rotate: Euler angles phi about z, theta about y, psi about z, around pivot."""
+        return self._op("rotate", shape, list(pivot), phi, theta, psi)
+
     def region(self, parent, msm, shape):
         return self._op("region", -1 if parent is None else parent, msm, shape)
+
+    def to_text(self):
+        """The construction calls as text, one per line: the call's name, then its arguments (SI units;
+        a handle is the line number of the call that made it; a list is its length, then its items,
+        except the fixed-size points of sphere/cylinder/translate/rotate and the four tables of
+        tabulated).  Any program that makes the reference's calls can replay it."""
+        out = []
+        for name, args in self.ops:
+            words = [name]
+
+            def put(a, counted=True):
+                if isinstance(a, H):
+                    words.append(str(a.idx))
+                elif isinstance(a, (list, tuple)):
+                    if counted:
+                        words.append(str(len(a)))
+                    for x in a:
+                        put(x)
+                elif isinstance(a, str):
+                    if any(c.isspace() for c in a):
+                        raise ValueError("paths with spaces cannot be written: %r" % a)
+                    words.append(a)
+                elif isinstance(a, (int, np.integer)):
+                    words.append(str(int(a)))
+                else:
+                    words.append(repr(float(a)))
+
+            if name == "material":
+                Z, A, wf, density, workfunction, ecb, bandgap, core = args
+                put(Z)
+                for x in A + wf:
+                    put(x)
+                for x in (density, workfunction, ecb, bandgap):
+                    put(x)
+                put(core)
+            elif name == "planes":
+                normals, points = args
+                put(len(normals) // 3)
+                for x in normals + points:
+                    put(x)
+            elif name in ("sphere", "cylinder", "translate", "rotate", "tabulated"):
+                for a in args:
+                    put(a, counted=False)
+            else:
+                for a in args:
+                    put(a)
+            out.append(" ".join(words))
+        return "\n".join(out) + "\n"
 
 
 def _resolve(a, res):
@@ -200,12 +252,12 @@ class Scene:
         self.h = handles
 
 
-def halfspace(tables=None, material="si", mott_method=1):
+def halfspace(tables=None, material="si", mott_method=1, phonon=False):
     """Flat Si (or PMMA: material="pmma") filling z >= 0 (plane normal (0,0,-1) through the origin), in a
-    0.1 m vacuum chamber."""
+    0.1 m vacuum chamber.  phonon adds GanachaudMokraniPhononInelasticSM to Si as LinesOnLayers.cu:198,205."""
     s = SceneSpec()
     vac = vacuum(s)
-    si = silicon(s, tables, mott_method=mott_method) if material == "si" else pmma(s, mott_method)
+    si = silicon(s, tables, phonon=phonon, mott_method=mott_method) if material == "si" else pmma(s, mott_method)
     sphere = s.sphere([0.0, 0.0, 0.0], 0.1)
     chamber = s.region(None, vac, sphere)
     surf = s.planes([0.0, 0.0, -1.0], [0.0, 0.0, 0.0])
@@ -356,6 +408,40 @@ def features(options=1, tables=None):
             p += pp
     block = s.planes(n, p)
     breg = s.region(chamber, si, block)
+    return Scene(s, chamber, vac=vac, si=si, pmma=pm, si_region=sireg, cylinder=creg, line=lreg, block=breg)
+
+
+def features_ref(tables=None):
+    """A feature scene the reference itself can run: a Si substrate carrying a PMMA cylinder lying along y
+    (radius 30 nm, axis at x = -150 nm, z = -30 nm), a rounded PMMA line (NShapes::createLine at the
+    origin, corner radii 10 nm, 5 deg sidewalls, with the reference's left-corner quirk) and a Si block
+    centred at x = +150 nm.  The run is bug-compatible; only the cylinder is built with its axis
+    normalised (the reference's as-compiled cylinder is never struck; an identity rotate fixes it there)."""
+    s = SceneSpec()
+    vac = vacuum(s)
+    si = silicon(s, tables)
+    pm = pmma(s)
+    chamber = s.region(None, vac, s.sphere([0.0, 0.0, 0.0], 0.1))
+    surf = s.planes([0.0, 0.0, -1.0], [0.0, 0.0, 0.0])
+    sireg = s.region(chamber, si, surf)
+    s.set_options(1)
+    cyl = s.cylinder([-150e-9, -500e-9, -30e-9], [-150e-9, 500e-9, -30e-9], 30e-9)
+    s.set_options(0)
+    creg = s.region(chamber, pm, cyl)
+    th = 5.0 * math.pi / 180.0
+    ln = s.line(-80e-9, 50e-9, 1e-6, th, th, 10e-9, 10e-9)
+    lreg = s.region(chamber, pm, ln)
+    n, p = [], []
+    c, hw = (150e-9, 0.0, -20e-9), 20e-9
+    for a in range(3):
+        for sg in (-1.0, 1.0):
+            nn = [0.0, 0.0, 0.0]
+            pp = list(c)
+            nn[a] = sg
+            pp[a] = c[a] + sg * hw
+            n += nn
+            p += pp
+    breg = s.region(chamber, si, s.planes(n, p))
     return Scene(s, chamber, vac=vac, si=si, pmma=pm, si_region=sireg, cylinder=creg, line=lreg, block=breg)
 
 

@@ -76,3 +76,77 @@ def yield_z(back1, n1, back2, n2, beam_eV, nbins, overdispersion=None):
     vb = od_b * (b1[0] / n1 + b2[0] / n2)
     vs = od_s * (s1[0] / n1 + s2[0] / n2)
     return (b1[0] - b2[0]) / math.sqrt(vb), (s1[0] - s2[0]) / math.sqrt(vs)
+
+
+# ---------------------------------------------------------------- whole-run comparisons
+def family_z_bound(k, sigmas=3.0):
+    """|z| bound per comparison that gives a family of k independent comparisons the false-alarm
+    probability of one two-sided comparison at `sigmas` standard errors (Sidak correction).
+    k = 1 gives `sigmas` itself."""
+    from scipy.stats import norm
+    a = 2.0 * norm.sf(sigmas)
+    ak = 1.0 - (1.0 - a) ** (1.0 / max(int(k), 1))
+    return float(norm.isf(ak / 2.0))
+
+
+def t_to_z(t, dof):
+    """The standard-normal deviate with the same two-sided tail probability as Student's t."""
+    from scipy.stats import norm, t as tdist
+    t = np.asarray(t, dtype=np.float64)
+    p = 2.0 * tdist.sf(np.abs(t), dof)
+    return np.sign(t) * norm.isf(p / 2.0)
+
+
+def pooled_z(a_batches, b_batches):
+    """z of the difference of the means of two sets of equal-size batch values (yields of independent
+    batches of the same number of primaries within each set), from the pooled per-batch variance
+    (equal under the hypothesis that both sides sample the same process), as the normal equivalent
+    of the pooled t statistic.  Returns (z, mean_a, mean_b, standard error of the difference)."""
+    a = np.asarray(a_batches, dtype=np.float64)
+    b = np.asarray(b_batches, dtype=np.float64)
+    na, nb = len(a), len(b)
+    ma, mb = a.mean(), b.mean()
+    ssq = ((a - ma) ** 2).sum() + ((b - mb) ** 2).sum()
+    dof = na + nb - 2
+    var = ssq / dof
+    se = math.sqrt(var * (1.0 / na + 1.0 / nb))
+    if se == 0.0:
+        return 0.0 if ma == mb else math.copysign(float("inf"), ma - mb), ma, mb, se
+    return float(t_to_z((ma - mb) / se, dof)), ma, mb, se
+
+
+def pooled_z_weighted(a_batches, na_prim, b_batches, nb_prim):
+    """pooled_z for batches of different sizes on the two sides: per-primary variance pooled from both
+    (a batch of n primaries has variance sigma1^2 / n)."""
+    a = np.asarray(a_batches, dtype=np.float64)
+    b = np.asarray(b_batches, dtype=np.float64)
+    ma, mb = a.mean(), b.mean()
+    dof = len(a) + len(b) - 2
+    s1 = (((a - ma) ** 2).sum() * na_prim + ((b - mb) ** 2).sum() * nb_prim) / dof
+    se = math.sqrt(s1 * (1.0 / (len(a) * na_prim) + 1.0 / (len(b) * nb_prim)))
+    if se == 0.0:
+        return 0.0 if ma == mb else math.copysign(float("inf"), ma - mb), ma, mb, se
+    return float(t_to_z((ma - mb) / se, dof)), ma, mb, se
+
+
+def chi2_of_z(z):
+    """Sum of squared z over independent comparisons and its chi-squared tail probability."""
+    from scipy.stats import chi2 as chi2dist
+    z = np.asarray(z, dtype=np.float64).ravel()
+    c = float((z * z).sum())
+    return c, len(z), float(chi2dist.sf(c, len(z)))
+
+
+def scan_z(a_batches, na, b_mean, nb):
+    """Per-pixel z of a scan's yields: a_batches[B, npix] are side a's yields from B independent batches of
+    na primaries per pixel, b_mean[npix] side b's yields from nb primaries per pixel.  Each pixel's
+    variance comes from its own B batches (B - 1 degrees of freedom; under the hypothesis that both sides
+    sample the same process it is side b's too), and z is the normal equivalent of the t statistic:
+    a batch yield has variance v, a primary v * na, so the difference of the means has variance
+    v * na * (1 / (B na) + 1 / nb) = v * (1 / B + na / nb)."""
+    a = np.asarray(a_batches, dtype=np.float64)
+    B = a.shape[0]
+    v = a.var(0, ddof=1)
+    se = np.sqrt(v * (1.0 / B + na / float(nb)))
+    t = (a.mean(0) - np.asarray(b_mean, dtype=np.float64)) / np.maximum(se, 1e-300)
+    return t_to_z(t, B - 1)

@@ -67,7 +67,7 @@ int cm_set_options(cm_context* ctx, int options);
  * time), one set per precision.  0 = the built-in default.  Every setting gives the same tallies, because
  * each electron's random stream is keyed by its lineage, so they change only the speed. */
 typedef struct {
-  int wave;                    /* electrons per wave segment (default 2^21) */
+  int wave;                    /* electrons per wave segment (default 2^21; 1024 .. 2^24) */
   int tail_below;              /* k_steps runs the tail once fewer electrons are left (default 262144) */
   int tail_steps;              /* whole steps per thread and launch in the tail (default 32) */
   int blocks_per_sm;           /* grid = SMs x blocks_per_sm blocks of 256 threads (default 8) */
@@ -151,7 +151,9 @@ typedef struct {
   const int* pixel_nbins;      /* [npix], 1..1024 */
   uint64_t seed;
   int hist_stride;             /* >= max(pixel_nbins) + 2 */
-  int wave;                    /* electrons per wave; 0 = the context's cm_tuning.wave, else the default */
+  int wave;                    /* electrons per wave; 0 = the context's cm_tuning.wave, else the default;
+                                  at most 2^27 (CM_EINVAL beyond).  Run buffers that do not fit in the
+                                  device's free memory: CM_ENOMEM, nothing allocated, the context usable. */
   int max_iterations;          /* 0 = default */
   const uint64_t* pixel_key;   /* [npix] random-stream key of each pixel, or NULL: derived from seed and index.
                                   A pixel's result depends only on its key, its beam and primary count,
@@ -290,6 +292,14 @@ int cm_eval_nistmott(cm_context* ctx, int Z, int method, int n, const double* E,
                      int precision);
 /* NUTableInterpolation::interpolate (JMONSEL/NUTableInterpolation.cu:98-115); x[3n] */
 int cm_eval_table(cm_context* ctx, int table, int n, const double* x, int order, double* out, int precision);
+/* The windows that interpolation selects, NULagrangeInterpolation::locate per axis
+ * (JMONSELutils/NULagrangeInterpolation.cu:5-68): out[6n] = (first index, nearest index) for axes 0..2,
+ * -1 for axes the table does not have; x[3n] and order as for cm_eval_table (order applies to 1-D tables). */
+int cm_eval_locate(cm_context* ctx, int table, int n, const double* x, int order, int* out, int precision);
+/* MONSEL_MaterialScatterModel::scatter's choice of mechanism (MONSEL_MaterialScatterModel.cu:93-134):
+ * in[2n] = E (J), deviate u; out[2n] = (index of the mechanism in the order it was added, or -1 when
+ * the model has no rate; total scatter rate in 1/m) */
+int cm_eval_pick(cm_context* ctx, int msm, int n, const double* in, double* out, int precision);
 /* TabulatedInelasticSM::scatterRate + scatter (JMONSEL/TabulatedInelasticSM.cu:209-459);
  * in[9n] = E theta phi u0..u5, out[12n] = rate E' dx dy dz hasSE ESE sdx sdy sdz ndev 0 */
 int cm_eval_tabulated(cm_context* ctx, int msm, int mech, int n, const double* in, double* out, int precision);

@@ -40,7 +40,9 @@ import subprocess
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF = "/root/reference/CudaMONSEL/CudaMONSEL"
+# the reference checkout: $CM_REFERENCE_ROOT, else where this build's container mounts it
+REF_ROOT = os.environ.get("CM_REFERENCE_ROOT", "/root/reference")
+REF = os.path.join(REF_ROOT, "CudaMONSEL", "CudaMONSEL")
 OUT = os.path.join(HERE, "_ref")
 
 COMPAT_H = r"""
@@ -193,7 +195,8 @@ def main():
     ap.add_argument("--work", default=os.environ.get("CM_REF_WORK", "/tmp/cm_ref_build"))
     a = ap.parse_args()
     if not os.path.isdir(REF):
-        print("reference tree not present; nothing to build")
+        print("reference tree not found at %s (set CM_REFERENCE_ROOT to the CudaMONSEL checkout); "
+              "nothing to build" % REF_ROOT)
         return 0
     src = os.path.join(a.work, "src")
     objd = os.path.join(a.work, "obj")

@@ -2126,6 +2126,42 @@ void cmo_eval_freepath(cmo_scene* s, int msm, int n, const double* in, double* o
    }
 }
 
+/* MONSEL_MaterialScatterModel::scatter (MONSEL_MaterialScatterModel.cu:93-134): the mechanism the deviate
+ * picks from the cumulative rates at E; in[2n] = E u, out[2n] = index (-1: no rate), total rate (1/m) */
+void cmo_eval_pick(cmo_scene* s, int msm, int n, const double* in, double* out)
+{
+   const msm_t* m = &s->msms[msm];
+   for (int i = 0; i < n; ++i) {
+      electron e;
+      memset(&e, 0, sizeof(e));
+      e.E = in[2 * i];
+      double cum[MAXMECH];
+      const double total = msm_set_cache(s, m, &e, cum);
+      int index = -1;
+      if (total != 0.) {
+         const double rr = in[2 * i + 1] * total;
+         index = 0;
+         while (cum[index] < rr) index++;
+      }
+      out[2 * i] = index;
+      out[2 * i + 1] = total;
+   }
+}
+
+/* NULagrangeInterpolation::locate (JMONSELutils/NULagrangeInterpolation.cu:5-68) on every axis of a table:
+ * out[6n] = (first, nearest) per axis, -1 for axes the table does not have */
+void cmo_table_locate(cmo_scene* s, int table, int n, const double* x3, int order, int* out)
+{
+   const nu_table* t = &s->tables[table];
+   for (int i = 0; i < n; ++i)
+      for (int k = 0; k < 3; ++k) {
+         int loc[2] = { -1, -1 };
+         if (k < t->dim) cmo_nu_locate(x3[3 * i + k], t->x[k], t->n[k], order, loc);
+         out[6 * i + 2 * k] = loc[0];
+         out[6 * i + 2 * k + 1] = loc[1];
+      }
+}
+
 void cmo_eval_beam(int n, const double* in, double* out)
 {
    for (int i = 0; i < n; ++i) {

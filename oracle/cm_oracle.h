@@ -83,6 +83,8 @@ void cmo_eval_tabulated(cmo_scene* s, int msm, int mech, int n, const double* in
 void cmo_eval_tabulated_stride(cmo_scene* s, int msm, int mech, int n, const double* in, double* out, int stride);
 /* first index of the 4-point window NULagrangeInterpolation::locate picks on a table's first axis */
 int cmo_table_window(cmo_scene* s, int table, double x0);
+void cmo_table_locate(cmo_scene* s, int table, int n, const double* x3, int order, int* out /* [6n] */);
+void cmo_eval_pick(cmo_scene* s, int msm, int n, const double* in /* E u */, double* out /* index total */);
 void cmo_eval_elastic(cmo_scene* s, int msm, int mech, int n, const double* in /* E th ph u0..u3 */,
                       double* out /* rate th ph Z ndev */);
 void cmo_eval_pmma(cmo_scene* s, int msm, int n, const double* in /* E len */, double* out /* csd fittedRate polaronRate */);

@@ -64,6 +64,8 @@ def lib():
         L.cmo_eval_tabulated.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, d, d]
         L.cmo_eval_tabulated_stride.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, d, d, C.c_int]
         L.cmo_table_window.argtypes = [C.c_void_p, C.c_int, C.c_double]
+        L.cmo_table_locate.argtypes = [C.c_void_p, C.c_int, C.c_int, d, C.c_int, i]
+        L.cmo_eval_pick.argtypes = [C.c_void_p, C.c_int, C.c_int, d, d]
         L.cmo_eval_elastic.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, d, d]
         L.cmo_eval_pmma.argtypes = [C.c_void_p, C.c_int, C.c_int, d, d]
         L.cmo_eval_phonon.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, d, d]

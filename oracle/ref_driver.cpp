@@ -8,6 +8,8 @@
 //   ref_driver golden <outdir> <SiTablesDir>
 //   ref_driver run1 <nprim> <seed> <SiTablesDir> [beam_eV]
 //   ref_driver run2 <nprim_per_px> <seed> <SiTablesDir> <x0_nm> <dx_nm> <npix> [beam_eV]
+//   ref_driver scene <scene.txt> <pixels.txt> <seed> <beam_width_m> [angles]
+//     (scene.txt from cudamonsel_b200.scenes.SceneSpec.to_text; pixels.txt rows: x y z [m] E [J] nprim nbins)
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -683,6 +685,266 @@ static int run_scene(bool lines, int nprim, unsigned long long seed, const std::
    return 0;
 }
 
+// ---------------------------------------------------------------- scene replay
+// A scene written by cudamonsel_b200.scenes.SceneSpec.to_text: one construction call per line,
+// arguments in SI units, handles = line numbers of earlier calls.  Every call is made on the
+// reference's own classes as LinesOnLayers.cu:80-282 makes it.  Calls the reference cannot make
+// safely are refused (exit 3): translating or rotating an intersection or union (their casts
+// between ITransform and Shape, NormalIntersectionShape.cu:257-263), and a rounded line built
+// with the JMONSEL fixes on (the reference always has the left-corner quirk of NShapes.cu:140).
+// A line translated before use is assembled at its offset by make_line_at (radius 0 only).
+struct RObj {
+   int kind = -1;  // 0 material 1 msm 2 table 3 shape 4 region
+   SEmaterialT* mat = nullptr;
+   MONSEL_MaterialScatterModelT* msm = nullptr;
+   std::string path;
+   ShapeT* plain = nullptr;     // sphere
+   NormalShapeT* ns = nullptr;  // normal shapes
+   int skind = 0;               // 1 planes 2 cylinder 3 intersection 4 union 5 line (deferred) 6 sphere
+   NormalMultiPlaneShapeT* planes = nullptr;
+   NormalCylindricalShapeT* cyl = nullptr;
+   double line[7] = { 0, 0, 0, 0, 0, 0, 0 }, off[3] = { 0, 0, 0 };
+   bool fixes = false;
+   RegionT* region = nullptr;
+};
+
+[[noreturn]] static void refuse(const char* what)
+{
+   fprintf(stderr, "scene not reproducible by the reference: %s\n", what);
+   exit(3);
+}
+
+// NShapes::createLine (radius 0) with every plane point moved by (dx, dy, dz), as Plane::translate does
+static NormalIntersectionShapeT* make_line_at(const double* a, const double* off)
+{
+   const double topz = a[0], width = a[1], length = a[2], thetal = a[3], thetar = a[4];
+   const double dx = off[0], dy = off[1], dz = off[2];
+   NormalMultiPlaneShapeT* enclosure = new NormalMultiPlaneShapeT();
+   double signz = !topz ? 0 : (topz > 0 ? 1 : -1);
+   if (signz == 0.) signz = 1.;
+   double n0[] = { 0., 0., signz }, p0[] = { 0. + dx, 0. + dy, topz + dz };
+   enclosure->addPlane(*new PlaneT(n0, 3, p0, 3));
+   double n1[] = { 0., 0., -signz }, p1[] = { 0. + dx, 0. + dy, 0. + dz };
+   enclosure->addPlane(*new PlaneT(n1, 3, p1, 3));
+   double n2[] = { 0., 1., 0. }, p2[] = { 0. + dx, length / 2. + dy, 0. + dz };
+   enclosure->addPlane(*new PlaneT(n2, 3, p2, 3));
+   double n3[] = { 0., -1., 0. }, p3[] = { 0. + dx, -length / 2. + dy, 0. + dz };
+   enclosure->addPlane(*new PlaneT(n3, 3, p3, 3));
+   NormalMultiPlaneShapeT* rightNMPS = new NormalMultiPlaneShapeT();
+   double n4[] = { ::cos(thetar), 0., signz * ::sin(thetar) }, p4[] = { width / 2 + dx, 0. + dy, 0. + dz };
+   rightNMPS->addPlane(*new PlaneT(n4, 3, p4, 3));
+   NormalMultiPlaneShapeT* leftNMPS = new NormalMultiPlaneShapeT();
+   double n6[] = { -::cos(thetal), 0., signz * ::sin(thetal) }, p6[] = { -width / 2 + dx, 0. + dy, 0. + dz };
+   leftNMPS->addPlane(*new PlaneT(n6, 3, p6, 3));
+   NormalIntersectionShapeT* nts = new NormalIntersectionShapeT(*leftNMPS, *rightNMPS);
+   return new NormalIntersectionShapeT(*nts, *enclosure);
+}
+
+static NormalShapeT* normal_of(RObj& o)
+{
+   if (o.kind != 3 || o.skind == 6) refuse("a sphere used as a normal shape");
+   if (o.skind == 5 && !o.ns) {
+      const bool moved = o.off[0] != 0 || o.off[1] != 0 || o.off[2] != 0;
+      if (o.line[5] == 0 && o.line[6] == 0) o.ns = make_line_at(o.line, o.off);
+      else if (moved) refuse("a translated rounded line");
+      else if (o.fixes) refuse("a rounded line with the JMONSEL fixes");
+      else o.ns = NShapes::createLine(o.line[0], o.line[1], o.line[2], o.line[3], o.line[4], o.line[5], o.line[6]);
+   }
+   return o.ns;
+}
+
+static int replay_scene(const char* scenefile, const char* pixfile, unsigned long long seed, double width, bool angles)
+{
+   std::ifstream in(scenefile);
+   if (!in) { perror(scenefile); return 2; }
+   std::vector<RObj> ob;
+   std::string ln;
+   int options = 0, chamber = -1;
+   NullMaterialScatterModelT* nullmsm = new NullMaterialScatterModelT();
+   while (std::getline(in, ln)) {
+      std::istringstream s(ln);
+      std::string op;
+      s >> op;
+      RObj o;
+      auto I = [&]() { int v; s >> v; return v; };
+      auto D = [&]() { double v; s >> v; return v; };
+      if (op == "material") {
+         int n = I();
+         std::vector<const ElementT*> el(n);
+         std::vector<double> A(n), wf(n);
+         for (int i = 0; i < n; ++i) el[i] = &Element::byAtomicNumber(I());
+         for (int i = 0; i < n; ++i) A[i] = D();
+         for (int i = 0; i < n; ++i) wf[i] = D();
+         const double density = D(), workfun = D(), ecb = D(), gap = D();
+         const int nc = I();
+         std::vector<double> core(nc);
+         for (int i = 0; i < nc; ++i) core[i] = D();
+         o.kind = 0;
+         if (n == 0) {
+            o.mat = new SEmaterialT();  // vacuum, as LinesOnLayers.cu:80
+         } else {
+            o.mat = new SEmaterialT(el.data(), n, wf.data(), n, density, (char*)"material");
+            o.mat->setWorkfunction(workfun);
+            o.mat->setEnergyCBbottom(ecb);
+            o.mat->setBandgap(gap);
+            if (nc) o.mat->setCoreEnergy(core.data(), nc);
+         }
+      } else if (op == "msm") {
+         SEmaterialT* m = ob[I()].mat;
+         o.kind = 1;
+         o.mat = m;
+         o.msm = new MONSEL_MaterialScatterModelT(m, new ExpQMBarrierSMT(m));
+      } else if (op == "table") {
+         o.kind = 2;
+         s >> o.path;
+      } else if (op == "nistmott") {
+         RObj& m = ob[I()];
+         const int method = I();
+         const RandomizedScatterFactoryT& fac = method == 2 ? NISTMottRS::Factory100
+                                               : method == 3 ? NISTMottRS::Factory100Lin : NISTMottRS::Factory;
+         m.msm->addScatterMechanism(new SelectableElasticSMT(*m.mat, fac));
+      } else if (op == "tabulated") {
+         RObj& m = ob[I()];
+         const int mse = I();
+         const double offset = D();
+         StringT* t = new StringT[4];
+         for (int i = 0; i < 4; ++i) t[i] = ob[I()].path.c_str();
+         m.msm->addScatterMechanism(new TabulatedInelasticSMT(*m.mat, mse, t, offset));
+      } else if (op == "fitted") {
+         RObj& m = ob[I()];
+         const double e = D(), b = D();
+         m.msm->addScatterMechanism(new FittedInelSMT(*m.mat, e, *new JoyLuoNieminenCSDT(*m.mat, b)));
+      } else if (op == "phonon") {
+         RObj& m = ob[I()];
+         const double a = D(), b = D(), c = D(), d = D(), e = D();
+         m.msm->addScatterMechanism(new GanachaudMokraniPhononInelasticSMT(a, b, c, d, e));
+      } else if (op == "polaron") {
+         RObj& m = ob[I()];
+         const double a = D(), b = D();
+         m.msm->addScatterMechanism(new GanachaudMokraniPolaronTrapSMT(a, b));
+      } else if (op == "csd_jln") {
+         RObj& m = ob[I()];
+         m.msm->setCSD(new JoyLuoNieminenCSDT(*m.mat, D()));
+      } else if (op == "min_e") {
+         RObj& m = ob[I()];
+         m.msm->setMinEforTracking(D());
+      } else if (op == "set_options") {
+         options = I();
+      } else if (op == "sphere") {
+         double c[3] = { D(), D(), D() };
+         o.kind = 3;
+         o.skind = 6;
+         o.plain = new SphereT(c, D());
+      } else if (op == "planes") {
+         const int n = I();
+         std::vector<double> nv(3 * n), pv(3 * n);
+         for (auto& x : nv) x = D();
+         for (auto& x : pv) x = D();
+         o.kind = 3;
+         o.skind = 1;
+         o.planes = new NormalMultiPlaneShapeT();
+         for (int i = 0; i < n; ++i) o.planes->addPlane(*new PlaneT(&nv[3 * i], 3, &pv[3 * i], 3));
+         o.ns = (NormalShapeT*)o.planes;
+      } else if (op == "cylinder") {
+         double e0[3] = { D(), D(), D() }, e1[3] = { D(), D(), D() };
+         o.kind = 3;
+         o.skind = 2;
+         o.cyl = new NormalCylindricalShapeT(e0, e1, D());
+         if (options & 1) {  // the axis normalised: an identity rotation recomputes it from the set length
+            const double zero[] = { 0., 0., 0. };
+            o.cyl->rotate(zero, 0., 0., 0.);
+         }
+         o.ns = (NormalShapeT*)o.cyl;
+      } else if (op == "intersection" || op == "union") {
+         NormalShapeT* a = normal_of(ob[I()]);
+         NormalShapeT* b = normal_of(ob[I()]);
+         o.kind = 3;
+         o.skind = op == "union" ? 4 : 3;
+         if (op == "union") o.ns = new NormalUnionShapeT(*a, *b);
+         else o.ns = new NormalIntersectionShapeT(*a, *b);
+      } else if (op == "line") {
+         o.kind = 3;
+         o.skind = 5;
+         for (int i = 0; i < 7; ++i) o.line[i] = D();
+         o.fixes = (options & 1) != 0;
+      } else if (op == "translate") {
+         RObj& t = ob[I()];
+         double d[3] = { D(), D(), D() };
+         if (t.skind == 5 && !t.ns) for (int i = 0; i < 3; ++i) t.off[i] += d[i];
+         else if (t.skind == 1) t.planes->translate(d);
+         else if (t.skind == 2) t.cyl->translate(d);
+         else refuse("translating a composite shape");
+      } else if (op == "rotate") {
+         RObj& t = ob[I()];
+         double pv[3] = { D(), D(), D() };
+         const double phi = D(), th = D(), psi = D();
+         if (t.skind == 1) t.planes->rotate(pv, phi, th, psi);
+         else if (t.skind == 2) t.cyl->rotate(pv, phi, th, psi);
+         else refuse("rotating a composite shape");
+      } else if (op == "region") {
+         const int parent = I(), m = I(), sh = I();
+         o.kind = 4;
+         ShapeT* shape = ob[sh].skind == 6 ? ob[sh].plain : (ShapeT*)normal_of(ob[sh]);
+         if (parent < 0) {  // the chamber: a null model replaced by the vacuum's (LinesOnLayers.cu:80-84)
+            o.region = new RegionT(nullptr, nullmsm, shape);
+            o.region->updateMaterial(*o.region->getScatterModel(), *ob[m].msm);
+            chamber = (int)ob.size();
+         } else {
+            o.region = new RegionT(ob[parent].region, ob[m].msm, shape);
+         }
+      } else if (!op.empty()) {
+         fprintf(stderr, "unknown scene call %s\n", op.c_str());
+         return 2;
+      }
+      ob.push_back(o);
+   }
+   if (options) refuse("a run with the JMONSEL fixes on");
+   if (chamber < 0) { fprintf(stderr, "no chamber\n"); return 2; }
+   std::ifstream pin(pixfile);
+   if (!pin) { perror(pixfile); return 2; }
+   struct Px { double c[3], E; int n, nb; };
+   std::vector<Px> px;
+   Px p;
+   while (pin >> p.c[0] >> p.c[1] >> p.c[2] >> p.E >> p.n >> p.nb) px.push_back(p);
+   g_gen.seed(seed);
+   g_queue.clear();
+   double gunc[] = { 0, 0, -20e-9 };
+   GaussianBeamT eg(width, px.empty() ? ToSI::eV(500.) : px[0].E, gunc);
+   MonteCarloSS::MonteCarloSS monte(&eg, ob[chamber].region, eg.createElectron());
+   ScatterCounter cnt;
+   monte.addActionListener(cnt);
+   auto t0 = std::chrono::steady_clock::now();
+   printf("# scene=%s pixels=%zu seed=%llu width=%g\n", scenefile, px.size(), seed, width);
+   for (const Px& q : px) {
+      eg.setCenter(q.c);
+      eg.setBeamEnergy(q.E);
+      BackscatterStatsT back(monte, q.nb);
+      monte.addActionListener(back);
+      monte.runMultipleTrajectories(q.n);
+      const HistogramT& hist = back.backscatterEnergyHistogram();
+      const HistogramT& fwd = back.forwardscatterEnergyHistogram();
+      printf("pixel %.17g %.17g %.17g %d\nback", q.c[0], q.c[1], q.c[2], q.n);
+      for (int j = -1; j <= hist.binCount(); ++j) printf(" %d", hist.counts(j));
+      printf("\nfwd");
+      for (int j = -1; j <= fwd.binCount(); ++j) printf(" %d", fwd.counts(j));
+      printf("\n");
+      if (angles) {
+         const HistogramT& elev = back.elevationHistogram();
+         const HistogramT& azim = back.azimuthalHistogram();
+         printf("elev");
+         for (int j = -1; j <= elev.binCount(); ++j) printf(" %d", elev.counts(j));
+         printf("\nazim");
+         for (int j = -1; j <= azim.binCount(); ++j) printf(" %d", azim.counts(j));
+         printf("\n");
+      }
+      monte.removeActionListener(back);
+   }
+   auto t1 = std::chrono::steady_clock::now();
+   printf("steps %lld %lld %lld\n", cnt.scatters, cnt.nonscatters, cnt.secondaries);
+   printf("seconds %.6f\n", std::chrono::duration<double>(t1 - t0).count());
+   return 0;
+}
+
 int main(int argc, char** argv)
 {
    if (argc < 2) {
@@ -722,6 +984,10 @@ int main(int argc, char** argv)
    if (mode == "run2" && argc >= 8) {
       double E = argc > 8 ? atof(argv[8]) : 500.0;
       return run_scene(true, atoi(argv[2]), strtoull(argv[3], 0, 10), argv[4], E, atof(argv[5]), atof(argv[6]), atoi(argv[7]));
+   }
+   if (mode == "scene" && argc >= 6) {
+      const bool angles = argc > 6 && std::string(argv[6]) == "angles";
+      return replay_scene(argv[2], argv[3], strtoull(argv[4], 0, 10), atof(argv[5]), angles);
    }
    fprintf(stderr, "bad arguments\n");
    return 2;

@@ -2,8 +2,8 @@
 
 Builds the reference's own CPU code out of tree (oracle/build_ref.py), runs
 oracle/_ref/ref_driver in ``golden`` mode on the synthetic Si tables and
-gzips the text files into tests/golden/.  Needs the reference tree, so it runs
-only where /root/reference exists; the fixtures are committed.
+gzips the text files into tests/golden/.  Needs the reference checkout
+(found by oracle/build_ref.py, $CM_REFERENCE_ROOT); the fixtures are committed.
 
     python tests/golden/make_golden.py
 """

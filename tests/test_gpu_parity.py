@@ -198,13 +198,15 @@ def test_tables(lines_engine, oracle_lines, prec):
         out = e.eval_table(t, x, order, prec)
         r = rel(out, ref)
         if t == 2:
-            # beyond the first energy window the reference extrapolates (d3 quirk) and amplifies rounding
+            # beyond the first energy window the reference extrapolates (d3 quirk) and amplifies the
+            # rounding of its inputs by the Lebesgue constant of the first four energy nodes at E; both
+            # precisions evaluate the 3-D table in double, so the bound holds there too (as a maximum)
             first = theta_window(b, x[:, 0]) == 0
-            print("table %d prec %d first-window max rel %.3g, extrapolated median rel %.3g" % (
-                t, prec, r[first].max(), np.median(r[~first])))
-            assert first.sum() > 20
+            print("table %d prec %d first-window max rel %.3g, extrapolated max rel %.3g over %d" % (
+                t, prec, r[first].max(), r[~first].max(), (~first).sum()))
+            assert first.sum() > 20 and (~first).sum() > 20
             assert r[first].max() < (1e-9 if prec == FP64 else 1e-6)
-            assert np.median(r[~first]) < (1e-6 if prec == FP64 else 5e-2)
+            assert r[~first].max() < 1e-6
         else:
             print("table %d prec %d max rel %.3g" % (t, prec, r.max()))
             assert r.max() < (1e-9 if prec == FP64 else 1e-6)
@@ -244,10 +246,11 @@ def test_tabulated_inelastic(lines_engine, oracle_lines, prec):
     same_dev = out[:, 10] == ref[:, 8]
     print("SE decision agreement %.5f (first window %.5f), deviate count agreement %.5f (first window %.5f)" % (
         same_se.mean(), same_se[first].mean(), same_dev.mean(), same_dev[first].mean()))
-    if prec == FP64:
-        assert same_se.all() and same_dev.all()
-    else:
-        assert same_se[first].mean() > 0.995 and same_dev[first].mean() > 0.995
+    for i in np.where(~(same_se & same_dev))[0][:10]:
+        print("  decision differs: E %.9g eV theta %.9g phi %.9g u %s: engine SE %d deviates %d, oracle %d %d" % (
+            inp[i, 0] * FROMSI, inp[i, 1], inp[i, 2], np.array2string(inp[i, 3:9], precision=9), out[i, 5], out[i, 10],
+            ref[i, 4], ref[i, 8]))
+    assert same_se.all() and same_dev.all()
     ok = same_se & same_dev
     dE0 = inp[:, 0] - ref[:, 1]
     dE1 = inp[:, 0] - out[:, 1]
@@ -303,11 +306,174 @@ def test_elastic(lines_engine, oracle_lines, mat, prec):
     assert r.max() < (1e-9 if prec == FP64 else 1e-6)
     sameZ = out[:, 4] == ref[:, 3]
     print("element agreement %.5f" % sameZ.mean())
-    assert sameZ.all() if prec == FP64 else sameZ.mean() > 0.995
+    if prec == FP64:
+        assert sameZ.all()
+    else:
+        # a float cannot resolve the pick where u * total lies within float rounding of a cumulative
+        # cross section: those cases are where the oracle's own pick changes when u moves by 2e-6
+        lo, hi = inp.copy(), inp.copy()
+        lo[:, 3] *= 1 - 2e-6
+        hi[:, 3] = np.minimum(hi[:, 3] * (1 + 2e-6), 1.0)
+        edge = (oracle_eval(b, "cmo_eval_elastic", (omsm, 0), lo, 5)[:, 3] !=
+                oracle_eval(b, "cmo_eval_elastic", (omsm, 0), hi, 5)[:, 3])
+        for i in np.where(~sameZ)[0]:
+            print("  element differs at E %.9g eV u %.9g (within rounding of a boundary: %s)" % (
+                inp[i, 0] * FROMSI, inp[i, 3], bool(edge[i])))
+        print("element picks within float rounding of a boundary: %d of %d" % (edge.sum(), len(edge)))
+        assert sameZ[~edge].all()
     err = np.abs(out[:, 1:4] - unit(ref[:, 1], ref[:, 2])).max(axis=1)[sameZ]
     print("direction max abs err %.3g, 99.9%% %.3g" % (err.max(), np.quantile(err, 0.999)))
     assert np.quantile(err, 0.999) < (1e-8 if prec == FP64 else 5e-6)
     assert (out[:, 5] == ref[:, 4]).all()
+
+
+def window_inputs(axes):
+    """Arguments on both sides of every abscissa and of every midpoint between neighbours, one and two
+    float spacings away (in the units the FP32 kernels compute in: eV for energies), so that each one
+    has a well-defined window and nearest node in both precisions."""
+    xs = []
+    for a in axes:
+        pts = np.concatenate([a, 0.5 * (a[1:] + a[:-1])])
+        f = pts.astype(np.float32)
+        for k in (1, 2):
+            up, dn = f.copy(), f.copy()
+            for _ in range(k):
+                up = np.nextafter(up, np.float32(np.inf))
+                dn = np.nextafter(dn, np.float32(-np.inf))
+            xs.append(np.concatenate([up, dn]).astype(np.float64))
+    return xs
+
+
+@pytest.mark.parametrize("prec", [FP64, FP32], ids=["fp64", "fp32"])
+def test_table_windows_are_exact(lines_engine, oracle_lines, prec):
+    """NULagrangeInterpolation::locate (JMONSELutils/NULagrangeInterpolation.cu:5-68) on the four Si tables:
+    the window start and nearest node of every axis, identical to the oracle (the reference's locate, pinned
+    bit for bit) for the golden arguments and for arguments one and two float spacings either side of every
+    abscissa and every midpoint (FP32: the float arguments the kernels see, compared on the double axes)."""
+    import ctypes as C
+    import pyoracle as po
+    from cudamonsel_b200 import data
+    e, h = lines_engine
+    b, ho, _ = oracle_lines
+    g = golden("nutable")
+    tables = data.si_tables()
+    total = 0
+    for t in range(4):
+        dim, n, axes, vals = data.read_nu_table(tables[t])
+        ax = [np.asarray(axes[k]) for k in range(dim)]
+        order = int(g[g[:, 0] == t][0, 4])
+        rows = [g[g[:, 0] == t][:, 1:4]]
+        ax_eV = [ax[0] * FROMSI] + ax[1:]  # energies in eV, where the FP32 arguments are floats
+        per_axis = [window_inputs([a]) for a in ax_eV]
+        for k in range(dim):
+            for xk in per_axis[k]:
+                x = np.zeros((len(xk), 3))
+                for j in range(dim):  # the other axes at a fixed interior point
+                    x[:, j] = ax_eV[j][len(ax_eV[j]) // 3]
+                x[:, k] = xk
+                x[:, 0] /= FROMSI  # the energy axis in J, as cm_eval_locate takes it
+                rows.append(x)
+        x = np.ascontiguousarray(np.concatenate(rows))
+        if prec == FP32:
+            x = np.column_stack([f32_energy(x[:, 0]), f32(x[:, 1]), f32(x[:, 2])])
+        got = e.eval_locate(t, x, order, prec)
+        want = np.zeros((len(x), 6), dtype=np.int32)
+        b.L.cmo_table_locate(b.h, t, len(x), po.dp(x), order, want.ctypes.data_as(C.POINTER(C.c_int)))
+        bad = np.where((got != want).any(axis=1))[0]
+        for i in bad[:8]:
+            print("  table %d x %s: engine %s oracle %s" % (t, x[i], got[i], want[i]))
+        print("table %d prec %d: %d arguments, windows identical: %s" % (t, prec, len(x), len(bad) == 0))
+        total += len(x)
+        assert len(bad) == 0
+    assert total > 2000
+
+
+@pytest.mark.parametrize("prec", [FP64, FP32], ids=["fp64", "fp32"])
+@pytest.mark.parametrize("mat", ["si", "pmma"])
+def test_mechanism_pick(lines_engine, oracle_lines, mat, prec):
+    """MONSEL_MaterialScatterModel::scatter's choice of mechanism (MONSEL_MaterialScatterModel.cu:93-134) and
+    the total rate, energies 1 eV - 20 keV and uniform deviates: FP64 identical to the oracle; FP32 (float
+    arguments) identical except where u * total lies within float rounding of a cumulative rate -- the
+    cases where the oracle's own choice changes when u moves by 2e-6 -- which are counted and printed."""
+    e, h = lines_engine
+    b, ho, _ = oracle_lines
+    rng = np.random.default_rng(11)
+    n = 20000
+    E = np.exp(rng.uniform(np.log(1.0), np.log(20000.0), n)) * EV
+    u = rng.random(n)
+    u[:4] = [0.0, 1.0, 0.5, 1e-9]
+    inp = np.column_stack([E, u])
+    if prec == FP32:
+        inp = np.column_stack([f32_energy(E), f32(u)])
+    got = e.eval_pick(h[mat], inp, prec)
+    want = oracle_eval(b, "cmo_eval_pick", (ho[mat],), inp, 2)
+    live = want[:, 1] > 0
+    r = rel(got[live, 1], want[live, 1])
+    print("%s prec %d total rate max rel %.3g" % (mat, prec, r.max()))
+    assert r.max() < (1e-9 if prec == FP64 else 1e-6)
+    same = got[:, 0] == want[:, 0]
+    if prec == FP64:
+        assert same.all()
+        return
+    lo, hi = inp.copy(), inp.copy()
+    lo[:, 1] *= 1 - 2e-6
+    hi[:, 1] = np.minimum(hi[:, 1] * (1 + 2e-6), 1.0)
+    edge = oracle_eval(b, "cmo_eval_pick", (ho[mat],), lo, 2)[:, 0] != oracle_eval(b, "cmo_eval_pick", (ho[mat],),
+                                                                                   hi, 2)[:, 0]
+    for i in np.where(~same)[0][:10]:
+        print("  pick differs at E %.9g eV u %.9g: engine %d oracle %d (within rounding: %s)" % (
+            inp[i, 0] * FROMSI, inp[i, 1], got[i, 0], want[i, 0], bool(edge[i])))
+    print("%s picks within float rounding of a boundary: %d of %d; differing: %d" % (mat, edge.sum(), n,
+                                                                                      (~same).sum()))
+    assert same[~edge].all()
+
+
+@pytest.fixture(scope="module")
+def phonon_si():
+    """Si with GanachaudMokraniPhononInelasticSM (LinesOnLayers.cu:198,205) in an engine and in the oracle."""
+    import pyoracle
+    from cudamonsel_b200 import capi, scenes
+    sc = scenes.halfspace(phonon=True)
+    e = capi.Engine(0)
+    h = scenes.build_engine(sc, e)
+    b, ho = pyoracle.build_oracle(sc)
+    yield e, h, b, ho
+    e.close()
+
+
+@pytest.mark.parametrize("prec", [FP64, FP32], ids=["fp64", "fp32"])
+def test_phonon(phonon_si, prec):
+    """GanachaudMokraniPhononInelasticSM rate and scatter (JMONSEL/GanachaudMokraniPhononInelasticSM.cu:19-72):
+    rate, energy after the event, the step's starting energy, the deflected direction and the number of
+    deviates drawn (0 below the phonon energy, 2 otherwise).  FP64 against the reference's golden vectors:
+    values within 1e-9 relative, directions within 1e-9.  FP32 against the oracle on float-rounded
+    inputs: values within 1e-6 relative, directions within 1e-6."""
+    e, h, b, ho = phonon_si
+    rows = golden("phonon")
+    inp = np.ascontiguousarray(rows[:, 0:5])
+    if prec == FP64:
+        ref = rows[:, 5:11]
+        tol_v, tol_d = 1e-9, 1e-9
+    else:
+        inp = np.column_stack([f32_energy(inp[:, 0]), f32(inp[:, 1:5])])
+        ref = oracle_eval(b, "cmo_eval_phonon", (ho["si"], 2), inp, 6)
+        tol_v, tol_d = 1e-6, 1e-6
+    out = e.eval_phonon(h["si"], 2, inp, prec)
+    # the rate (1/m) is 0 below the phonon energy on both sides
+    assert ((out[:, 0] == 0) == (ref[:, 0] == 0)).all()
+    nz = ref[:, 0] > 0
+    for k, j, name in ((0, 0, "rate"), (1, 1, "E"), (5, 4, "Eprev")):
+        r = rel(out[nz, k], ref[nz, j]) if name == "rate" else rel(out[:, k], ref[:, j])
+        print("phonon %s prec %d max rel %.3g" % (name, prec, r.max()))
+        assert r.max() < tol_v, name
+    d_ref = unit(ref[:, 2], ref[:, 3])
+    dd = np.abs(out[:, 2:5] - d_ref).max(axis=1)
+    print("phonon direction prec %d max abs %.3g" % (prec, dd.max()))
+    assert dd.max() < tol_d
+    # events below the phonon energy change nothing; the others lose exactly one phonon energy
+    below = ref[:, 5] == 0
+    assert below.any() and (~below).any()
+    assert rel(out[below, 1], inp[below, 0]).max() < tol_v
 
 
 @pytest.mark.parametrize("prec", [FP64, FP32])

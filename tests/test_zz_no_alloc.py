@@ -84,3 +84,62 @@ def test_noalloc_rejects_too_many_pixels(setup):
     b, f = tallies(torch, t)
     with pytest.raises(capi.CMError, match="exceeds its maximum of 65536"):
         e.run_noalloc(desc(capi, h, t, FP32), b.data_ptr(), f.data_ptr())
+
+
+def test_noalloc_allocates_nothing(setup):
+    """After a first call (which looks up the scratch array's address), further calls leave the device's
+    free memory exactly where it was: nothing is allocated, not even transiently kept."""
+    torch, capi, scenes, e, h = setup
+    t = inputs(torch, scenes, 32, 80, 500.0, 77)
+    b, f = tallies(torch, t)
+    e.run_noalloc(desc(capi, h, t, FP32), b.data_ptr(), f.data_ptr())
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info(0)
+    for _ in range(2):
+        e.run_noalloc(desc(capi, h, t, FP32), b.data_ptr(), f.data_ptr())
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info(0)
+    assert free1 == free0
+
+
+def test_noalloc_rejects_bad_input_and_missing_scene(setup):
+    """A negative primary count is CM_EINVAL (checked on the device before any transport); a context whose
+    scene was never uploaded for the precision is CM_ESTATE (uploading would allocate)."""
+    torch, capi, scenes, e, h = setup
+    t = inputs(torch, scenes, 8, 10, 500.0, 3)
+    t["nprim"][3] = -1
+    b, f = tallies(torch, t)
+    with pytest.raises(capi.CMError, match="negative primary count") as ei:
+        e.run_noalloc(desc(capi, h, t, FP32), b.data_ptr(), f.data_ptr())
+    assert ei.value.code == capi.EINVAL
+    fresh = capi.Engine(0)
+    try:
+        hf = scenes.build_engine(scenes.lines(), fresh)
+        t = inputs(torch, scenes, 8, 10, 500.0, 3)
+        with pytest.raises(capi.CMError) as ei:
+            fresh.run_noalloc(desc(capi, hf, t, FP64), b.data_ptr(), f.data_ptr())
+        assert ei.value.code == capi.ESTATE
+    finally:
+        fresh.close()
+
+
+def test_noalloc_stops_with_a_status_and_the_scratch_recovers(setup):
+    """A call that hits its iteration limit (desc.max_iterations = 16, far fewer than the run needs) returns
+    CM_ELIMIT with electrons still in the shared scratch; the next call clears what must start at zero and
+    gives cm_run_device's tallies again."""
+    torch, capi, scenes, e, h = setup
+    t = inputs(torch, scenes, 24, 50, 500.0, 4242)
+    b, f = tallies(torch, t)
+    d = desc(capi, h, t, FP32)
+    d.max_iterations = 16
+    with pytest.raises(capi.CMError, match="iteration limit") as ei:
+        e.run_noalloc(d, b.data_ptr(), f.data_ptr())
+    assert ei.value.code == capi.ELIMIT
+    b, f = tallies(torch, t)
+    e.run_device(desc(capi, h, t, FP32), b.data_ptr(), f.data_ptr())
+    torch.cuda.synchronize()
+    want = b.cpu().numpy()
+    b, f = tallies(torch, t)
+    e.run_noalloc(desc(capi, h, t, FP32), b.data_ptr(), f.data_ptr())
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(b.cpu().numpy(), want)
