@@ -124,6 +124,7 @@ template <typename R>
 struct DevScene {
   std::vector<void*> allocs;
   SceneView<R> view;
+  unsigned long long gen = 0;  // counts builds: a cached launch graph holds the view of one build
   bool valid = false;
   bool host = false;  // tables in host memory (only for host-side checks of the device code)
   void release() {
@@ -133,15 +134,38 @@ struct DevScene {
   }
 };
 
+// what a cached launch graph was built for: a graph holds the RunView of these buffers and scene build
+struct LoopKey {
+  unsigned long long scene_gen;
+  int chamber, grid, inel_grid, tail_steps, stage;
+  bool operator==(const LoopKey& o) const {
+    return scene_gen == o.scene_gen && chamber == o.chamber && grid == o.grid && inel_grid == o.inel_grid &&
+           tail_steps == o.tail_steps && stage == o.stage;
+  }
+};
+
 template <typename R>
 struct RunBuffers {
   int cap = 0, poolCap = 0;
   std::vector<void*> allocs;
   Wave<R> w[2], pool;
   int* q[3] = {nullptr, nullptr, nullptr};
+  RunIO* io = nullptr;  // device copy of the run's RunIO
+  // the device-driven transport loop, instantiated once and launched by every run that matches its key
+  cudaGraph_t loop_graph = nullptr;
+  cudaGraphExec_t loop_exec = nullptr;
+  LoopKey loop_key{};
+  void drop_graph() {
+    if (loop_exec) cudaGraphExecDestroy(loop_exec);
+    if (loop_graph) cudaGraphDestroy(loop_graph);
+    loop_exec = nullptr;
+    loop_graph = nullptr;
+  }
   void release() {
+    drop_graph();
     for (void* p : allocs) cudaFree(p);
     allocs.clear();
+    io = nullptr;
     cap = poolCap = 0;
   }
 };
@@ -166,8 +190,12 @@ struct cm_context {
   RunBuffers<float> rb32;
   Counters* counters = nullptr;
   Counters* counters_host = nullptr;
+  RunIO* io_host = nullptr;        // pinned staging of the run's RunIO
   cudaStream_t stream = nullptr;
-  const std::atomic<int>* cancel = nullptr;  // set by a job server: checked between graph launches
+  cudaStream_t cap_stream = nullptr;  // stream the launch graphs are captured on
+  const std::atomic<int>* cancel = nullptr;  // set by a job server for the running job
+  int* cancel_host = nullptr;      // mapped host flag the device loop reads (the server sets it on cancel)
+  const int* cancel_dev = nullptr; // its device address
   cm_tuning tune[2] = {{0, 0, 0, 0, 0.0}, {0, 0, 0, 0, 0.0}};  // launch settings per precision (0: default)
   void dirty() {
     d64.release();
@@ -725,6 +753,7 @@ static int build_scene(cm_context* ctx, DevScene<R>& ds) {
   v.maxMott = 20.0 * kToSIkeV * kFromSIeV;
   v.nstaged = 0;
   v.nstage = nstage;
+  ++ds.gen;
   ds.valid = true;
   return 0;
 }
@@ -994,6 +1023,37 @@ __global__ void k_tail(RunView<R> v, int cur, int steps) {
   if (blockIdx.x == 0 && threadIdx.x == 0) tail_update(v.c, cur, v.W, v.poolCap, steps != 0);
 }
 
+// The device-driven loop: each of its iterations ends with k_loop, which updates the counters as k_tail
+// does and then sets the condition of the conditional node it runs under: another iteration, or not when
+// the run is done or failed (a device error, the iteration limit, a cancel flag set by the host), and for
+// the queue loop also once every primary has started and fewer electrons are left than io.tail_below
+// (the tail loop of whole steps per thread takes over).  Iterations of a loop body after its end do no
+// work: their kernels find no electrons.
+template <typename R>
+__global__ void k_loop(RunView<R> v, int cur, int steps, cudaGraphConditionalHandle h) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  Counters* c = v.c;
+  tail_update(c, cur, v.W, v.poolCap, steps != 0);
+  const RunIO& io = *v.io;
+  c->slots += 1;
+  if (steps) c->tail_slots += 1;
+  if (!c->done && !c->error) {
+    if ((long long)c->slots >= io.max_slots) c->error = CM_ELIMIT;
+    else if (io.cancel && *io.cancel) c->error = CM_ECANCELED;
+  }
+  bool go = !c->done && !c->error;
+  if (go && !steps && !io.queue_only) {
+    const long long left = (long long)c->n[cur ^ 1] + (c->pool < v.poolCap ? c->pool : v.poolCap);
+    if (c->next_primary == c->total_primaries && left < io.tail_below) go = false;
+  }
+  cudaGraphSetConditional(h, go ? 1u : 0u);
+}
+
+// opens a loop of the device-driven run unless the run is already done or failed
+__global__ void k_gate(const Counters* c, cudaGraphConditionalHandle h) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(h, (!c->done && !c->error) ? 1u : 0u);
+}
+
 #ifdef CM_TRACE
 static TraceRec* g_trace = nullptr;
 static int* g_ntrace = nullptr;
@@ -1064,18 +1124,157 @@ static int ensure_buffers(cm_context* ctx, int W, int poolCap) {
     }
     rb.q[k] = (int*)p;
   }
+  if ((rc = run_alloc(rb.allocs, (void**)&rb.io, sizeof(RunIO)))) {
+    rb.release();
+    return rc;
+  }
   rb.cap = W;
   rb.poolCap = poolCap;
   return 0;
 }
 
-// Transport loop.  Inputs are device arrays.
+// iterations of a loop body (an even number: the waves alternate)
+constexpr int kLoopBody = 16;
+
+// the kernels of one transport iteration of the queue loop and of the tail loop, launched on s
+template <typename R>
+static void launch_queue_iteration(const cm_context* ctx, const RunView<R>& v, const RunView<R>& vs, int cur, int grid,
+                                   size_t smem, cudaStream_t s, cudaGraphConditionalHandle* h, cudaEvent_t* ev) {
+  if (CM_STAGE_KERNELS & 1) launch_flight(vs, cur, grid, s, smem);
+  else launch_flight(v, cur, grid, s);
+  if (ev) cudaEventRecordWithFlags(ev[0], s, cudaEventRecordExternal);
+  if (CM_STAGE_KERNELS & 2) k_elastic<R><<<grid, 256, smem, s>>>(vs, cur);
+  else k_elastic<R><<<grid, 256, 0, s>>>(v, cur);
+  if (ev) cudaEventRecordWithFlags(ev[1], s, cudaEventRecordExternal);
+  if (CM_STAGE_KERNELS & 4) k_inelastic<R><<<ctx->nsm * CM_INEL_BLOCKS_PER_SM, 256, smem, s>>>(vs, cur);
+  else k_inelastic<R><<<grid, 256, 0, s>>>(v, cur);
+  if (ev) cudaEventRecordWithFlags(ev[2], s, cudaEventRecordExternal);
+  launch_misc<R>(v, cur, grid, s);
+  if (ev) cudaEventRecordWithFlags(ev[3], s, cudaEventRecordExternal);
+  launch_spawn<R>(v, cur, grid, s);
+  if (ev) cudaEventRecordWithFlags(ev[4], s, cudaEventRecordExternal);
+  if (h) k_loop<R><<<1, 32, 0, s>>>(v, cur, 0, *h);
+  else k_tail<R><<<1, 32, 0, s>>>(v, cur, 0);
+  if (ev) cudaEventRecordWithFlags(ev[5], s, cudaEventRecordExternal);
+}
+
+template <typename R>
+static void launch_tail_iteration(const RunView<R>& v, const RunView<R>& vs, int cur, int grid, int tail_steps,
+                                  size_t smem, cudaStream_t s, cudaGraphConditionalHandle* h, cudaEvent_t* ev) {
+  if (CM_STAGE_KERNELS & 8) launch_steps(vs, cur, grid, tail_steps, s, smem);
+  else launch_steps(v, cur, grid, tail_steps, s, 0);
+  if (ev) cudaEventRecordWithFlags(ev[0], s, cudaEventRecordExternal);
+  launch_spawn<R>(v, cur, grid, s);
+  if (ev) cudaEventRecordWithFlags(ev[1], s, cudaEventRecordExternal);
+  if (h) k_loop<R><<<1, 32, 0, s>>>(v, cur, 1, *h);
+  else k_tail<R><<<1, 32, 0, s>>>(v, cur, 1);
+  if (ev) cudaEventRecordWithFlags(ev[2], s, cudaEventRecordExternal);
+}
+
+// One graph for a whole run: a gate, a WHILE loop of queue iterations, a gate, a WHILE loop of tail
+// iterations (CUDA conditional nodes; k_loop decides on the device whether a loop goes on).  Its kernels
+// read the run's inputs through v.io, so the instantiated graph is kept in the buffers and serves every
+// later run with the same key; the host launches it once per run and reads the counters once.
+template <typename R>
+static int build_loop_graph(cm_context* ctx, RunBuffers<R>& rb, const RunView<R>& v, const RunView<R>& vs, int grid,
+                            size_t smem, int tail_steps) {
+  rb.drop_graph();
+  cudaGraph_t g = nullptr;
+  CM_CUDA(cudaGraphCreate(&g, 0));
+  auto bail = [&](cudaError_t e, const char* what) -> int {
+    cudaGraphDestroy(g);
+    return fail(CM_ECUDA, std::string(what) + ": " + cudaGetErrorString(e));
+  };
+  cudaError_t e;
+  cudaGraphConditionalHandle h[2];
+  for (int k = 0; k < 2; ++k)
+    if ((e = cudaGraphConditionalHandleCreate(&h[k], g, 0, cudaGraphCondAssignDefault)) != cudaSuccess)
+      return bail(e, "cudaGraphConditionalHandleCreate");
+  cudaGraphNode_t prev = nullptr;
+  for (int loop = 0; loop < 2; ++loop) {
+    // the gate kernel, then the WHILE node whose body holds kLoopBody iterations
+    const Counters* cp = v.c;
+    cudaGraphConditionalHandle hh = h[loop];
+    void* args[] = {(void*)&cp, (void*)&hh};
+    cudaKernelNodeParams kp = {};
+    kp.func = (void*)k_gate;
+    kp.gridDim = dim3(1);
+    kp.blockDim = dim3(32);
+    kp.kernelParams = args;
+    cudaGraphNode_t gate, wnode;
+    if ((e = cudaGraphAddKernelNode(&gate, g, prev ? &prev : nullptr, prev ? 1 : 0, &kp)) != cudaSuccess)
+      return bail(e, "cudaGraphAddKernelNode");
+    cudaGraphNodeParams cp2 = {};
+    cp2.type = cudaGraphNodeTypeConditional;
+    cp2.conditional.handle = hh;
+    cp2.conditional.type = cudaGraphCondTypeWhile;
+    cp2.conditional.size = 1;
+    if ((e = cudaGraphAddNode(&wnode, g, &gate, 1, &cp2)) != cudaSuccess) return bail(e, "cudaGraphAddNode");
+    cudaGraph_t body = cp2.conditional.phGraph_out[0];
+    if ((e = cudaStreamBeginCaptureToGraph(ctx->cap_stream, body, nullptr, nullptr, 0,
+                                           cudaStreamCaptureModeThreadLocal)) != cudaSuccess)
+      return bail(e, "cudaStreamBeginCaptureToGraph");
+    for (int it = 0; it < kLoopBody; ++it) {
+      if (loop == 0) launch_queue_iteration<R>(ctx, v, vs, it & 1, grid, smem, ctx->cap_stream, &hh, nullptr);
+      else launch_tail_iteration<R>(v, vs, it & 1, grid, tail_steps, smem, ctx->cap_stream, &hh, nullptr);
+    }
+    cudaGraph_t captured = nullptr;
+    if ((e = cudaStreamEndCapture(ctx->cap_stream, &captured)) != cudaSuccess) return bail(e, "cudaStreamEndCapture");
+    prev = wnode;
+  }
+  cudaGraphExec_t exec = nullptr;
+  if ((e = cudaGraphInstantiate(&exec, g, 0)) != cudaSuccess) return bail(e, "cudaGraphInstantiate");
+  rb.loop_graph = g;
+  rb.loop_exec = exec;
+  return 0;
+}
+
+// the message of a device-side error code of a run
+static int run_error(int err, const Counters& hc) {
+  switch (err) {
+    case CM_ETIMEOUT: return fail(err, "a table copy into shared memory did not complete in time");
+    case CM_EOVERFLOW: return fail(err, "secondary pool overflow; raise the wave size");
+    case CM_ECANCELED: return fail(err, "cancelled");
+    case CM_ELIMIT: {
+      char msg[256];
+      snprintf(msg, sizeof(msg), "iteration limit reached (live %d %d, pool %d, primaries %llu of %llu)", hc.n[0],
+               hc.n[1], hc.pool, hc.next_primary, hc.total_primaries);
+      return fail(err, msg);
+    }
+    default: return fail(err, "the transport kernels reported error " + std::to_string(err));
+  }
+}
+
+// print a few of the electrons still alive after an iteration limit (CM_DEBUG_DUMP set)
+template <typename R> static void dump_live(const RunBuffers<R>& rb, const Counters& hc) {
+  if (!getenv("CM_DEBUG_DUMP")) return;
+  const int cur = hc.n[0] ? 0 : 1;
+  const int k = std::min(8, hc.n[cur]);
+  std::vector<double> px(k), py(k), pz(k);
+  std::vector<R> E(k), dz(k);
+  std::vector<int> reg(k);
+  std::vector<uint32_t> stp(k);
+  cudaMemcpy(px.data(), rb.w[cur].px, k * 8, cudaMemcpyDeviceToHost);
+  cudaMemcpy(py.data(), rb.w[cur].py, k * 8, cudaMemcpyDeviceToHost);
+  cudaMemcpy(pz.data(), rb.w[cur].pz, k * 8, cudaMemcpyDeviceToHost);
+  cudaMemcpy(E.data(), rb.w[cur].E, k * sizeof(R), cudaMemcpyDeviceToHost);
+  cudaMemcpy(dz.data(), rb.w[cur].dz, k * sizeof(R), cudaMemcpyDeviceToHost);
+  cudaMemcpy(reg.data(), rb.w[cur].region, k * 4, cudaMemcpyDeviceToHost);
+  cudaMemcpy(stp.data(), rb.w[cur].step, k * 4, cudaMemcpyDeviceToHost);
+  for (int i = 0; i < k; ++i)
+    fprintf(stderr, "live[%d] pos %g %g %g nm E %g eV dz %g region %d step %u\n", i, px[i], py[i], pz[i], (double)E[i],
+            (double)dz[i], reg[i], stp[i]);
+}
+
+// Transport loop.  Inputs are device arrays.  A run launches the cached device-driven loop graph once; a
+// profiled run (d->profile) replays iterations from the host instead, with CUDA events between the kernels.
 template <typename R>
 static int run_device_once(cm_context* ctx, const cm_run_desc* d, uint32_t* back, uint32_t* fwd, cm_run_stats* st,
                       cudaStream_t stream, const unsigned long long* prefix_dev, const double* e0ref_dev,
                       const unsigned long long* pkey_dev, unsigned long long total) {
   int rc;
-  if ((rc = build_scene<R>(ctx, scene_of<R>(ctx)))) return rc;
+  DevScene<R>& ds = scene_of<R>(ctx);
+  if ((rc = build_scene<R>(ctx, ds))) return rc;
   const cm_tuning tu = resolved_tuning<R>(ctx);
   const int W = d->wave > 0 ? d->wave : tu.wave;
   RunBuffers<R>& rb0 = buffers_of<R>(ctx);
@@ -1088,7 +1287,7 @@ static int run_device_once(cm_context* ctx, const cm_run_desc* d, uint32_t* back
   v.ntrace = g_ntrace;
   v.tracecap = g_tracecap;
 #endif
-  v.s = scene_of<R>(ctx).view;
+  v.s = ds.view;
   v.s.chamber = d->chamber;
   v.w[0] = rb.w[0];
   v.w[1] = rb.w[1];
@@ -1097,21 +1296,30 @@ static int run_device_once(cm_context* ctx, const cm_run_desc* d, uint32_t* back
   v.c = ctx->counters;
   v.W = W;
   v.poolCap = rb.poolCap;
-  v.pc = d->pixel_center;
-  v.pe0 = d->pixel_energy;
-  v.pe0ref = e0ref_dev;
-  v.pnbins = d->pixel_nbins;
-  v.prefix = prefix_dev;
-  v.npix = d->npix;
-  v.width = d->beam_width * 1e9;  // m -> nm
-  v.pkey = pkey_dev;
-  v.back = back;
-  v.fwd = fwd;
-  v.stride = d->hist_stride;
-  v.elev = d->elevation && d->azimuth ? d->elevation : nullptr;
-  v.azim = v.elev ? d->azimuth : nullptr;
-  v.log = d->escape_log && d->escape_log_cap > 0 ? d->escape_log : nullptr;
-  v.logCap = v.log ? d->escape_log_cap : 0;
+  v.io = rb.io;
+  const int maxIt = d->max_iterations > 0 ? d->max_iterations : 500000;
+  RunIO& io = *ctx->io_host;
+  memset(&io, 0, sizeof(io));
+  io.pc = d->pixel_center;
+  io.pe0 = d->pixel_energy;
+  io.pe0ref = e0ref_dev;
+  io.pnbins = d->pixel_nbins;
+  io.prefix = prefix_dev;
+  io.npix = d->npix;
+  io.width = d->beam_width * 1e9;  // m -> nm
+  io.pkey = pkey_dev;
+  io.back = back;
+  io.fwd = fwd;
+  io.stride = d->hist_stride;
+  io.elev = d->elevation && d->azimuth ? d->elevation : nullptr;
+  io.azim = io.elev ? d->azimuth : nullptr;
+  io.log = d->escape_log && d->escape_log_cap > 0 ? d->escape_log : nullptr;
+  io.logCap = io.log ? d->escape_log_cap : 0;
+  io.max_slots = maxIt;
+  io.tail_below = tu.tail_below;
+  io.queue_only = (ctx->options & CM_OPT_QUEUE_STEPS) ? 1 : 0;
+  io.cancel = ctx->cancel ? ctx->cancel_dev : nullptr;
+  CM_CUDA(cudaMemcpyAsync(rb.io, &io, sizeof(RunIO), cudaMemcpyHostToDevice, stream));
 
   Counters c0;
   memset(&c0, 0, sizeof(c0));
@@ -1124,153 +1332,105 @@ static int run_device_once(cm_context* ctx, const cm_run_desc* d, uint32_t* back
   RunView<R> vs = v;
   if (!(ctx->options & CM_OPT_GLOBAL_TABLES)) vs.s.nstaged = v.s.nstage;
   const size_t smem = (size_t)vs.s.nstaged * sizeof(R);
-  const int maxIt = d->max_iterations > 0 ? d->max_iterations : 500000;
   cudaEvent_t e0, e1;
   CM_CUDA(cudaEventCreate(&e0));
   CM_CUDA(cudaEventCreate(&e1));
-  // capture 2*K iterations once, replay until done
-  const int K = 8;
-  cudaGraph_t graph;
-  cudaGraphExec_t exec;
-  // profile: an event before the first kernel and after each kernel of every iteration
-  std::vector<cudaEvent_t> pev;
-  if (d->profile) {
-    pev.resize((size_t)2 * K * 6 + 1);
-    for (auto& ev : pev) CM_CUDA(cudaEventCreate(&ev));
-  }
   double kms[6] = {0, 0, 0, 0, 0, 0};
-  CM_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
-  if (d->profile) cudaEventRecordWithFlags(pev[0], stream, cudaEventRecordExternal);
-  for (int it = 0; it < 2 * K; ++it) {
-    const int cur = it & 1;
-    cudaEvent_t* ev = d->profile ? &pev[(size_t)it * 6 + 1] : nullptr;
-    if (CM_STAGE_KERNELS & 1) launch_flight(vs, cur, grid, stream, smem);
-    else launch_flight(v, cur, grid, stream);
-    if (ev) cudaEventRecordWithFlags(ev[0], stream, cudaEventRecordExternal);
-    if (CM_STAGE_KERNELS & 2) k_elastic<R><<<grid, 256, smem, stream>>>(vs, cur);
-    else k_elastic<R><<<grid, 256, 0, stream>>>(v, cur);
-    if (ev) cudaEventRecordWithFlags(ev[1], stream, cudaEventRecordExternal);
-    if (CM_STAGE_KERNELS & 4) k_inelastic<R><<<ctx->nsm * CM_INEL_BLOCKS_PER_SM, 256, smem, stream>>>(vs, cur);
-    else k_inelastic<R><<<grid, 256, 0, stream>>>(v, cur);
-    if (ev) cudaEventRecordWithFlags(ev[2], stream, cudaEventRecordExternal);
-    launch_misc<R>(v, cur, grid, stream);
-    if (ev) cudaEventRecordWithFlags(ev[3], stream, cudaEventRecordExternal);
-    launch_spawn<R>(v, cur, grid, stream);
-    if (ev) cudaEventRecordWithFlags(ev[4], stream, cudaEventRecordExternal);
-    k_tail<R><<<1, 32, 0, stream>>>(v, cur, 0);
-    if (ev) cudaEventRecordWithFlags(ev[5], stream, cudaEventRecordExternal);
-  }
-  CM_CUDA(cudaStreamEndCapture(stream, &graph));
-  CM_CUDA(cudaGraphInstantiate(&exec, graph, 0));
-  // the tail graph (k_steps, spawn, tail per iteration), captured when first wanted; profiled, with an
-  // event before the first kernel and after each kernel of every iteration
-  cudaGraph_t tgraph = nullptr;
-  cudaGraphExec_t texec = nullptr;
-  bool tail = false;
-  int titers = 0;
-  std::vector<cudaEvent_t> tev;
   double step_ms = 0;
-  CM_CUDA(cudaEventRecord(e0, stream));
-  int iters = 0;
+  long long qslots = 0, tslots = 0;
   int status = 0;
-  for (;;) {
-    CM_CUDA(cudaGraphLaunch(tail ? texec : exec, stream));
-    iters += 2 * K;
-    if (tail) titers += 2 * K;
+  if (!d->profile) {
+    const LoopKey key{ds.gen, d->chamber, grid, ctx->nsm * CM_INEL_BLOCKS_PER_SM, tu.tail_steps, (int)vs.s.nstaged};
+    if (!rb.loop_exec || !(rb.loop_key == key)) {
+      if ((rc = build_loop_graph<R>(ctx, rb, v, vs, grid, smem, tu.tail_steps))) {
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        return rc;
+      }
+      rb.loop_key = key;
+    }
+    CM_CUDA(cudaEventRecord(e0, stream));
+    CM_CUDA(cudaGraphLaunch(rb.loop_exec, stream));
+    CM_CUDA(cudaEventRecord(e1, stream));
     CM_CUDA(cudaMemcpyAsync(ctx->counters_host, ctx->counters, sizeof(Counters), cudaMemcpyDeviceToHost, stream));
     CM_CUDA(cudaStreamSynchronize(stream));
-    if (d->profile && !tail) {
-      for (int it = 0; it < 2 * K; ++it)
-        for (int k = 0; k < 6; ++k) {
-          float t = 0;
-          cudaEventElapsedTime(&t, pev[(size_t)it * 6 + k], pev[(size_t)it * 6 + k + 1]);
-          kms[k] += t;
-        }
-    } else if (d->profile) {
-      for (int it = 0; it < 2 * K; ++it) {
-        float t[3] = {0, 0, 0};
-        for (int k = 0; k < 3; ++k) cudaEventElapsedTime(&t[k], tev[(size_t)it * 3 + k], tev[(size_t)it * 3 + k + 1]);
-        step_ms += t[0];
-        kms[CM_K_SPAWN] += t[1];
-        kms[CM_K_TAIL] += t[2];
+    const Counters& hc = *ctx->counters_host;
+    tslots = (long long)hc.tail_slots;
+    qslots = (long long)hc.slots - tslots;
+    if (hc.error) {
+      status = run_error(hc.error, hc);
+      if (hc.error == CM_ELIMIT) dump_live(rb, hc);
+    }
+  } else {
+    // profiled: the host replays captured iterations (events between the kernels) and reads the
+    // counters after each replay
+    const int K = kLoopBody;
+    std::vector<cudaEvent_t> pev((size_t)K * 6 + 1), tev((size_t)K * 3 + 1);
+    for (auto& ev : pev) CM_CUDA(cudaEventCreate(&ev));
+    for (auto& ev : tev) CM_CUDA(cudaEventCreate(&ev));
+    cudaGraph_t graph[2] = {nullptr, nullptr};
+    cudaGraphExec_t exec[2] = {nullptr, nullptr};
+    for (int loop = 0; loop < 2; ++loop) {
+      CM_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+      std::vector<cudaEvent_t>& ev = loop == 0 ? pev : tev;
+      cudaEventRecordWithFlags(ev[0], stream, cudaEventRecordExternal);
+      for (int it = 0; it < K; ++it) {
+        if (loop == 0) launch_queue_iteration<R>(ctx, v, vs, it & 1, grid, smem, stream, nullptr, &pev[(size_t)it * 6 + 1]);
+        else launch_tail_iteration<R>(v, vs, it & 1, grid, tu.tail_steps, smem, stream, nullptr, &tev[(size_t)it * 3 + 1]);
       }
+      CM_CUDA(cudaStreamEndCapture(stream, &graph[loop]));
+      CM_CUDA(cudaGraphInstantiate(&exec[loop], graph[loop], 0));
     }
-    if (ctx->counters_host->error) {
-      const int err = ctx->counters_host->error;
-      status = err == CM_ETIMEOUT ? fail(err, "a table copy into shared memory did not complete in time")
-                                  : fail(err, "secondary pool overflow; raise the wave size");
-      break;
-    }
-    if (ctx->counters_host->done) break;
-    if (ctx->cancel && ctx->cancel->load()) {
-      status = fail(CM_ECANCELED, "cancelled");
-      break;
-    }
-    {
-      // all primaries started and fewer electrons left (waves and pool) than CM_TAIL_BELOW: tail graph
-      // (unless CM_OPT_QUEUE_STEPS keeps the queue kernels to the end)
+    bool tail = false;
+    CM_CUDA(cudaEventRecord(e0, stream));
+    for (;;) {
+      CM_CUDA(cudaGraphLaunch(exec[tail ? 1 : 0], stream));
+      (tail ? tslots : qslots) += K;
+      CM_CUDA(cudaMemcpyAsync(ctx->counters_host, ctx->counters, sizeof(Counters), cudaMemcpyDeviceToHost, stream));
+      CM_CUDA(cudaStreamSynchronize(stream));
+      for (int it = 0; it < K; ++it) {
+        float ms[6] = {0, 0, 0, 0, 0, 0};
+        if (!tail) {
+          for (int k = 0; k < 6; ++k) cudaEventElapsedTime(&ms[k], pev[(size_t)it * 6 + k], pev[(size_t)it * 6 + k + 1]);
+          for (int k = 0; k < 6; ++k) kms[k] += ms[k];
+        } else {
+          for (int k = 0; k < 3; ++k) cudaEventElapsedTime(&ms[k], tev[(size_t)it * 3 + k], tev[(size_t)it * 3 + k + 1]);
+          step_ms += ms[0];
+          kms[CM_K_SPAWN] += ms[1];
+          kms[CM_K_TAIL] += ms[2];
+        }
+      }
       const Counters& hc = *ctx->counters_host;
+      if (hc.error) {
+        status = run_error(hc.error, hc);
+        break;
+      }
+      if (hc.done) break;
+      if (ctx->cancel && ctx->cancel->load()) {
+        status = fail(CM_ECANCELED, "cancelled");
+        break;
+      }
+      // all primaries started and fewer electrons left (waves and pool) than the tail threshold: the tail
+      // iterations (unless CM_OPT_QUEUE_STEPS keeps the queue kernels to the end)
       const long long left = (long long)hc.n[0] + hc.n[1] + std::min(hc.pool, v.poolCap);
       tail = !(ctx->options & CM_OPT_QUEUE_STEPS) && hc.next_primary == hc.total_primaries && left < tu.tail_below;
-      if (tail && !texec) {
-        if (d->profile) {
-          tev.resize((size_t)2 * K * 3 + 1);
-          for (auto& ev : tev) CM_CUDA(cudaEventCreate(&ev));
-        }
-        CM_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
-        if (d->profile) cudaEventRecordWithFlags(tev[0], stream, cudaEventRecordExternal);
-        for (int it = 0; it < 2 * K; ++it) {
-          const int cur = it & 1;
-          cudaEvent_t* ev = d->profile ? &tev[(size_t)it * 3 + 1] : nullptr;
-          if (CM_STAGE_KERNELS & 8) launch_steps(vs, cur, grid, tu.tail_steps, stream, smem);
-          else launch_steps(v, cur, grid, tu.tail_steps, stream, 0);
-          if (ev) cudaEventRecordWithFlags(ev[0], stream, cudaEventRecordExternal);
-          launch_spawn<R>(v, cur, grid, stream);
-          if (ev) cudaEventRecordWithFlags(ev[1], stream, cudaEventRecordExternal);
-          k_tail<R><<<1, 32, 0, stream>>>(v, cur, 1);
-          if (ev) cudaEventRecordWithFlags(ev[2], stream, cudaEventRecordExternal);
-        }
-        CM_CUDA(cudaStreamEndCapture(stream, &tgraph));
-        CM_CUDA(cudaGraphInstantiate(&texec, tgraph, 0));
+      if (qslots + tslots >= maxIt) {
+        status = run_error(CM_ELIMIT, hc);
+        dump_live(rb, hc);
+        break;
       }
     }
-    if (iters >= maxIt) {
-      const Counters& hc = *ctx->counters_host;
-      char msg[256];
-      snprintf(msg, sizeof(msg), "iteration limit reached (live %d %d, pool %d, primaries %llu of %llu)", hc.n[0],
-               hc.n[1], hc.pool, hc.next_primary, hc.total_primaries);
-      status = fail(CM_ELIMIT, msg);
-      if (getenv("CM_DEBUG_DUMP")) {  // print a few of the electrons still alive
-        const int cur = hc.n[0] ? 0 : 1;
-        const int k = std::min(8, hc.n[cur]);
-        std::vector<double> px(k), py(k), pz(k);
-        std::vector<R> E(k), dz(k);
-        std::vector<int> reg(k);
-        std::vector<uint32_t> stp(k);
-        cudaMemcpy(px.data(), rb.w[cur].px, k * 8, cudaMemcpyDeviceToHost);
-        cudaMemcpy(py.data(), rb.w[cur].py, k * 8, cudaMemcpyDeviceToHost);
-        cudaMemcpy(pz.data(), rb.w[cur].pz, k * 8, cudaMemcpyDeviceToHost);
-        cudaMemcpy(E.data(), rb.w[cur].E, k * sizeof(R), cudaMemcpyDeviceToHost);
-        cudaMemcpy(dz.data(), rb.w[cur].dz, k * sizeof(R), cudaMemcpyDeviceToHost);
-        cudaMemcpy(reg.data(), rb.w[cur].region, k * 4, cudaMemcpyDeviceToHost);
-        cudaMemcpy(stp.data(), rb.w[cur].step, k * 4, cudaMemcpyDeviceToHost);
-        for (int i = 0; i < k; ++i)
-          fprintf(stderr, "live[%d] pos %g %g %g nm E %g eV dz %g region %d step %u\n", i, px[i], py[i], pz[i],
-                  (double)E[i], (double)dz[i], reg[i], stp[i]);
-      }
-      break;
+    CM_CUDA(cudaEventRecord(e1, stream));
+    for (int loop = 0; loop < 2; ++loop) {
+      cudaGraphExecDestroy(exec[loop]);
+      cudaGraphDestroy(graph[loop]);
     }
+    for (auto& ev : pev) cudaEventDestroy(ev);
+    for (auto& ev : tev) cudaEventDestroy(ev);
   }
-  CM_CUDA(cudaEventRecord(e1, stream));
   CM_CUDA(cudaEventSynchronize(e1));
   float ms = 0;
   cudaEventElapsedTime(&ms, e0, e1);
-  cudaGraphExecDestroy(exec);
-  cudaGraphDestroy(graph);
-  if (texec) cudaGraphExecDestroy(texec);
-  if (tgraph) cudaGraphDestroy(tgraph);
-  for (auto& ev : pev) cudaEventDestroy(ev);
-  for (auto& ev : tev) cudaEventDestroy(ev);
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   CM_CUDA(cudaGetLastError());
@@ -1286,10 +1446,10 @@ static int run_device_once(cm_context* ctx, const cm_run_desc* d, uint32_t* back
     st->device_ms = ms;
     for (int k = 0; k < 6; ++k) {
       st->kernel_ms[k] = kms[k];
-      st->kernel_launches[k] = (int64_t)(k < 4 ? iters - titers : iters);
+      st->kernel_launches[k] = (int64_t)(k < 4 ? qslots : qslots + tslots);
     }
     for (int k = 0; k < 4; ++k) st->units[k] = (int64_t)c.units[k];
-    st->step_launches = titers;
+    st->step_launches = tslots;
     st->step_units = (int64_t)c.step_units;
     st->step_ms = step_ms;
   }
@@ -1517,8 +1677,13 @@ int cm_context_create(int device, cm_context** out) {
   CM_CUDA(cudaDeviceGetLimit(&stack, cudaLimitStackSize));
   if (stack < 8192) CM_CUDA(cudaDeviceSetLimit(cudaLimitStackSize, 8192));
   CM_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+  CM_CUDA(cudaStreamCreateWithFlags(&c->cap_stream, cudaStreamNonBlocking));
   CM_CUDA(cudaMalloc(&c->counters, sizeof(Counters)));
   CM_CUDA(cudaMallocHost(&c->counters_host, sizeof(Counters)));
+  CM_CUDA(cudaMallocHost(&c->io_host, sizeof(RunIO)));
+  CM_CUDA(cudaHostAlloc(&c->cancel_host, sizeof(int), cudaHostAllocMapped));
+  *c->cancel_host = 0;
+  CM_CUDA(cudaHostGetDevicePointer((void**)&c->cancel_dev, c->cancel_host, 0));
   *out = c.release();
   return 0;
 }
@@ -1545,7 +1710,10 @@ int cm_context_destroy(cm_context* ctx) {
   ctx->rb32.release();
   cudaFree(ctx->counters);
   cudaFreeHost(ctx->counters_host);
+  cudaFreeHost(ctx->io_host);
+  cudaFreeHost(ctx->cancel_host);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  if (ctx->cap_stream) cudaStreamDestroy(ctx->cap_stream);
   delete ctx;
   return 0;
 }
@@ -2408,8 +2576,22 @@ static void* g_noalloc_addr[kNoAllocMaxDevices];  // device address of g_noalloc
 __global__ void k_noalloc_pixels(int n, int stride, const double* center_m, const double* energy_j, const int* nprim,
                                  const int* nbins, const uint64_t* keys, unsigned long long seedmix, double* pc,
                                  double* pe0, unsigned long long* pkey, unsigned long long* prefix, Counters* c,
-                                 int* bad) {
+                                 int* bad, RunIO* io, double width_nm, uint32_t* back, uint32_t* fwd) {
   __shared__ unsigned long long part[1024];
+  if (threadIdx.x == 0) {  // the run's inputs and tallies as the transport kernels read them
+    memset(io, 0, sizeof(RunIO));
+    io->pc = pc;
+    io->pe0 = pe0;
+    io->pe0ref = pe0;  // BackscatterStats: FromSI::eV(beam energy), the same value
+    io->pnbins = nbins;
+    io->prefix = prefix;
+    io->pkey = pkey;
+    io->npix = n;
+    io->width = width_nm;
+    io->back = back;
+    io->fwd = fwd;
+    io->stride = stride;
+  }
   for (int i = threadIdx.x; i < n; i += blockDim.x) {
     for (int k = 0; k < 3; ++k) pc[3 * i + k] = center_m[3 * i + k] * 1e9;
     pe0[i] = energy_j[i] * kFromSIeVc;
@@ -2479,10 +2661,12 @@ static int run_noalloc(cm_context* ctx, const cm_run_desc* d, uint32_t* back, ui
                            "allocates, so make one cm_run, cm_run_device or cm_eval_* call with this precision "
                            "after the last scene change first");
   const int n = d->npix;
-  // layout: counters | bad flag | pixel tables | wave 0 | wave 1 (kClasses W each) | 3 queues | pool (8 W)
+  // layout: counters | bad flag | run inputs | pixel tables | wave 0 | wave 1 (kClasses W each) | 3 queues |
+  // pool (8 W)
   Carve a{scratch};
   Counters* c = a.take<Counters>(1);
   int* bad = a.take<int>(1);
+  RunIO* io = a.take<RunIO>(1);
   double* pc = a.take<double>(3 * (size_t)n);
   double* pe0 = a.take<double>(n);
   unsigned long long* pkey = a.take<unsigned long long>(n);
@@ -2512,20 +2696,7 @@ static int run_noalloc(cm_context* ctx, const cm_run_desc* d, uint32_t* back, ui
   v.c = c;
   v.W = (int)W;
   v.poolCap = poolCap;
-  v.pc = pc;
-  v.pe0 = pe0;
-  v.pe0ref = pe0;  // BackscatterStats: FromSI::eV(beam energy), the same value
-  v.pnbins = d->pixel_nbins;
-  v.prefix = prefix;
-  v.pkey = pkey;
-  v.npix = n;
-  v.width = d->beam_width * 1e9;  // m -> nm
-  v.back = back;
-  v.fwd = fwd;
-  v.stride = d->hist_stride;
-  v.elev = v.azim = nullptr;  // not taken here (no room in the fixed scratch)
-  v.log = nullptr;
-  v.logCap = 0;
+  v.io = io;  // written by k_noalloc_pixels (no angle histograms or escape log: no room in the fixed scratch)
   // the array keeps the previous call's contents: the counters, the bad-input
   // flag and the caller's tallies start at zero; waves, queues and pool are
   // only read below the counts, so they need no clearing
@@ -2536,7 +2707,7 @@ static int run_noalloc(cm_context* ctx, const cm_run_desc* d, uint32_t* back, ui
   CM_CUDA(cudaMemsetAsync(fwd, 0, hbytes, s));
   k_noalloc_pixels<<<1, 1024, 0, s>>>(n, d->hist_stride, d->pixel_center, d->pixel_energy, d->pixel_nprim,
                                       d->pixel_nbins, d->pixel_key, mix64(d->seed ^ 0x243F6A8885A308D3ULL), pc, pe0,
-                                      pkey, prefix, c, bad);
+                                      pkey, prefix, c, bad, io, d->beam_width * 1e9, back, fwd);
   CM_CUDA(cudaGetLastError());
   int hbad = 0;
   CM_CUDA(cudaMemcpyAsync(&hbad, bad, sizeof(int), cudaMemcpyDeviceToHost, s));

@@ -9,8 +9,9 @@
 // tallies depend only on its scene, its pixels and their stream keys, so a job
 // gives the same result alone and in any mix.
 //
-// Each slot is driven by one host thread: the transport loop of a context
-// synchronises with its own stream between graph launches only.
+// Each slot is driven by one host thread: a run launches its context's cached
+// loop graph on the slot's stream once and waits for it; cancelling a running
+// job sets a flag in mapped host memory that the loop reads every iteration.
 #pragma once
 
 #include <chrono>
@@ -44,7 +45,14 @@ struct JobRecord {
   cm_run_stats stats;
   double t_submit = 0, t_start = 0, t_end = 0;
   std::atomic<int> cancel{0};
+  int* running_cancel = nullptr;  // while the job runs: its slot context's mapped cancel flag (the device loop reads it)
 };
+
+// ask a job to stop: the host flag, and for a running job the flag its device loop reads (server lock held)
+static void request_cancel(JobRecord* j) {
+  j->cancel.store(1);
+  if (j->running_cancel) *(volatile int*)j->running_cancel = 1;
+}
 
 // device buffers of one slot, grown to the largest job it has run
 struct SlotBuffers {
@@ -173,6 +181,8 @@ static void slot_worker(cm_server* srv, int slot) {
       srv->in_use += job->footprint;
       job->state = CM_JOB_RUNNING;
       job->t_start = srv->now();
+      *(volatile int*)ctx->cancel_host = job->cancel.load();
+      job->running_cancel = ctx->cancel_host;
     }
     srv->cv_work.notify_all();
     // the slot takes the job's scene; the device copy is rebuilt on the first run
@@ -190,6 +200,7 @@ static void slot_worker(cm_server* srv, int slot) {
     ctx->cancel = nullptr;
     {
       std::lock_guard<std::mutex> lk(srv->mu);
+      job->running_cancel = nullptr;
       srv->in_use -= job->footprint;
       job->t_end = srv->now();
       job->error = rc;
@@ -240,7 +251,7 @@ int cm_server_destroy(cm_server* srv) {
   if (!srv) return 0;
   {
     std::lock_guard<std::mutex> lk(srv->mu);
-    for (auto& kv : srv->jobs) kv.second->cancel.store(1);  // running jobs stop at their next graph boundary
+    for (auto& kv : srv->jobs) request_cancel(kv.second.get());  // running jobs stop at their next iteration
     srv->stop = true;
   }
   srv->cv_work.notify_all();
@@ -337,7 +348,7 @@ int cm_job_cancel(cm_server* srv, int job) {
       j->error = CM_ECANCELED;
       j->t_end = srv->now();
     } else if (j->state == CM_JOB_RUNNING) {
-      j->cancel.store(1);
+      request_cancel(j);
     }
   }
   srv->cv_done.notify_all();

@@ -36,6 +36,7 @@ struct Counters {
   unsigned long long units[4];
   unsigned long long step_units;  // electrons the several-steps kernel started with
   unsigned long long logged;      // escapes offered to the escape log
+  unsigned long long slots, tail_slots;  // iteration slots the device-driven loop ran (all, tail)
 };
 
 template <typename R>
@@ -105,19 +106,10 @@ struct TraceRec {
 };
 #endif
 
-template <typename R>
-struct RunView {
-#ifdef CM_TRACE
-  TraceRec* trace;
-  int* ntrace;
-  int tracecap;
-#endif
-  SceneView<R> s;
-  Wave<R> w[2];
-  Wave<R> pool;
-  int* q[3];
-  Counters* c;
-  int W, poolCap;
+// What changes from run to run: the pixels, the tallies and the loop's limits.  It sits in device memory
+// (written before each run) and the kernels read it through RunView::io, so the launch graph of a run
+// does not depend on it and an instantiated graph serves every run of the same scene and buffers.
+struct RunIO {
   const double* pc;      // pixel centres, nm
   const double* pe0;     // beam energy, eV
   const double* pe0ref;  // histogram top edge in eV as the reference computes it
@@ -131,6 +123,28 @@ struct RunView {
   uint32_t *elev, *azim;       // per-pixel angle histograms (182 and 362 counts), or null
   cm_escape_record* log;       // escape log, or null
   long long logCap;
+  // the device-driven loop (k_loop): iteration slots allowed, the tail threshold, queue kernels only to
+  // the end, and a flag in host memory that cancels the run (null: not cancellable)
+  long long max_slots;
+  int tail_below;
+  int queue_only;
+  const volatile int* cancel;
+};
+
+template <typename R>
+struct RunView {
+#ifdef CM_TRACE
+  TraceRec* trace;
+  int* ntrace;
+  int tracecap;
+#endif
+  SceneView<R> s;
+  Wave<R> w[2];
+  Wave<R> pool;
+  int* q[3];
+  Counters* c;
+  int W, poolCap;
+  const RunIO* io;
 };
 
 // per-thread event counts, reduced once per warp by the kernels
@@ -157,22 +171,23 @@ CM_D int hist_bin(double max, int nbins, double val) {
 // BackscatterStats::actionPerformed for a BackscatterEvent (NISTMonte/BackscatterStats.cu:147-170):
 // elevation and azimuth histograms, the log, then the forward or back energy histogram
 template <typename R, typename Sink> CM_D void tally_escape(const RunView<R>& v, const El<R>& e, Sink& sink) {
+  const RunIO& io = *v.io;
   const int px = e.pixel;
-  const double E0ref = v.pe0ref[px];
+  const double E0ref = io.pe0ref[px];
   double val = (double)e.E;
-  if (e.E == (R)v.pe0[px]) val = E0ref;  // electrons that never lost energy carry E0 exactly, as in the reference
+  if (e.E == (R)io.pe0[px]) val = E0ref;  // electrons that never lost energy carry E0 exactly, as in the reference
   const double elevation = (kPi / 2) - atan2(e.p[2], sqrt((e.p[0] * e.p[0]) + (e.p[1] * e.p[1])));
-  if (v.elev) {
+  if (io.elev) {
     double azimuth = atan2(e.p[1], e.p[0]);
     if (azimuth < 0.0) azimuth = (2.0 * kPi) + azimuth;
     const int be = hist_bin(kPi, 180, elevation) + 1, ba = hist_bin(2.0 * kPi, 360, azimuth) + 1;
-    if (be <= 181) sink.count(v.elev + (size_t)px * 182 + be);  // past the overflow slot: never counted
-    if (ba <= 361) sink.count(v.azim + (size_t)px * 362 + ba);
+    if (be <= 181) sink.count(io.elev + (size_t)px * 182 + be);  // past the overflow slot: never counted
+    if (ba <= 361) sink.count(io.azim + (size_t)px * 362 + ba);
   }
-  if (v.log) {
+  if (io.log) {
     const unsigned long long k = sink.ticket(&v.c->logged);
-    if (k < (unsigned long long)v.logCap) {
-      cm_escape_record& r = v.log[k];
+    if (k < (unsigned long long)io.logCap) {
+      cm_escape_record& r = io.log[k];
       r.electron = e.key;
       r.pixel = px;
       r.step = (int)e.step;
@@ -182,11 +197,11 @@ template <typename R, typename Sink> CM_D void tally_escape(const RunView<R>& v,
       r.phi = atan2((double)e.d[1], (double)e.d[0]);
     }
   }
-  const int nb = v.pnbins[px];
+  const int nb = io.pnbins[px];
   const int b = hist_bin(E0ref, nb, val) + 1;
   if (b > nb + 1) return;  // past the overflow slot: the reference writes out of bounds and never counts it
-  uint32_t* h = elevation < (kPi / 2.0) ? v.fwd : v.back;
-  sink.count(h + (size_t)px * v.stride + b);
+  uint32_t* h = elevation < (kPi / 2.0) ? io.fwd : io.back;
+  sink.count(h + (size_t)px * io.stride + b);
 }
 
 #ifdef CM_TRACE
@@ -501,26 +516,27 @@ CM_D void spawn_one(const RunView<R>& v, int nxt, int j, int take_se, int poolTo
     return;
   }
   // GaussianBeam::createElectron (NISTMonte/GaussianBeam.cu:52-65) + initializeTrajectory (MonteCarloSS.cu:99-105)
+  const RunIO& io = *v.io;
   const unsigned long long gi = first + (unsigned long long)(j - take_se);
-  int lo = 0, hi = v.npix;
+  int lo = 0, hi = io.npix;
   while (hi - lo > 1) {
     const int mid = (lo + hi) >> 1;
-    if (v.prefix[mid] <= gi) lo = mid;
+    if (io.prefix[mid] <= gi) lo = mid;
     else hi = mid;
   }
   const int px = lo;
-  const unsigned long long k = gi - v.prefix[px];
+  const unsigned long long k = gi - io.prefix[px];
   El<R> e;
-  e.key = mix64(v.pkey[px] + mix64(k + 1));
+  e.key = mix64(io.pkey[px] + mix64(k + 1));
   Rng<R> g(e.key, 0xFFFFFFFFu, 0);
   const double u1 = (double)g.next(), u2 = (double)g.next();
-  const double r = sqrt(-2. * log(u1)) * v.width;
+  const double r = sqrt(-2. * log(u1)) * io.width;
   const double th = 2.0 * kPi * u2;
-  e.p[0] = v.pc[3 * px] + r * cos(th);
-  e.p[1] = v.pc[3 * px + 1] + r * sin(th);
-  e.p[2] = v.pc[3 * px + 2];
+  e.p[0] = io.pc[3 * px] + r * cos(th);
+  e.p[1] = io.pc[3 * px + 1] + r * sin(th);
+  e.p[2] = io.pc[3 * px + 2];
   e.d[0] = 0; e.d[1] = 0; e.d[2] = 1;
-  e.E = (R)v.pe0[px];
+  e.E = (R)io.pe0[px];
   e.Ep = e.E;
   e.region = containing_subregion<R, D>(v.s, v.s.chamber, e.p);
   e.pixel = px;

@@ -544,3 +544,32 @@ def test_oversized_wave_is_enomem_and_the_context_stays_usable(half):
     assert ei.value.code == capi.EINVAL
     back, fwd, st = e.run(h["chamber"], c, scenes.eV(1000.0), 10, 100, 0.0, 1, precision=FP64)
     assert st.primaries == 10 and back.sum() > 0
+
+
+@pytest.mark.parametrize("prec", [FP64, FP32], ids=["fp64", "fp32"])
+def test_device_loop_limit_and_graph_reuse(half, prec):
+    """The device-driven loop (one launch per run of a graph cached in the context): an iteration limit stops
+    the run on the device with CM_ELIMIT; the following runs reuse the cached graph and give identical
+    tallies and counts run after run, equal to a fresh context's and to a profiled run's (the host replays
+    iterations there)."""
+    from cudamonsel_b200 import capi, scenes
+    e, h = half
+    c = np.tile([0.0, 0.0, -20e-9], (16, 1))
+    with pytest.raises(capi.CMError, match="iteration limit") as ei:
+        e.run(h["chamber"], c, scenes.eV(1000.0), 200, 100, 0.0, 3, precision=prec, max_iterations=16)
+    assert ei.value.code == capi.ELIMIT
+    runs = [e.run(h["chamber"], c, scenes.eV(1000.0), 200, 100, 0.0, 3, precision=prec) for _ in range(3)]
+    runs.append(e.run(h["chamber"], c, scenes.eV(1000.0), 200, 100, 0.0, 3, precision=prec, profile=1))
+    fresh = capi.Engine(0)
+    hf = scenes.build_engine(scenes.halfspace(), fresh)
+    runs.append(fresh.run(hf["chamber"], c, scenes.eV(1000.0), 200, 100, 0.0, 3, precision=prec))
+    fresh.close()
+    b0, f0, s0 = runs[0]
+    print("iterations %d, queue launches %d, tail launches %d; device ms %s" % (
+        s0.iterations, s0.kernel_launches[0], s0.step_launches, [round(r[2].device_ms, 2) for r in runs]))
+    assert s0.primaries == 16 * 200
+    for k, (b, f, s) in enumerate(runs[1:], start=1):
+        assert np.array_equal(b, b0) and np.array_equal(f, f0)
+        assert s.steps == s0.steps and s.secondaries == s0.secondaries
+        if k != 3:  # the profiled run switches to the tail at a replay boundary: other iteration counts
+            assert s.iterations == s0.iterations
