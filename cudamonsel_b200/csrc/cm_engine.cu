@@ -850,11 +850,11 @@ template <typename R, int D> __device__ __forceinline__ void flight_loop(const R
   StepCounts sc;
   const int n = v.c->n[cur];
   if ((int)(blockIdx.x * blockDim.x) >= n || !stage_tables(v)) return;  // blocks without work stage nothing
-  int cnt[kClasses];
-  for (int k = 0; k < kClasses; ++k) cnt[k] = v.c->nc[cur][k];
+  int cnt[kSegments];
+  for (int k = 0; k < kSegments; ++k) cnt[k] = v.c->nc[cur][k];
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     int k = 0, j = i;  // i-th electron over the class segments in order
-    while (k < kClasses - 1 && j >= cnt[k]) j -= cnt[k++];
+    while (k < kSegments - 1 && j >= cnt[k]) j -= cnt[k++];
     flight_one<R, D>(v, cur, k * v.W + j, sink, sc);
   }
   flush_counts(v.c, sc);
@@ -967,11 +967,11 @@ template <typename R, int D> __global__ void CM_LB_STEPS k_steps(RunView<R> v, i
   StepCounts sc;
   const int n = v.c->n[cur];
   if ((int)(blockIdx.x * blockDim.x) >= n || !stage_tables(v)) return;
-  int cnt[kClasses];
-  for (int k = 0; k < kClasses; ++k) cnt[k] = v.c->nc[cur][k];
+  int cnt[kSegments];
+  for (int k = 0; k < kSegments; ++k) cnt[k] = v.c->nc[cur][k];
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     int k = 0, j = i;
-    while (k < kClasses - 1 && j >= cnt[k]) j -= cnt[k++];
+    while (k < kSegments - 1 && j >= cnt[k]) j -= cnt[k++];
     steps_one<R, D>(v, cur, k * v.W + j, nsteps, sink, sc);
   }
   flush_counts(v.c, sc);
@@ -1099,9 +1099,9 @@ static int ensure_buffers(cm_context* ctx, int W, int poolCap) {
   RunBuffers<R>& rb = buffers_of<R>(ctx);
   if (rb.cap == W && rb.poolCap >= poolCap) return 0;
   rb.release();
-  // two waves of kClasses segments, the pool, three queues: refused before any allocation when the
+  // two waves of kSegments segments, the pool, three queues: refused before any allocation when the
   // device has not that much free memory (less a reserve for the run's other buffers)
-  const size_t need = ((size_t)2 * kClasses * W + (size_t)poolCap) * record_bytes<R>() + (size_t)3 * W * 4;
+  const size_t need = ((size_t)2 * kSegments * W + (size_t)poolCap) * record_bytes<R>() + (size_t)3 * W * 4;
   size_t freeb = 0, totalb = 0;
   CM_CUDA(cudaMemGetInfo(&freeb, &totalb));
   if (need + ((size_t)256 << 20) > freeb) {
@@ -1111,7 +1111,7 @@ static int ensure_buffers(cm_context* ctx, int W, int poolCap) {
     return fail(CM_ENOMEM, msg);
   }
   int rc;
-  if ((rc = alloc_wave(rb.allocs, rb.w[0], kClasses * W)) || (rc = alloc_wave(rb.allocs, rb.w[1], kClasses * W)) ||
+  if ((rc = alloc_wave(rb.allocs, rb.w[0], kSegments * W)) || (rc = alloc_wave(rb.allocs, rb.w[1], kSegments * W)) ||
       (rc = alloc_wave(rb.allocs, rb.pool, poolCap))) {
     rb.release();  // nothing half-built stays behind: the next run allocates afresh
     return rc;
@@ -2661,7 +2661,7 @@ static int run_noalloc(cm_context* ctx, const cm_run_desc* d, uint32_t* back, ui
                            "allocates, so make one cm_run, cm_run_device or cm_eval_* call with this precision "
                            "after the last scene change first");
   const int n = d->npix;
-  // layout: counters | bad flag | run inputs | pixel tables | wave 0 | wave 1 (kClasses W each) | 3 queues |
+  // layout: counters | bad flag | run inputs | pixel tables | wave 0 | wave 1 (kSegments W each) | 3 queues |
   // pool (8 W)
   Carve a{scratch};
   Counters* c = a.take<Counters>(1);
@@ -2676,7 +2676,7 @@ static int run_noalloc(cm_context* ctx, const cm_run_desc* d, uint32_t* back, ui
   const size_t rec = 3 * 8 + 8 * sizeof(R) + 4 * 4 + 8;
   const size_t pad = (3 * 16 + 3) * 256;  // worst-case rounding of the 51 pieces below
   const size_t left = kNoAllocScratchBytes - a.off;
-  long long W = (long long)((left > pad ? left - pad : 0) / ((2 * kClasses + 8) * rec + 3 * 4));
+  long long W = (long long)((left > pad ? left - pad : 0) / ((2 * kSegments + 8) * rec + 3 * 4));
   if (d->wave > 0 && d->wave < W) W = d->wave;
   if (W < 1024) return fail(CM_EINVAL, "cm_run_noalloc: no room for a wave of 1024 electrons");
   const int poolCap = (int)(8 * W);
@@ -2688,8 +2688,8 @@ static int run_noalloc(cm_context* ctx, const cm_run_desc* d, uint32_t* back, ui
 #endif
   v.s = ds.view;
   v.s.chamber = d->chamber;
-  carve_wave(a, v.w[0], kClasses * (int)W);
-  carve_wave(a, v.w[1], kClasses * (int)W);
+  carve_wave(a, v.w[0], kSegments * (int)W);
+  carve_wave(a, v.w[1], kSegments * (int)W);
   for (int k = 0; k < 3; ++k) v.q[k] = a.take<int>(W);
   carve_wave(a, v.pool, poolCap);
   if (a.off > kNoAllocScratchBytes) return fail(CM_EINVAL, "cm_run_noalloc: scratch layout does not fit");

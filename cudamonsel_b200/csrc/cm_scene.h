@@ -61,7 +61,12 @@ struct ChildGrid {
 // electrons are kept in one wave segment per material class, so that the
 // threads of a warp mostly run the same material's code
 constexpr int kClasses = 4;
-constexpr int kMaxWave = 1 << 27;  // electrons per wave segment: kClasses x and 8 x (the pool) stay within int
+// a wave has two segments per class: electrons at or above kSegmentSplitEv and below it (the low band
+// takes the Browning branch of the elastic cross sections and the low-energy secondary paths), so that
+// a warp's threads mostly run the same branches
+constexpr int kSegments = 2 * kClasses;
+constexpr double kSegmentSplitEv = 50.0;
+constexpr int kMaxWave = 1 << 27;  // electrons per wave segment: kSegments x and 8 x (the pool) stay within int
 
 // JoyLuoNieminenCSD (JMONSEL/JoyLuoNieminenCSD.cu:42-121) in eV/nm units
 struct Jln {

@@ -24,8 +24,8 @@ struct Wave {
 
 struct Counters {
   int n[2];              // electrons in each wave
-  int nc[2][kClasses];   // of which in each class segment (segment k holds slots [k W, k W + nc))
-  int ns[kClasses];      // electrons the refill appends after the survivors of each segment
+  int nc[2][kSegments];  // of which in each segment (segment k holds slots [k W, k W + nc))
+  int ns[kSegments];     // electrons the refill appends after the survivors of each segment
   int pool;
   int q[3];
   int error;
@@ -353,9 +353,15 @@ CM_D void flight_one(const RunView<R>& v, int cur, int i, Sink& sink, StepCounts
   v.q[queue][slot] = i;
 }
 
-// append a surviving electron to its class segment of the next wave
+// wave segment of an electron in `region` at energy E: its material's class, split at kSegmentSplitEv
+template <typename R> CM_D int wave_segment(const SceneView<R>& s, int region, R E) {
+  const int cls = region >= 0 ? s.regions[region].cls : 0;
+  return 2 * cls + (E < (R)kSegmentSplitEv ? 1 : 0);
+}
+
+// append a surviving electron to its segment of the next wave
 template <typename R, typename Sink> CM_D void keep(const RunView<R>& v, int nxt, const El<R>& e, Sink& sink) {
-  const int k = v.s.regions[e.region].cls;
+  const int k = wave_segment(v.s, e.region, e.E);
   const int slot = sink.append_q(v.c->nc[nxt], k);
   store_live(v.w[nxt], k * v.W + slot, e);
 }
@@ -363,7 +369,7 @@ template <typename R, typename Sink> CM_D void keep(const RunView<R>& v, int nxt
 // wave index of the i-th electron of a wave counted over its class segments in order
 CM_D int wave_index(const Counters* c, int cur, int W, int i) {
   int k = 0;
-  while (k < kClasses - 1 && i >= c->nc[cur][k]) {
+  while (k < kSegments - 1 && i >= c->nc[cur][k]) {
     i -= c->nc[cur][k];
     ++k;
   }
@@ -372,7 +378,7 @@ CM_D int wave_index(const Counters* c, int cur, int W, int i) {
 
 CM_D int survivors(const Counters* c, int nxt) {
   int n = 0;
-  for (int k = 0; k < kClasses; ++k) n += c->nc[nxt][k];
+  for (int k = 0; k < kSegments; ++k) n += c->nc[nxt][k];
   return n;
 }
 
@@ -511,7 +517,7 @@ CM_D void spawn_one(const RunView<R>& v, int nxt, int j, int take_se, int poolTo
                     Sink& sink) {
   if (j < take_se) {
     const El<R> se = load_live(v.pool, poolTop - 1 - j);
-    const int seg = v.s.regions[se.region].cls;
+    const int seg = wave_segment(v.s, se.region, se.E);
     store_live(v.w[nxt], seg * v.W + v.c->nc[nxt][seg] + sink.append_q(v.c->ns, seg), se);
     return;
   }
@@ -543,7 +549,7 @@ CM_D void spawn_one(const RunView<R>& v, int nxt, int j, int take_se, int poolTo
   e.aux = 0;
   e.step = 0;
   e.h[0] = e.h[1] = e.h[2] = 0;
-  const int seg = e.region >= 0 ? v.s.regions[e.region].cls : 0;
+  const int seg = wave_segment(v.s, e.region, e.E);
   store_live(v.w[nxt], seg * v.W + v.c->nc[nxt][seg] + sink.append_q(v.c->ns, seg), e);
 }
 
@@ -562,7 +568,7 @@ CM_D void tail_update(Counters* c, int cur, int W, int poolCap, bool steps) {
     c->iterations += 1;
   }
   c->n[nxt] = nn + take_se + take_p;
-  for (int k = 0; k < kClasses; ++k) {
+  for (int k = 0; k < kSegments; ++k) {
     c->nc[nxt][k] += c->ns[k];
     c->ns[k] = 0;
     c->nc[cur][k] = 0;
