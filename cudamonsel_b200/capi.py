@@ -25,10 +25,11 @@ EINVAL, ECUDA, ENOMEM, ESTATE, EOVERFLOW, ELIMIT, ECANCELED, ETIMEOUT = -1, -2, 
 # every symbol include/cudamonsel_b200.h declares
 EXPORTS = (
     "cm_context_create", "cm_context_destroy", "cm_context_reset", "cm_last_error", "cm_set_options", "cm_version",
+    "cm_data_dir",
     "cm_add_mott_element", "cm_add_table", "cm_add_material", "cm_add_msm", "cm_msm_add_nistmott",
     "cm_msm_add_tabulated", "cm_msm_add_fitted", "cm_msm_add_phonon", "cm_msm_add_polaron", "cm_msm_set_csd_jln",
     "cm_msm_set_min_e", "cm_msm_set_barrier", "cm_shape_sphere", "cm_shape_planes", "cm_shape_intersection",
-    "cm_shape_union", "cm_shape_cylinder", "cm_shape_translate", "cm_shape_line", "cm_region_add", "cm_run", "cm_run_device", "cm_run_noalloc",
+    "cm_shape_union", "cm_shape_cylinder", "cm_shape_translate", "cm_shape_rotate", "cm_shape_line", "cm_region_add", "cm_run", "cm_run_device", "cm_run_noalloc",
     "cm_eval_nistmott", "cm_eval_table", "cm_eval_locate", "cm_eval_pick", "cm_eval_tabulated", "cm_eval_elastic", "cm_eval_csd", "cm_eval_phonon",
     "cm_eval_shape", "cm_eval_barrier", "cm_eval_freepath", "cm_server_create", "cm_server_destroy", "cm_job_submit",
     "cm_job_poll", "cm_job_wait", "cm_job_cancel", "cm_job_result", "cm_get_tuning", "cm_set_tuning", "cm_autotune",
@@ -131,6 +132,7 @@ def load(path=LIBPATH):
         "cm_shape_planes": [ctx, C.c_int, d, d, i],
         "cm_shape_intersection": [ctx, C.c_int, C.c_int, i],
         "cm_shape_translate": [ctx, C.c_int, d],
+        "cm_shape_rotate": [ctx, C.c_int, d, C.c_double, C.c_double, C.c_double],
         "cm_shape_union": [ctx, C.c_int, C.c_int, i],
         "cm_shape_cylinder": [ctx, d, d, C.c_double, i],
         "cm_shape_line": [ctx] + [C.c_double] * 7 + [i],
@@ -293,6 +295,10 @@ class Engine:
     def translate(self, shape, d):
         a, pa = _d(d)
         self._check(self.L.cm_shape_translate(self.h, shape, pa))
+
+    def rotate(self, shape, pivot, phi, theta, psi):
+        a, pa = _d(pivot)
+        self._check(self.L.cm_shape_rotate(self.h, shape, pa, phi, theta, psi))
 
     def union(self, a, b):
         return self._out(self.L.cm_shape_union, a, b)

@@ -19,6 +19,7 @@
 // step), so results do not depend on scheduling or on what else is in the wave.
 #include <cooperative_groups.h>
 #include <cuda_runtime.h>
+#include <dlfcn.h>
 
 #include <algorithm>
 #include <array>
@@ -109,6 +110,7 @@ struct HShape {
   std::vector<double> n, p;  // planes
   int a, b;
   double e0[3], ax[3], nax[3], radius;  // cylinder (SI); nax as NormalCylindricalShape computed it
+  double len2;                          // |axis|^2 as the cylinder was built (rotations keep it)
 };
 
 struct HRegion {
@@ -1658,6 +1660,23 @@ extern "C" {
 const char* cm_last_error(void) { return g_err.c_str(); }
 int cm_version(void) { return 1; }
 
+}  // extern "C"
+static void cm_library_anchor() {}  // an address inside this library, whoever calls
+extern "C" {
+const char* cm_data_dir(void) {
+  if (const char* d = getenv("CM_DATA_DIR")) return d;
+  static std::string dir;
+  static std::mutex mu;
+  std::lock_guard<std::mutex> lock(mu);
+  if (dir.empty()) {
+    Dl_info info;
+    std::string p = dladdr((void*)&cm_library_anchor, &info) && info.dli_fname ? info.dli_fname : "";
+    const size_t k = p.rfind('/');
+    dir = (k == std::string::npos ? std::string(".") : p.substr(0, k)) + "/data";
+  }
+  return dir.c_str();
+}
+
 int cm_context_create(int device, cm_context** out) {
   if (!out) return fail(CM_EINVAL, "out is null");
   int n = 0;
@@ -1976,6 +1995,7 @@ int cm_shape_cylinder(cm_context* ctx, const double end0[3], const double end1[3
   }
   const double len2 = (s.ax[0] * s.ax[0]) + (s.ax[1] * s.ax[1]) + (s.ax[2] * s.ax[2]);
   if (!(len2 > 0)) return fail(CM_EINVAL, "cylinder of zero length");
+  s.len2 = len2;
   const double len = (ctx->options & CM_OPT_JMONSEL_FIXES) ? sqrt(len2) : 0.0;
   for (int k = 0; k < 3; ++k) s.nax[k] = s.ax[k] / len;
   s.radius = radius;
@@ -2040,6 +2060,81 @@ static void translate_rec(cm_context* ctx, int id, const double* d) {
   } else {
     for (int k = 0; k < 3; ++k) s.c[k] += d[k];
   }
+}
+
+// Transform3D::rotation (Utility/Transform3D.cu:5-40): Euler angles phi about z, theta about y, psi about z,
+// with the reference's separate form for phi == 0
+static void euler_matrix(double phi, double th, double psi, double r[3][3]) {
+  if (phi != 0.0) {
+    const double cTh = cos(th), sTh = sin(th), cPhi = cos(phi), sPhi = sin(phi), cPsi = cos(psi), sPsi = sin(psi);
+    r[0][0] = cPhi * cTh * cPsi - sPhi * sPsi;
+    r[0][1] = -sPhi * cTh * cPsi - cPhi * sPsi;
+    r[0][2] = sTh * cPsi;
+    r[1][0] = sPhi * cPsi + cPhi * cTh * sPsi;
+    r[1][1] = -sPhi * cTh * sPsi + cPhi * cPsi;
+    r[1][2] = sTh * sPsi;
+    r[2][0] = -cPhi * sTh;
+    r[2][1] = sTh * sPhi;
+    r[2][2] = cTh;
+  } else {
+    const double cTh = cos(th), sTh = sin(th), cPsi = cos(psi), sPsi = sin(psi);
+    r[0][0] = cTh * cPsi;
+    r[0][1] = -sPsi;
+    r[0][2] = sTh * cPsi;
+    r[1][0] = cTh * sPsi;
+    r[1][1] = cPsi;
+    r[1][2] = sTh * sPsi;
+    r[2][0] = -sTh;
+    r[2][1] = 0.0;
+    r[2][2] = cTh;
+  }
+}
+
+// Transform3D::rotate (Transform3D.cu:73-92, 125-128): the matrix times v, each component summed from zero
+// over the columns in order; a point turns about the pivot
+static void rot_vec(const double r[3][3], const double* v, double* out) {
+  double o[3];
+  for (int i = 0; i < 3; ++i) {
+    double acc = 0.0;
+    for (int k = 0; k < 3; ++k) acc += r[i][k] * v[k];
+    o[i] = acc;
+  }
+  for (int i = 0; i < 3; ++i) out[i] = o[i];
+}
+static void rot_point(const double r[3][3], const double* pt, const double* pivot, double* out) {
+  double d[3], q[3];
+  for (int k = 0; k < 3; ++k) d[k] = pt[k] - pivot[k];
+  rot_vec(r, d, q);
+  for (int k = 0; k < 3; ++k) out[k] = q[k] + pivot[k];
+}
+
+static void rotate_rec(cm_context* ctx, int id, const double r[3][3], const double* pivot) {
+  HShape& s = ctx->shapes[id];
+  if (s.kind == SHAPE_PLANES) {  // Plane::rotate (MultiPlaneShape.cu:53-57): normal and point
+    for (size_t i = 0; i + 2 < s.n.size(); i += 3) {
+      rot_vec(r, &s.n[i], &s.n[i]);
+      rot_point(r, &s.p[i], pivot, &s.p[i]);
+    }
+  } else if (s.kind == SHAPE_INTERSECTION || s.kind == SHAPE_UNION) {
+    rotate_rec(ctx, s.a, r, pivot);
+    rotate_rec(ctx, s.b, r, pivot);
+  } else if (s.kind == SHAPE_CYLINDER) {  // NormalCylindricalShape.cu:324-330
+    rot_point(r, s.e0, pivot, s.e0);
+    rot_vec(r, s.ax, s.ax);
+    const double l = sqrt(s.len2);
+    for (int k = 0; k < 3; ++k) s.nax[k] = s.ax[k] / l;
+  } else {
+    rot_point(r, s.c, pivot, s.c);
+  }
+}
+
+int cm_shape_rotate(cm_context* ctx, int shape, const double pivot[3], double phi, double theta, double psi) {
+  if (!ctx || !pivot || shape < 0 || shape >= (int)ctx->shapes.size()) return fail(CM_EINVAL, "bad shape handle");
+  double r[3][3];
+  euler_matrix(phi, theta, psi, r);
+  rotate_rec(ctx, shape, r, pivot);
+  ctx->dirty();
+  return 0;
 }
 
 int cm_shape_translate(cm_context* ctx, int shape, const double d[3]) {

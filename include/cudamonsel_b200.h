@@ -76,6 +76,10 @@ typedef struct {
 int cm_get_tuning(cm_context* ctx, int precision, cm_tuning* out);
 int cm_set_tuning(cm_context* ctx, int precision, const cm_tuning* tuning);
 int cm_version(void);
+/* The directory of the data files the library ships (NistXSec/E%02d.bin: NIST SRD-64 elastic tables):
+ * $CM_DATA_DIR, else the "data" folder beside the loaded libcudamonsel_b200.so.  No reference counterpart
+ * (the reference opens its data by paths relative to the working directory). */
+const char* cm_data_dir(void);
 
 /* ---- data ------------------------------------------------------------------- */
 /* NIST SRD-64 elastic table of one element, as NISTMottScatteringAngle::loadData
@@ -127,6 +131,12 @@ int cm_shape_union(cm_context* ctx, int a, int b, int* out_shape);
  * never struck by a step; that is reproduced unless CM_OPT_JMONSEL_FIXES is set when it is created. */
 int cm_shape_cylinder(cm_context* ctx, const double end0[3], const double end1[3], double radius, int* out_shape);
 int cm_shape_translate(cm_context* ctx, int shape, const double distance[3]);
+/* ITransform::rotate(pivot, phi, theta, psi): Euler angles phi about z, theta about y, psi about z, around
+ * pivot (Utility/Transform3D.cu:5-128), for NormalMultiPlaneShape (NormalMultiPlaneShape.cu:257-261: every
+ * plane's normal and point), NormalCylindricalShape (NormalCylindricalShape.cu:324-330: its end, its axis
+ * and the axis normalised by the length it was built with, so a rotation also normalises the axis of a
+ * cylinder built without CM_OPT_JMONSEL_FIXES) and Sphere; intersections and unions rotate their parts. */
+int cm_shape_rotate(cm_context* ctx, int shape, const double pivot[3], double phi, double theta, double psi);
 /* NShapes::createLine(topz, width, length, thetal, thetar, radl, radr) (JMONSEL/NShapes.cu:55-149); a corner
  * radius adds a clipping plane and a cylinder joined by a union.  The reference's left corner uses the right
  * sidewall (NShapes.cu:140); CM_OPT_JMONSEL_FIXES set when the line is created uses the left one. */

@@ -810,6 +810,96 @@ int cmo_shape_translate(cmo_scene* s, int shape, const double d[3])
    return 0;
 }
 
+/* Transform3D::rotation (Utility/Transform3D.cu:5-40): Euler angles phi about z, theta about y, psi about
+ * z, with the reference's separate form for phi == 0 */
+static void euler_matrix(double phi, double th, double psi, double r[3][3])
+{
+   if (phi != 0.0) {
+      const double cTh = cos(th), sTh = sin(th), cPhi = cos(phi), sPhi = sin(phi), cPsi = cos(psi), sPsi = sin(psi);
+      r[0][0] = cPhi * cTh * cPsi - sPhi * sPsi;
+      r[0][1] = -sPhi * cTh * cPsi - cPhi * sPsi;
+      r[0][2] = sTh * cPsi;
+      r[1][0] = sPhi * cPsi + cPhi * cTh * sPsi;
+      r[1][1] = -sPhi * cTh * sPsi + cPhi * cPsi;
+      r[1][2] = sTh * sPsi;
+      r[2][0] = -cPhi * sTh;
+      r[2][1] = sTh * sPhi;
+      r[2][2] = cTh;
+   }
+   else {
+      const double cTh = cos(th), sTh = sin(th), cPsi = cos(psi), sPsi = sin(psi);
+      r[0][0] = cTh * cPsi;
+      r[0][1] = -sPsi;
+      r[0][2] = sTh * cPsi;
+      r[1][0] = cTh * sPsi;
+      r[1][1] = cPsi;
+      r[1][2] = sTh * sPsi;
+      r[2][0] = -sTh;
+      r[2][1] = 0.0;
+      r[2][2] = cTh;
+   }
+}
+
+/* Transform3D::rotate(v, phi, th, psi) (Transform3D.cu:73-92): the matrix times v, each component summed
+ * from zero over the columns in order, as its times() does */
+static void rot_vec(const double r[3][3], const double v[3], double out[3])
+{
+   for (int i = 0; i < 3; ++i) {
+      double acc = 0.0;
+      for (int k = 0; k < 3; ++k) acc += r[i][k] * v[k];
+      out[i] = acc;
+   }
+}
+
+/* Transform3D::rotate(point, pivot, ...) (Transform3D.cu:125-128): about the pivot */
+static void rot_point(const double r[3][3], const double pt[3], const double pivot[3], double out[3])
+{
+   double d[3], q[3];
+   for (int k = 0; k < 3; ++k) d[k] = pt[k] - pivot[k];
+   rot_vec(r, d, q);
+   for (int k = 0; k < 3; ++k) out[k] = q[k] + pivot[k];
+}
+
+/* ITransform::rotate: NormalMultiPlaneShape (NormalMultiPlaneShape.cu:257-261 -> MultiPlaneShape.cu:306-310
+ * -> Plane::rotate, MultiPlaneShape.cu:53-57: normal and point), NormalCylindricalShape
+ * (NormalCylindricalShape.cu:324-330: end point about the pivot, axis, and the normalised axis from the
+ * rotated axis and the length set at construction), Sphere (its centre).  Intersections and unions pass it
+ * to their parts (the reference's cast makes that unsafe to run there). */
+int cmo_shape_rotate(cmo_scene* s, int shape, const double pivot[3], double phi, double theta, double psi)
+{
+   double r[3][3];
+   euler_matrix(phi, theta, psi, r);
+   shape_t* sh = &s->shapes[shape];
+   if (sh->kind == S_PLANES) {
+      for (int i = 0; i < sh->np; ++i) {
+         double n[3], p[3];
+         rot_vec(r, sh->n[i], n);
+         rot_point(r, sh->p[i], pivot, p);
+         memcpy(sh->n[i], n, sizeof(n));
+         memcpy(sh->p[i], p, sizeof(p));
+      }
+   }
+   else if (sh->kind == S_INTERSECTION || sh->kind == S_UNION) {
+      cmo_shape_rotate(s, sh->a, pivot, phi, theta, psi);
+      cmo_shape_rotate(s, sh->b, pivot, phi, theta, psi);
+   }
+   else if (sh->kind == S_CYLINDER) {
+      double e0[3], ax[3];
+      rot_point(r, sh->e0, pivot, e0);
+      rot_vec(r, sh->ax, ax);
+      memcpy(sh->e0, e0, sizeof(e0));
+      memcpy(sh->ax, ax, sizeof(ax));
+      const double l = sqrt(sh->len2);
+      for (int k = 0; k < 3; ++k) sh->nax[k] = sh->ax[k] / l;
+   }
+   else if (sh->kind == S_SPHERE) {
+      double c[3];
+      rot_point(r, sh->c, pivot, c);
+      memcpy(sh->c, c, sizeof(c));
+   }
+   return 0;
+}
+
 /* JMONSEL/NShapes.cu:55-149.  With a corner radius the sidewall becomes the
  * union of the sidewall (plus a clipping plane) and a cylinder along y.  The
  * reference builds the left union from the RIGHT sidewall's plane set

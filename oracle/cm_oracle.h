@@ -66,6 +66,7 @@ int cmo_shape_intersection(cmo_scene* s, int a, int b);
 int cmo_shape_cylinder(cmo_scene* s, const double end0[3], const double end1[3], double radius);
 int cmo_shape_union(cmo_scene* s, int a, int b);
 int cmo_shape_translate(cmo_scene* s, int shape, const double d[3]);
+int cmo_shape_rotate(cmo_scene* s, int shape, const double pivot[3], double phi, double theta, double psi);
 int cmo_shape_line(cmo_scene* s, double topz, double width, double length, double thetal, double thetar, double radl,
                    double radr);
 int cmo_region(cmo_scene* s, int parent, int msm, int shape);

@@ -54,6 +54,7 @@ def lib():
         L.cmo_shape_planes.argtypes = [C.c_void_p, C.c_int, d, d]
         L.cmo_shape_intersection.argtypes = [C.c_void_p, C.c_int, C.c_int]
         L.cmo_shape_translate.argtypes = [C.c_void_p, C.c_int, d]
+        L.cmo_shape_rotate.argtypes = [C.c_void_p, C.c_int, d, C.c_double, C.c_double, C.c_double]
         L.cmo_shape_line.argtypes = [C.c_void_p] + [C.c_double] * 7
         L.cmo_shape_cylinder.argtypes = [C.c_void_p, d, d, C.c_double]
         L.cmo_shape_union.argtypes = [C.c_void_p, C.c_int, C.c_int]
@@ -204,6 +205,10 @@ class OracleBackend:
     def translate(self, shape, d):
         d = np.array(d, dtype=np.float64)
         return self.L.cmo_shape_translate(self.h, shape, dp(d))
+
+    def rotate(self, shape, pivot, phi, theta, psi):
+        pv = np.array(pivot, dtype=np.float64)
+        return self.L.cmo_shape_rotate(self.h, shape, dp(pv), phi, theta, psi)
 
     def line(self, topz, width, length, thetal, thetar, radl=0.0, radr=0.0):
         return self._chk(self.L.cmo_shape_line(self.h, topz, width, length, thetal, thetar, radl, radr))

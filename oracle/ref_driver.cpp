@@ -6,6 +6,7 @@
 // uniform deviates through the Math2::random() hook.
 //
 //   ref_driver golden <outdir> <SiTablesDir>
+//   ref_driver golden2 <outdir>                  (sets added later: rotated shapes)
 //   ref_driver run1 <nprim> <seed> <SiTablesDir> [beam_eV]
 //   ref_driver run2 <nprim_per_px> <seed> <SiTablesDir> <x0_nm> <dx_nm> <npix> [beam_eV]
 //   ref_driver scene <scene.txt> <pixels.txt> <seed> <beam_width_m> [angles]
@@ -685,6 +686,70 @@ static int run_scene(bool lines, int nprim, unsigned long long seed, const std::
    return 0;
 }
 
+// ---------------------------------------------------------------- rotated shapes
+// ITransform::rotate of the Normal shapes that rotate safely (NormalMultiPlaneShape.cu:257-261 through
+// MultiPlaneShape::rotate and Plane::rotate, NormalCylindricalShape.cu:324-330), with the Euler-angle
+// matrix of Utility/Transform3D.cu (both branches: phi != 0 and the phi == 0 special case).
+static void golden_rotate(const std::string& out)
+{
+   FILE* f = openw(out, "rotate.txt");
+   fprintf(f, "# shape(0 block rotated phi,theta,psi about a pivot, 1 block rotated with phi=0, 2 tilted half-space,"
+              " 3 cylinder rotated (axis normalised by the rotation), 4 cylinder rotated twice) "
+              "p0(3) p1(3) | nx ny nz u contains(p0) contains(p0,p1)\n");
+   std::mt19937_64 gin(777);
+   auto u = [&]() { return (double)(gin() >> 11) * (1.0 / 9007199254740992.0); };
+   auto block = [&]() {
+      NormalMultiPlaneShapeT* b = new NormalMultiPlaneShapeT();
+      double c[] = { 5e-9, -3e-9, 12e-9 }, h[] = { 15e-9, 10e-9, 5e-9 };
+      for (int a = 0; a < 3; ++a)
+         for (int sg = -1; sg <= 1; sg += 2) {
+            double n[] = { 0, 0, 0 }, p[] = { c[0], c[1], c[2] };
+            n[a] = sg;
+            p[a] += sg * h[a];
+            b->addPlane(*new PlaneT(n, 3, p, 3));
+         }
+      return b;
+   };
+   NormalMultiPlaneShapeT* b0 = block();
+   const double piv0[] = { 3e-9, -2e-9, 10e-9 };
+   b0->rotate(piv0, 0.7, 0.4, -1.1);
+   NormalMultiPlaneShapeT* b1 = block();
+   const double piv1[] = { -4e-9, 6e-9, 0. };
+   b1->rotate(piv1, 0.0, 0.9, 0.3);
+   NormalMultiPlaneShapeT* hs = new NormalMultiPlaneShapeT();
+   double nz[] = { 0., 0., -1. }, o[] = { 0., 0., 0. };
+   hs->addPlane(*new PlaneT(nz, 3, o, 3));
+   const double piv2[] = { 10e-9, 0., 0. };
+   hs->rotate(piv2, 0.2, 0.3, 0.0);
+   double e0[] = { -20e-9, -10e-9, 30e-9 }, e1[] = { 25e-9, 15e-9, 50e-9 };
+   NormalCylindricalShapeT* c0 = new NormalCylindricalShapeT(e0, e1, 12e-9);
+   const double piv3[] = { 0., 5e-9, 20e-9 };
+   c0->rotate(piv3, -0.5, 1.2, 0.8);
+   NormalCylindricalShapeT* c1 = new NormalCylindricalShapeT(e0, e1, 9e-9);
+   c1->rotate(piv3, 0.0, 0.5, 0.0);
+   c1->rotate(piv0, 1.3, -0.2, 0.6);
+   NormalShapeT* shapes[] = { (NormalShapeT*)b0, (NormalShapeT*)b1, (NormalShapeT*)hs, (NormalShapeT*)c0,
+                              (NormalShapeT*)c1 };
+   const double* around[] = { piv0, piv1, piv2, piv3, piv0 };  // segments start near each shape
+   for (int s = 0; s < 5; ++s) {
+      for (int i = 0; i < 3000; ++i) {
+         double p0[3], p1[3];
+         for (int k = 0; k < 3; ++k) p0[k] = around[s][k] + (u() * 50 - 25) * 1e-9;
+         double len = ::exp(::log(0.05e-9) + (::log(60e-9) - ::log(0.05e-9)) * u());
+         double th2 = Math2::PI * u(), ph = 2 * Math2::PI * u();
+         p1[0] = p0[0] + len * ::sin(th2) * ::cos(ph);
+         p1[1] = p0[1] + len * ::sin(th2) * ::sin(ph);
+         p1[2] = p0[2] + len * ::cos(th2);
+         VectorXd r = shapes[s]->getFirstNormal(p0, p1);
+         int inside = ((ShapeT*)shapes[s])->contains(p0) ? 1 : 0;
+         int inside2 = shapes[s]->contains(p0, p1) ? 1 : 0;
+         fprintf(f, "%d " G " " G " " G " " G " " G " " G " " G " " G " " G " " G " %d %d\n", s, p0[0], p0[1], p0[2], p1[0],
+                 p1[1], p1[2], r[0], r[1], r[2], r[3], inside, inside2);
+      }
+   }
+   fclose(f);
+}
+
 // ---------------------------------------------------------------- scene replay
 // A scene written by cudamonsel_b200.scenes.SceneSpec.to_text: one construction call per line,
 // arguments in SI units, handles = line numbers of earlier calls.  Every call is made on the
@@ -975,6 +1040,10 @@ int main(int argc, char** argv)
       golden_barrier(out, si);
       golden_shapes2(out);
       golden_nistmott23(out);  // last, so the earlier sets keep their input streams
+      return 0;
+   }
+   if (mode == "golden2" && argc >= 3) {  // sets added later, each with its own input stream
+      golden_rotate(argv[2]);
       return 0;
    }
    if (mode == "run1" && argc >= 5) {

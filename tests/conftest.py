@@ -79,3 +79,40 @@ def shapes2_scene(fixes=0):
     cylt = s.cylinder([-20e-9, -10e-9, 30e-9], [25e-9, 15e-9, 50e-9], 12e-9)
     s.translate(cylt, [30e-9, 0.0, -10e-9])
     return s, [cyl, cyly, uni, rline, cylt]
+
+
+def rotate_scene():
+    """The shapes of the rotated-shapes fixture (ITransform::rotate): a 6-plane block rotated by Euler angles
+    about a pivot, the same block rotated with phi = 0, a tilted half-space, a cylinder rotated once (the
+    rotation normalises the reference's cylinder axis) and a cylinder rotated twice."""
+    from cudamonsel_b200 import scenes
+    s = scenes.SceneSpec()
+
+    def block():
+        c, hh = (5e-9, -3e-9, 12e-9), (15e-9, 10e-9, 5e-9)
+        n, p = [], []
+        for a in range(3):
+            for sg in (-1, 1):
+                nn = [0.0, 0.0, 0.0]
+                pp = list(c)
+                nn[a] = float(sg)
+                pp[a] += sg * hh[a]
+                n += nn
+                p += pp
+        return s.planes(n, p)
+
+    piv0, piv1, piv2, piv3 = [3e-9, -2e-9, 10e-9], [-4e-9, 6e-9, 0.0], [10e-9, 0.0, 0.0], [0.0, 5e-9, 20e-9]
+    b0 = block()
+    s.rotate(b0, piv0, 0.7, 0.4, -1.1)
+    b1 = block()
+    s.rotate(b1, piv1, 0.0, 0.9, 0.3)
+    hs = s.planes([0.0, 0.0, -1.0], [0.0, 0.0, 0.0])
+    s.rotate(hs, piv2, 0.2, 0.3, 0.0)
+    e0, e1 = [-20e-9, -10e-9, 30e-9], [25e-9, 15e-9, 50e-9]
+    c0 = s.cylinder(e0, e1, 12e-9)
+    s.rotate(c0, piv3, -0.5, 1.2, 0.8)
+    c1 = s.cylinder(e0, e1, 9e-9)
+    s.rotate(c1, piv3, 0.0, 0.5, 0.0)
+    s.rotate(c1, piv0, 1.3, -0.2, 0.6)
+    return s, [b0, b1, hs, c0, c1]
+

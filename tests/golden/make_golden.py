@@ -25,6 +25,7 @@ def main():
     with tempfile.TemporaryDirectory() as tmp:
         subprocess.check_call([os.path.join(ref, "ref_driver"), "golden", tmp, tables], cwd=ref,
                               stdout=subprocess.DEVNULL)
+        subprocess.check_call([os.path.join(ref, "ref_driver"), "golden2", tmp], cwd=ref, stdout=subprocess.DEVNULL)
         for name in sorted(os.listdir(tmp)):
             src = os.path.join(tmp, name)
             with open(src, "rb") as f, gzip.open(os.path.join(HERE, name + ".gz"), "wb", compresslevel=9) as g:

@@ -218,6 +218,28 @@ def test_shapes2(fixes):
             assert ok, (k, j, bad)
 
 
+def test_rotate():
+    """ITransform::rotate of plane sets and cylinders (Utility/Transform3D.cu, NormalMultiPlaneShape.cu:257-261,
+    NormalCylindricalShape.cu:324-330): first normal, u, contains(p0), contains(p0, p1) of the rotated shapes
+    equal the reference's bit for bit."""
+    import pyoracle as po
+    from cudamonsel_b200 import scenes
+    from conftest import rotate_scene
+    s, shapes = rotate_scene()
+    b = po.OracleBackend()
+    res = scenes.replay(s, b)
+    g = golden("rotate")
+    for k, sh in enumerate(shapes):
+        rows = g[g[:, 0] == k]
+        assert len(rows) == 3000
+        p01 = np.ascontiguousarray(rows[:, 1:7])
+        out = np.zeros((len(rows), 6))
+        b.L.cmo_eval_shape(b.h, res[sh.idx], len(rows), po.dp(p01), D(out))
+        for j in range(6):
+            ok, bad = exact(out[:, j], rows[:, 7 + j])
+            assert ok, (k, j, bad)
+
+
 def test_barrier(oracle_halfspace):
     """ExpQMBarrierSM (classical) on the vacuum/Si surface, both directions, above and
     below the 3.75 eV barrier."""
