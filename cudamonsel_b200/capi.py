@@ -72,7 +72,8 @@ class RunStats(C.Structure):
                 ("barrier_events", C.c_int64), ("escapes", C.c_int64), ("secondaries", C.c_int64),
                 ("iterations", C.c_int64), ("device_ms", C.c_double), ("kernel_ms", C.c_double * 6),
                 ("kernel_launches", C.c_int64 * 6), ("units", C.c_int64 * 4), ("step_launches", C.c_int64),
-                ("step_units", C.c_int64), ("step_ms", C.c_double)]
+                ("step_units", C.c_int64), ("step_ms", C.c_double), ("ended_zero_energy", C.c_int64),
+                ("ended_step_limit", C.c_int64)]
 
     KERNELS = ("flight", "elastic", "inelastic", "misc", "spawn", "tail")
 
@@ -84,6 +85,8 @@ class RunStats(C.Structure):
         d["step_launches"] = self.step_launches
         d["step_units"] = self.step_units
         d["step_ms"] = self.step_ms
+        d["ended_zero_energy"] = self.ended_zero_energy
+        d["ended_step_limit"] = self.ended_step_limit
         return d
 
 

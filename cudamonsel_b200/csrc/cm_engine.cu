@@ -837,6 +837,8 @@ __device__ __forceinline__ void flush_counts(Counters* c, StepCounts& sc) {
     sc.bar += __shfl_down_sync(0xffffffffu, sc.bar, off);
     sc.esc += __shfl_down_sync(0xffffffffu, sc.esc, off);
     sc.sec += __shfl_down_sync(0xffffffffu, sc.sec, off);
+    sc.zero += __shfl_down_sync(0xffffffffu, sc.zero, off);
+    sc.limit += __shfl_down_sync(0xffffffffu, sc.limit, off);
   }
   if ((threadIdx.x & 31) == 0) {
     if (sc.steps) atomicAdd(&c->steps, sc.steps);
@@ -844,6 +846,8 @@ __device__ __forceinline__ void flush_counts(Counters* c, StepCounts& sc) {
     if (sc.bar) atomicAdd(&c->barriers, sc.bar);
     if (sc.esc) atomicAdd(&c->escapes, sc.esc);
     if (sc.sec) atomicAdd(&c->secondaries, sc.sec);
+    if (sc.zero) atomicAdd(&c->ended_zero, sc.zero);
+    if (sc.limit) atomicAdd(&c->ended_limit, sc.limit);
   }
 }
 
@@ -1454,6 +1458,8 @@ static int run_device_once(cm_context* ctx, const cm_run_desc* d, uint32_t* back
     st->step_launches = tslots;
     st->step_units = (int64_t)c.step_units;
     st->step_ms = step_ms;
+    st->ended_zero_energy = (int64_t)c.ended_zero;
+    st->ended_step_limit = (int64_t)c.ended_limit;
   }
   return status;
 }
@@ -1787,6 +1793,15 @@ int cm_add_table(cm_context* ctx, int dim, const int* n, const double* axes, con
     t.x[k].assign(axes + off, axes + off + n[k]);
     off += n[k];
     total *= n[k];
+    // a corrupt table is refused here (the reference throws on a table it cannot read,
+    // NUTableInterpolation.cu:121): every abscissa finite, each axis strictly monotonic
+    const std::vector<double>& x = t.x[k];
+    const bool up = x[1] > x[0];
+    for (int i = 0; i < n[k]; ++i) {
+      if (!std::isfinite(x[i])) return fail(CM_EINVAL, "table axis " + std::to_string(k) + " has a non-finite value");
+      if (i > 0 && (up ? !(x[i] > x[i - 1]) : !(x[i] < x[i - 1])))
+        return fail(CM_EINVAL, "table axis " + std::to_string(k) + " is not strictly monotonic");
+    }
     // NUTableInterpolation::ReadTable (:152-159)
     if (t.x[k][0] < t.x[k][n[k] - 1]) {
       t.domain[k][0] = t.x[k][0];
@@ -1797,6 +1812,8 @@ int cm_add_table(cm_context* ctx, int dim, const int* n, const double* axes, con
     }
   }
   t.v.assign(values, values + total);
+  for (double v : t.v)
+    if (!std::isfinite(v)) return fail(CM_EINVAL, "table value not finite");
   for (double v : t.v) {  // (:169-172): if / else-if, as written
     if (v < t.range[0]) t.range[0] = v;
     else if (v > t.range[1]) t.range[1] = v;
@@ -2242,8 +2259,11 @@ static int prep_pixels(const cm_run_desc* d, const double* center, const double*
   p.prefix.resize(d->npix + 1);
   p.prefix[0] = 0;
   for (int i = 0; i < d->npix; ++i) {
-    for (int k = 0; k < 3; ++k) p.center_nm[3 * i + k] = center[3 * i + k] * 1e9;
-    if (!(energy[i] > 0)) return fail(CM_EINVAL, "beam energy must be positive");
+    for (int k = 0; k < 3; ++k) {
+      if (!std::isfinite(center[3 * i + k])) return fail(CM_EINVAL, "pixel centre not finite");
+      p.center_nm[3 * i + k] = center[3 * i + k] * 1e9;
+    }
+    if (!(energy[i] > 0) || !std::isfinite(energy[i])) return fail(CM_EINVAL, "beam energy must be positive and finite");
     if (nprim[i] < 0) return fail(CM_EINVAL, "negative primary count");
     if (nbins[i] < 1 || nbins[i] + 2 > stride) return fail(CM_EINVAL, "pixel_nbins out of range");
     p.e0[i] = energy[i] * kFromSIeV;
@@ -2857,6 +2877,8 @@ static int run_noalloc(cm_context* ctx, const cm_run_desc* d, uint32_t* back, ui
     st->secondaries = (int64_t)hc.secondaries;
     st->iterations = (int64_t)hc.iterations;
     st->device_ms = ms;
+    st->ended_zero_energy = (int64_t)hc.ended_zero;
+    st->ended_step_limit = (int64_t)hc.ended_limit;
     for (int k = 0; k < 6; ++k) st->kernel_launches[k] = it;
     for (int k = 0; k < 4; ++k) st->units[k] = (int64_t)hc.units[k];
   }

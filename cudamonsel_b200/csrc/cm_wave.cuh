@@ -37,6 +37,7 @@ struct Counters {
   unsigned long long step_units;  // electrons the several-steps kernel started with
   unsigned long long logged;      // escapes offered to the escape log
   unsigned long long slots, tail_slots;  // iteration slots the device-driven loop ran (all, tail)
+  unsigned long long ended_zero, ended_limit;  // electrons ended by the zero-energy cut, by the step limit
 };
 
 template <typename R>
@@ -149,7 +150,7 @@ struct RunView {
 
 // per-thread event counts, reduced once per warp by the kernels
 struct StepCounts {
-  unsigned long long steps = 0, scat = 0, bar = 0, esc = 0, sec = 0;
+  unsigned long long steps = 0, scat = 0, bar = 0, esc = 0, sec = 0, zero = 0, limit = 0;
 };
 
 // Histogram::bin (Utility/Histogram.cu:73-80) over bins min + i*delta with
@@ -266,13 +267,16 @@ CM_D int flight_apply(const RunView<R>& v, El<R>& e, Sink& sink, StepCounts& sc,
       kind = s.mechs[m.mech0 + idx].kind;
     } else if (e.step > 1000000u) {  // MONSEL_MaterialScatterModel::randomMeanPathLength (:86-90)
       complete = true;
+      ++sc.limit;
     } else if (!(e.E > R(0)) && e.step > 4096u) {
       // With no energy and no mechanism an electron only flies straight and is reflected by every
       // barrier it meets (ExpQMBarrierSM: perpE = 0 never transmits); trapped between two walls it
       // bounces until the 1e6-step limit above, one wave iteration per bounce.  It is ended here
       // once it has taken 4096 steps (one that would have reached the chamber later, tallied at
-      // 0 eV, is lost; that needs more than 4096 steps and never occurred in the tests).
+      // 0 eV, is lost; that needs more than 4096 steps and never occurred in the tests).  Counted in
+      // cm_run_stats.ended_zero_energy.
       complete = true;
+      ++sc.zero;
     }
   }
   double p1[3] = {e.p[0] + fp * (double)e.d[0], e.p[1] + fp * (double)e.d[1], e.p[2] + fp * (double)e.d[2]};

@@ -34,15 +34,25 @@ def read_nu_table(path):
     Returns (dim, n[], axes[], values ndarray with the last index fastest)."""
     with open(path) as f:
         tok = f.read().split()
-    pos = 0
-    dim = int(tok[pos]); pos += 1
-    n, axes = [], []
-    for _ in range(dim):
-        k = int(tok[pos]); pos += 1
-        axes.append(np.array([float(t) for t in tok[pos:pos + k]], dtype=np.float64)); pos += k
-        n.append(k)
-    total = int(np.prod(n))
-    vals = np.array([float(t) for t in tok[pos:pos + total]], dtype=np.float64).reshape(n)
+    try:
+        pos = 0
+        dim = int(tok[pos]); pos += 1
+        if not 1 <= dim <= 4:
+            raise ValueError("dimension %d" % dim)
+        n, axes = [], []
+        for _ in range(dim):
+            k = int(tok[pos]); pos += 1
+            if k < 1 or pos + k > len(tok):
+                raise ValueError("axis of %d points" % k)
+            axes.append(np.array([float(t) for t in tok[pos:pos + k]], dtype=np.float64)); pos += k
+            n.append(k)
+        total = int(np.prod(n))
+        if pos + total > len(tok):
+            raise ValueError("%d values of %d" % (len(tok) - pos, total))
+        vals = np.array([float(t) for t in tok[pos:pos + total]], dtype=np.float64).reshape(n)
+    except (IndexError, ValueError) as e:
+        # the reference throws on a table it cannot read (NUTableInterpolation.cu:121)
+        raise ValueError("corrupt or truncated scattering table %s: %s" % (path, e)) from None
     return dim, n, axes, vals
 
 

@@ -217,6 +217,10 @@ typedef struct {
                                   flight .. misc do not run in those iterations */
   int64_t step_units;          /* electrons those launches started with */
   double step_ms;              /* their time (profile != 0 only) */
+  int64_t ended_zero_energy;   /* electrons with no energy left, in a region without scatter mechanisms,
+                                  ended after 4096 steps (each one only bounces between barriers) */
+  int64_t ended_step_limit;    /* electrons ended by the reference's 10^6-step limit
+                                  (MONSEL_MaterialScatterModel.cu:86-90) */
 } cm_run_stats;
 
 /* back/fwd: [npix * hist_stride] counts, index = histogram bin + 1 (0 = underflow,
