@@ -18,6 +18,7 @@
 // from its own Philox stream (key = primary or parent lineage, counter =
 // step), so results do not depend on scheduling or on what else is in the wave.
 #include <cooperative_groups.h>
+#include <cooperative_groups/reduce.h>
 #include <cuda_runtime.h>
 #include <dlfcn.h>
 
@@ -788,6 +789,13 @@ struct DeviceSink {
     return base + (int)part.thread_rank();
   }
   __device__ __forceinline__ void count(uint32_t* h) { atomicAdd(h, 1u); }
+  // counters[idx] += value, one atomic per group of converged lanes with the same idx
+  __device__ __forceinline__ void add_by(unsigned long long* counters, int idx, unsigned long long value) {
+    cg::coalesced_group g = cg::coalesced_threads();
+    cg::coalesced_group part = cg::labeled_partition(g, idx);
+    const unsigned long long sum = cg::reduce(part, value, cg::plus<unsigned long long>());
+    if (part.thread_rank() == 0) atomicAdd(counters + idx, sum);
+  }
   __device__ __forceinline__ unsigned long long ticket(unsigned long long* c) { return atomicAdd(c, 1ull); }
   __device__ __forceinline__ void error(int* e, int code) { atomicExch(e, code); }
 };

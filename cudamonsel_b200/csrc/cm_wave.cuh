@@ -130,6 +130,17 @@ struct RunIO {
   int tail_below;
   int queue_only;
   const volatile int* cancel;
+  // A run of several jobs (the job server's shared wave; all null otherwise): per pixel its chamber, the
+  // offset of its tally row (u32 elements into back/fwd) and its job; per job the electrons alive (a
+  // primary or secondary counts from its start to its end), their steps (added when each ends) and a stop
+  // flag that keeps its unstarted primaries out of the wave.
+  const int* pchamber;
+  const double* pwidth;  // Gaussian beam width per pixel, nm
+  const unsigned long long* ptally;
+  const int* pjob;
+  unsigned long long* job_alive;
+  unsigned long long* job_steps;
+  const int* job_stop;
 };
 
 template <typename R>
@@ -202,7 +213,7 @@ template <typename R, typename Sink> CM_D void tally_escape(const RunView<R>& v,
   const int b = hist_bin(E0ref, nb, val) + 1;
   if (b > nb + 1) return;  // past the overflow slot: the reference writes out of bounds and never counts it
   uint32_t* h = elevation < (kPi / 2.0) ? io.fwd : io.back;
-  sink.count(h + (size_t)px * io.stride + b);
+  sink.count(h + (io.ptally ? (size_t)io.ptally[px] : (size_t)px * io.stride) + b);
 }
 
 #ifdef CM_TRACE
@@ -214,6 +225,25 @@ template <typename R, typename Sink> CM_D void cm_trace(const RunView<R>& v, con
   for (int j = 0; j < 3; ++j) { t.p[j] = e.p[j]; t.d[j] = (double)e.d[j]; }
 }
 #endif
+
+// job accounting of a run of several jobs: an electron of pixel px starts, or ends after `steps` steps
+template <typename R, typename Sink> CM_D void job_start(const RunView<R>& v, int px, Sink& sink) {
+  const RunIO& io = *v.io;
+  if (io.job_alive) sink.add_by(io.job_alive, io.pjob[px], 1ull);
+}
+template <typename R, typename Sink> CM_D void job_end(const RunView<R>& v, int px, uint32_t steps, Sink& sink) {
+  const RunIO& io = *v.io;
+  if (!io.job_alive) return;
+  const int j = io.pjob[px];
+  sink.add_by(io.job_alive, j, ~0ull);  // minus one
+  sink.add_by(io.job_steps, j, (unsigned long long)steps);
+}
+
+// the chamber a pixel's electrons fly in
+template <typename R> CM_D int chamber_of(const RunView<R>& v, int px) {
+  const RunIO& io = *v.io;
+  return io.pchamber ? io.pchamber[px] : v.s.chamber;
+}
 
 // MONSEL_MaterialScatterModel::setCache (MONSEL_MaterialScatterModel.cu:44-62): the cumulative scatter rates
 // of the model's mechanisms at E (1/nm) into cum[0..nmech); returns the total
@@ -246,7 +276,8 @@ template <typename R, int D, typename Sink>
 CM_D int flight_apply(const RunView<R>& v, El<R>& e, Sink& sink, StepCounts& sc, const int* pixel_src = nullptr) {
   const SceneView<R>& s = v.s;
   int reg = e.region;
-  if (reg < 0 || !shape_contains<R, D>(s, s.regions[reg].shape, e.p)) reg = containing_subregion<R, D>(s, s.chamber, e.p);
+  if (reg < 0 || !shape_contains<R, D>(s, s.regions[reg].shape, e.p))
+    reg = containing_subregion<R, D>(s, chamber_of(v, pixel_src ? *pixel_src : e.pixel), e.p);
   if (reg < 0) return -1;
   const Msm& m = s.msms[s.regions[reg].msm];
   bool complete = false;
@@ -347,7 +378,10 @@ CM_D void flight_one(const RunView<R>& v, int cur, int i, Sink& sink, StepCounts
   e.region = W.region[i];
   e.key = W.key[i];
   const int queue = flight_apply<R, D>(v, e, sink, sc, W.pixel + i);  // the pixel is read only on escape
-  if (queue < 0) return;
+  if (queue < 0) {
+    if (v.io->job_alive) job_end(v, W.pixel[i], e.step, sink);
+    return;
+  }
   W.px[i] = e.p[0]; W.py[i] = e.p[1]; W.pz[i] = e.p[2];
   W.E[i] = e.E; W.Ep[i] = e.Ep;
   W.region[i] = e.region; W.aux[i] = e.aux;
@@ -407,6 +441,7 @@ CM_D void push_secondary(const RunView<R>& v, const El<R>& pe, const R sd[3], R 
     return;
   }
   store_live(v.pool, slot, se);
+  job_start(v, pe.pixel, sink);
   ++sc.sec;
 }
 
@@ -448,7 +483,8 @@ template <typename R, int D, typename Sink> CM_D bool misc_apply(const RunView<R
     e.p[0] += kSmallDispNm * (double)e.d[0];
     e.p[1] += kSmallDispNm * (double)e.d[1];
     e.p[2] += kSmallDispNm * (double)e.d[2];
-    if (!shape_contains<R, D>(s, s.regions[e.region].shape, e.p)) e.region = containing_subregion<R, D>(s, s.chamber, e.p);
+    if (!shape_contains<R, D>(s, s.regions[e.region].shape, e.p))
+      e.region = containing_subregion<R, D>(s, chamber_of(v, e.pixel), e.p);
     return true;
   }
   if (kind == AUX_MECH) {
@@ -470,17 +506,20 @@ template <typename R, int D, typename Sink> CM_D bool misc_apply(const RunView<R
 template <typename R, typename Sink> CM_D void elastic_one(const RunView<R>& v, int cur, int j, Sink& sink) {
   El<R> e = load_event(v.w[cur], v.q[Q_EL][j]);
   if (elastic_apply(v, e)) keep(v, cur ^ 1, e, sink);
+  else job_end(v, e.pixel, e.step, sink);
 }
 
 template <typename R, typename Sink> CM_D void inelastic_one(const RunView<R>& v, int cur, int j, Sink& sink, StepCounts& sc) {
   El<R> e = load_event(v.w[cur], v.q[Q_TAB][j]);
   if (inelastic_apply(v, e, sink, sc)) keep(v, cur ^ 1, e, sink);
+  else job_end(v, e.pixel, e.step, sink);
 }
 
 template <typename R, int D, typename Sink>
 CM_D void misc_one(const RunView<R>& v, int cur, int j, Sink& sink, StepCounts& sc) {
   El<R> e = load(v.w[cur], v.q[Q_MISC][j]);
   if (misc_apply<R, D>(v, e, sink, sc)) keep(v, cur ^ 1, e, sink);
+  else job_end(v, e.pixel, e.step, sink);
 }
 
 // Up to nsteps whole steps (flight and event) of wave slot i in one thread, the survivor kept.  The
@@ -491,10 +530,13 @@ CM_D void steps_one(const RunView<R>& v, int cur, int i, int nsteps, Sink& sink,
   El<R> e = load_live(v.w[cur], i);
   for (int k = 0; k < nsteps; ++k) {
     const int q = flight_apply<R, D>(v, e, sink, sc);
-    if (q < 0) return;
-    const bool alive = q == Q_EL ? elastic_apply(v, e) : q == Q_TAB ? inelastic_apply(v, e, sink, sc)
-                                                                    : misc_apply<R, D>(v, e, sink, sc);
-    if (!alive) return;
+    const bool alive = q < 0 ? false
+                             : q == Q_EL ? elastic_apply(v, e)
+                                         : q == Q_TAB ? inelastic_apply(v, e, sink, sc) : misc_apply<R, D>(v, e, sink, sc);
+    if (!alive) {
+      job_end(v, e.pixel, e.step, sink);
+      return;
+    }
   }
   keep(v, cur ^ 1, e, sink);
 }
@@ -535,12 +577,13 @@ CM_D void spawn_one(const RunView<R>& v, int nxt, int j, int take_se, int poolTo
     else hi = mid;
   }
   const int px = lo;
+  if (io.job_stop && io.job_stop[io.pjob[px]]) return;  // a stopped job starts no more primaries
   const unsigned long long k = gi - io.prefix[px];
   El<R> e;
   e.key = mix64(io.pkey[px] + mix64(k + 1));
   Rng<R> g(e.key, 0xFFFFFFFFu, 0);
   const double u1 = (double)g.next(), u2 = (double)g.next();
-  const double r = sqrt(-2. * log(u1)) * io.width;
+  const double r = sqrt(-2. * log(u1)) * (io.pwidth ? io.pwidth[px] : io.width);
   const double th = 2.0 * kPi * u2;
   e.p[0] = io.pc[3 * px] + r * cos(th);
   e.p[1] = io.pc[3 * px + 1] + r * sin(th);
@@ -548,13 +591,14 @@ CM_D void spawn_one(const RunView<R>& v, int nxt, int j, int take_se, int poolTo
   e.d[0] = 0; e.d[1] = 0; e.d[2] = 1;
   e.E = (R)io.pe0[px];
   e.Ep = e.E;
-  e.region = containing_subregion<R, D>(v.s, v.s.chamber, e.p);
+  e.region = containing_subregion<R, D>(v.s, chamber_of(v, px), e.p);
   e.pixel = px;
   e.aux = 0;
   e.step = 0;
   e.h[0] = e.h[1] = e.h[2] = 0;
   const int seg = wave_segment(v.s, e.region, e.E);
   store_live(v.w[nxt], seg * v.W + v.c->nc[nxt][seg] + sink.append_q(v.c->ns, seg), e);
+  job_start(v, px, sink);
 }
 
 // end of an iteration: counters of the next wave, reset of this one (steps: the iteration ran k_steps)
@@ -571,12 +615,15 @@ CM_D void tail_update(Counters* c, int cur, int W, int poolCap, bool steps) {
     c->units[3] += (unsigned long long)c->q[2];
     c->iterations += 1;
   }
-  c->n[nxt] = nn + take_se + take_p;
+  (void)nn;
+  int appended = 0;  // survivors and refills as appended (a stopped job's primaries are not)
   for (int k = 0; k < kSegments; ++k) {
     c->nc[nxt][k] += c->ns[k];
     c->ns[k] = 0;
     c->nc[cur][k] = 0;
+    appended += c->nc[nxt][k];
   }
+  c->n[nxt] = appended;
   c->pool -= take_se;
   c->next_primary += (unsigned long long)take_p;
   c->n[cur] = 0;
