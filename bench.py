@@ -35,7 +35,8 @@ METRIC = "primary electrons/s at <=1% BSE/SE yield error vs FP64"
 WORKLOAD = ("linescan: 3 PMMA lines (h 100 nm, bottom w 40 nm, 3 deg, pitch 200 nm) on Si, 500 eV Gaussian "
             "sigma 1 nm, 256 px x 1 nm, 2000 primaries/px (512k primaries)")
 # served stream (latency line): jobs, mean arrival rate (1/s), server slots and budget, size scale
-SERVE_JOBS, SERVE_RATE, SERVE_SLOTS, SERVE_BUDGET_GB, SERVE_SCALE = 64, 8.0, 4, 16.0, 1 / 8
+SERVE_JOBS, SERVE_RATE, SERVE_SLOTS, SERVE_BUDGET_GB, SERVE_SCALE = 64, 8.0, 16, 16.0, 1 / 8
+IMAGE_REPEATS = 3  # runs per precision of the rough-line image
 BYTES_PER_STEP = 128  # algorithmic bytes per electron-step: a 64 B SoA record read and written
 
 
@@ -176,6 +177,11 @@ def main():
     ap.add_argument("--no-serving", action="store_true", help="skip the served-stream latency measurement")
     ap.add_argument("--no-image", action="store_true", help="skip the rough-line image (FP32 vs FP64)")
     ap.add_argument("--no-deep", action="store_true", help="skip the 10 keV deep-penetration layout")
+    ap.add_argument("--deep-side", type=int, default=128, help="pixels per side of the deep scan (full size 512)")
+    ap.add_argument("--deep-primaries", type=int, default=250, help="primaries per pixel of the deep scan (full 500)")
+    ap.add_argument("--serve-jobs", type=int, default=None, help="jobs in the served stream (full size 2000)")
+    ap.add_argument("--serve-scale", type=float, default=None, help="size scale of the served jobs (full size 1)")
+    ap.add_argument("--serve-rate", type=float, default=None, help="mean arrival rate of the served stream (1/s)")
     ap.add_argument("--no-autotune", action="store_true", help="run with the default launch settings")
     ap.add_argument("--profile-run", action="store_true",
                     help="run one FP32 step of the workload and exit (the case for ncu captures)")
@@ -191,6 +197,7 @@ def main():
     import torch.distributed as dist
     from datetime import timedelta
     from cudamonsel_b200 import capi, replicas, scenes
+    from cudamonsel_b200 import stats as ystats
 
     torch.cuda.set_device(local)
     if world > 1:
@@ -272,6 +279,28 @@ def main():
     b64, s64 = scenes.yields(back64.sum(0), prim_per_rank, BEAM_EV, NBINS)
     yerr = {"bse_fp32": float(b32[0]), "bse_fp64": float(b64[0]), "se_fp32": float(s32[0]), "se_fp64": float(s64[0]),
             "bse_rel_err": float(abs(b32[0] - b64[0]) / b64[0]), "se_rel_err": float(abs(s32[0] - s64[0]) / s64[0])}
+    # per pixel: the FP32 yields against LB independent FP64 batches of LN primaries per pixel (streams of
+    # their own), each pixel's variance from its batches; and the per-pixel difference from the FP64 run on
+    # the same streams
+    LB, LN = 8, 500
+    fb, fs = [], []
+    for r in range(LB):
+        kb = keys + np.uint64((r + 1) * 1_000_000_007)
+        bb, _, _ = eng.run(h["chamber"], centers, scenes.eV(BEAM_EV), LN, NBINS, 1e-9, 0, precision=capi.PREC_FP64,
+                           pixel_keys=kb)
+        yb = scenes.yields(bb, LN, BEAM_EV, NBINS)
+        fb.append(yb[0])
+        fs.append(yb[1])
+    pb32, ps32 = scenes.yields(back32, NPRIM, BEAM_EV, NBINS)
+    pb64, ps64 = scenes.yields(back64, NPRIM, BEAM_EV, NBINS)
+    yerr["per_pixel"] = {
+        "method": "FP32 run (2000/px) vs %d independent FP64 batches of %d/px; t per pixel as normal z" % (LB, LN),
+        "bse": ystats.z_summary(ystats.scan_z(np.array(fb), LN, pb32, NPRIM)),
+        "se": ystats.z_summary(ystats.scan_z(np.array(fs), LN, ps32, NPRIM)),
+        "same_streams_abs_err": {"bse_mean": float(np.abs(pb32 - pb64).mean()),
+                                 "bse_max": float(np.abs(pb32 - pb64).max()),
+                                 "se_mean": float(np.abs(ps32 - ps64).mean()),
+                                 "se_max": float(np.abs(ps32 - ps64).max())}}
 
     # end to end through the C ABI with host buffers: H2D of the pixel arrays, D2H of the tallies
     e2e_ms = 0.0
@@ -286,7 +315,8 @@ def main():
     d2h = 2 * NPIX * stride * 4
 
     steps_total = sum(s.steps for s in stats)
-    launches = sum(sum(int(x) for x in s.kernel_launches) + int(s.step_launches) for s in stats)
+    # the queue kernels, spawn and loop kernel of every iteration, the tail kernel, and the run's two gates
+    launches = sum(sum(int(x) for x in s.kernel_launches) + int(s.step_launches) + 2 for s in stats)
     # roofline of the dominant kernel: one more step of the same workload with CUDA events
     # between the kernels of every iteration (event nodes inside the captured graphs); the tail
     # iterations run k_steps ("steps" in the shares), the others the six queue kernels
@@ -329,56 +359,89 @@ def main():
                 tt = eimg.autotune(hi["chamber"], ic[band], ie[band], inp[band], inb[band], 1e-9, 0, precision=pr,
                                    pixel_keys=ikeys[band])
                 itune[name] = {k: v for k, v in tt.as_dict().items() if k != "ms"}
-        runs = {}
-        for name, pr in (("fp32", capi.PREC_FP32), ("fp64", capi.PREC_FP64)):
-            t0 = time.perf_counter()
-            ib, _, ist = eimg.run(hi["chamber"], ic, ie, inp, inb, 1e-9, 0, precision=pr, pixel_keys=ikeys)
-            runs[name] = (ib, ist, time.perf_counter() - t0)
+        # IMAGE_REPEATS runs per precision, each on streams of its own: throughput as the median with its
+        # spread, yields compared per pixel (pooled t over the repeats) and over the image
+        reps = {"fp32": [], "fp64": []}
+        ys = {"fp32": [], "fp64": []}
+        e_eV = ie / scenes.EV
+        for r in range(IMAGE_REPEATS):
+            for q, (name, pr) in enumerate((("fp32", capi.PREC_FP32), ("fp64", capi.PREC_FP64))):
+                kr = ikeys + np.uint64((2 * r + q + 1) * 1_000_000_007)
+                t0 = time.perf_counter()
+                ib, _, ist = eimg.run(hi["chamber"], ic, ie, inp, inb, 1e-9, 0, precision=pr, pixel_keys=kr)
+                reps[name].append((ist.device_ms, time.perf_counter() - t0, int(ist.steps)))
+                ys[name].append(scenes.yields(ib.astype(np.int64), np.maximum(inp, 1), e_eV, inb))
         eimg.close()
         ntot = int(inp.sum())
-        e_eV = ie / scenes.EV
-        y = {k: scenes.yields(v[0].astype(np.int64), np.maximum(inp, 1), e_eV, inb) for k, v in runs.items()}
+        rate = {k: [ntot / (m / 1e3) for m, _, _ in v] for k, v in reps.items()}
         err = {}
         for j, nm in ((0, "bse"), (1, "se")):
-            a32, a64 = (y["fp32"][j] * inp).sum() / ntot, (y["fp64"][j] * inp).sum() / ntot
+            m32 = [(y[j] * inp).sum() / ntot for y in ys["fp32"]]
+            m64 = [(y[j] * inp).sum() / ntot for y in ys["fp64"]]
+            z, a32, a64, se = ystats.pooled_z(m32, m64)
             err[nm + "_fp32"], err[nm + "_fp64"], err[nm + "_rel_err"] = a32, a64, abs(a32 - a64) / a64
+            err[nm + "_image_z"] = z
+            err[nm + "_per_pixel"] = ystats.z_summary(ystats.repeats_z(
+                [y[j] for y in ys["fp32"]], [y[j] for y in ys["fp64"]], nprim=np.maximum(inp, 1), groups=ie))
+        err["per_pixel_method"] = ("%d FP32 vs %d FP64 repeats on streams of their own; each pixel's variance "
+                                   "v(yield)/nprim, v pooled over the pixels of the same beam energy and mean-yield "
+                                   "quantile (32 bins)" % (IMAGE_REPEATS, IMAGE_REPEATS))
         image_line = {"workload": "rough lines 3 x 128 segments (sidewall offsets N(0, 1.5 nm)), 256 x 256 px at "
                                   "2 nm, Poisson(300)/px, E per row in {300, 500, 1000} eV",
-                      "primaries": ntot, "tuning": itune or "defaults",
-                      "fp32_primaries_per_s": ntot / (runs["fp32"][1].device_ms / 1e3),
-                      "fp64_primaries_per_s": ntot / (runs["fp64"][1].device_ms / 1e3),
-                      "fp32_over_fp64": runs["fp64"][1].device_ms / runs["fp32"][1].device_ms,
-                      "fp32_e2e_s": runs["fp32"][2], "fp64_e2e_s": runs["fp64"][2],
-                      "electron_steps_fp32": int(runs["fp32"][1].steps),
+                      "primaries": ntot, "tuning": itune or "defaults", "repeats": IMAGE_REPEATS,
+                      "fp32_primaries_per_s": statistics.median(rate["fp32"]),
+                      "fp64_primaries_per_s": statistics.median(rate["fp64"]),
+                      "fp32_primaries_per_s_range": [min(rate["fp32"]), max(rate["fp32"])],
+                      "fp64_primaries_per_s_range": [min(rate["fp64"]), max(rate["fp64"])],
+                      "fp32_over_fp64": statistics.median(rate["fp32"]) / statistics.median(rate["fp64"]),
+                      "fp32_over_fp64_worst": min(rate["fp32"]) / max(rate["fp64"]),
+                      "fp32_e2e_s": statistics.median(v[1] for v in reps["fp32"]),
+                      "fp64_e2e_s": statistics.median(v[1] for v in reps["fp64"]),
+                      "electron_steps_fp32": reps["fp32"][0][2],
                       "yield_error_vs_fp64": err}
 
-    # deep penetration: 16 x 16 seed-placed blocks and cylinders (PMMA or Si, 20-300 nm) on Si, 10 keV,
-    # a 64 x 64 scan at 80 nm over the 5.12 um layout, 100 primaries per pixel, FP32 against FP64
+    # deep penetration: 16 x 16 seed-placed blocks and cylinders (PMMA or Si, 20-300 nm) on Si, 10 keV, a
+    # --deep-side^2 scan over the 5.12 um layout, --deep-primaries per pixel, FP32 against FP64; the
+    # roofline of its dominant kernel from a profiled FP32 run of every second row and column
     deep_line = None
     if not a.no_deep:
         dsc, dtop = scenes.deep_features(seed=0)
         edeep = capi.Engine(local)
         hd = scenes.build_engine(dsc, edeep)
-        side, step = 64, 80e-9
-        xs = (np.arange(side) - (side - 1) / 2.0) * step
+        side, dprim = a.deep_side, a.deep_primaries
+        step_m = 5.12e-6 / side
+        xs = (np.arange(side) - (side - 1) / 2.0) * step_m
         gx, gy = np.meshgrid(xs, xs)
         dc = np.stack([gx.ravel(), gy.ravel(), np.full(side * side, -(dtop + 20e-9))], axis=1)
         dkeys = np.arange(side * side, dtype=np.uint64) + np.uint64(5_000_011 * (rank + 1))
         druns = {}
         for name, pr in (("fp32", capi.PREC_FP32), ("fp64", capi.PREC_FP64)):
-            db, _, dst = edeep.run(hd["chamber"], dc, scenes.eV(10000.0), 100, 1000, 1e-9, 0, precision=pr,
+            db, _, dst = edeep.run(hd["chamber"], dc, scenes.eV(10000.0), dprim, 1000, 1e-9, 0, precision=pr,
                                    pixel_keys=dkeys)
             druns[name] = (db, dst)
+        sub = (np.arange(side)[:, None] % 2 == 0) & (np.arange(side)[None, :] % 2 == 0)
+        sub = sub.ravel()
+        _, _, pst = edeep.run(hd["chamber"], dc[sub], scenes.eV(10000.0), dprim, 1000, 1e-9, 0,
+                              precision=capi.PREC_FP32, pixel_keys=dkeys[sub], profile=1)
         edeep.close()
-        y32 = scenes.yields(druns["fp32"][0].astype(np.int64), 100, 10000.0, 1000)
-        y64 = scenes.yields(druns["fp64"][0].astype(np.int64), 100, 10000.0, 1000)
-        nd = side * side * 100
-        deep_line = {"workload": "16 x 16 blocks/cylinders (PMMA or Si, 20-300 nm) on Si, 10 keV, 64 x 64 px at "
-                                 "80 nm, 100 primaries/px", "primaries": nd,
+        dk = int(np.argmax(list(pst.kernel_ms)[:4]))
+        dach = pst.units[dk] * BYTES_PER_STEP / (pst.kernel_ms[dk] / 1000.0) / 1e9
+        y32 = scenes.yields(druns["fp32"][0].astype(np.int64), dprim, 10000.0, 1000)
+        y64 = scenes.yields(druns["fp64"][0].astype(np.int64), dprim, 10000.0, 1000)
+        nd = side * side * dprim
+        deep_line = {"workload": "16 x 16 blocks/cylinders (PMMA or Si, 20-300 nm) on Si, 10 keV, %d x %d px at "
+                                 "%.0f nm, %d primaries/px" % (side, side, step_m * 1e9, dprim), "primaries": nd,
                      "fp32_primaries_per_s": nd / (druns["fp32"][1].device_ms / 1e3),
                      "fp64_primaries_per_s": nd / (druns["fp64"][1].device_ms / 1e3),
                      "fp32_over_fp64": druns["fp64"][1].device_ms / druns["fp32"][1].device_ms,
                      "electron_steps_fp32": int(druns["fp32"][1].steps),
+                     "electron_steps_per_s_fp32": druns["fp32"][1].steps / (druns["fp32"][1].device_ms / 1e3),
+                     "roofline": {"bound": "hbm", "kernel": names[dk], "achieved": dach, "peak": peak,
+                                  "unit": "GB/s", "frac": dach / peak, "peak_kind": peak_kind,
+                                  "sample": "profiled FP32 run of every 2nd row and column",
+                                  "kernel_ms_share": dict({n: float(v / (sum(pst.kernel_ms) + pst.step_ms))
+                                                           for n, v in zip(names, pst.kernel_ms)},
+                                                          steps=float(pst.step_ms / (sum(pst.kernel_ms) + pst.step_ms)))},
                      "yield_error_map_vs_fp64": {
                          "bse_mean_abs": float(np.abs(y32[0] - y64[0]).mean()),
                          "bse_max_abs": float(np.abs(y32[0] - y64[0]).max()),
@@ -398,16 +461,30 @@ def main():
     serving_line = None
     if not a.no_serving:
         from cudamonsel_b200 import serving
-        js = serving.make_jobs(SERVE_JOBS, seed=100 + rank, scale=SERVE_SCALE)
-        out = serving.serve(js, rate_per_s=SERVE_RATE, slots=SERVE_SLOTS, budget_gb=SERVE_BUDGET_GB, seed=200 + rank,
+        njobs = a.serve_jobs or SERVE_JOBS
+        sscale = a.serve_scale or SERVE_SCALE
+        srate = a.serve_rate or SERVE_RATE
+        js = serving.make_jobs(njobs, seed=100 + rank, scale=sscale)
+        out = serving.serve(js, rate_per_s=srate, slots=SERVE_SLOTS, budget_gb=SERVE_BUDGET_GB, seed=200 + rank,
                             device=local)
         lat = out["latency"]
-        serving_line = {"jobs": SERVE_JOBS, "rate_per_s": SERVE_RATE, "slots": SERVE_SLOTS,
-                        "budget_gb": SERVE_BUDGET_GB, "size_scale": SERVE_SCALE,
+        # the same jobs submitted all at once (the server saturated), FP32 and FP64: served throughput
+        sat = {}
+        for name, pr in (("fp32", capi.PREC_FP32), ("fp64", capi.PREC_FP64)):
+            o = serving.serve(js, rate_per_s=None, slots=SERVE_SLOTS, budget_gb=SERVE_BUDGET_GB, precision=pr,
+                              device=local)
+            sat[name] = {"primaries_per_s": o["primaries"] / o["makespan"],
+                         "electron_steps_per_s": o["steps"] / o["makespan"], "makespan_s": o["makespan"],
+                         "p50_s": float(np.percentile(o["latency"], 50)),
+                         "p99_s": float(np.percentile(o["latency"], 99))}
+        sat["fp32_over_fp64"] = sat["fp32"]["primaries_per_s"] / sat["fp64"]["primaries_per_s"]
+        serving_line = {"jobs": njobs, "rate_per_s": srate, "slots": SERVE_SLOTS,
+                        "budget_gb": SERVE_BUDGET_GB, "size_scale": sscale,
                         "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
                         "makespan_s": out["makespan"], "primaries": out["primaries"],
                         "primaries_per_s": out["primaries"] / out["makespan"],
-                        "electron_steps_per_s": out["steps"] / out["makespan"]}
+                        "electron_steps_per_s": out["steps"] / out["makespan"],
+                        "saturated": sat}
 
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:

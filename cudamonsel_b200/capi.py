@@ -31,7 +31,7 @@ EXPORTS = (
     "cm_msm_set_min_e", "cm_msm_set_barrier", "cm_shape_sphere", "cm_shape_planes", "cm_shape_intersection",
     "cm_shape_union", "cm_shape_cylinder", "cm_shape_translate", "cm_shape_rotate", "cm_shape_line", "cm_region_add", "cm_run", "cm_run_device", "cm_run_noalloc",
     "cm_eval_nistmott", "cm_eval_table", "cm_eval_locate", "cm_eval_pick", "cm_eval_tabulated", "cm_eval_elastic", "cm_eval_csd", "cm_eval_phonon",
-    "cm_eval_shape", "cm_eval_barrier", "cm_eval_freepath", "cm_server_create", "cm_server_destroy", "cm_job_submit",
+    "cm_eval_shape", "cm_eval_barrier", "cm_eval_freepath", "cm_server_create", "cm_server_tune", "cm_server_destroy", "cm_job_submit",
     "cm_job_poll", "cm_job_wait", "cm_job_cancel", "cm_job_result", "cm_get_tuning", "cm_set_tuning", "cm_autotune",
 )
 
@@ -56,7 +56,7 @@ ESCAPE_RECORD = np.dtype([("electron", np.uint64), ("pixel", np.int32), ("step",
 
 class Tuning(C.Structure):
     _fields_ = [("wave", C.c_int), ("tail_below", C.c_int), ("tail_steps", C.c_int), ("blocks_per_sm", C.c_int),
-                ("ms", C.c_double)]
+                ("ms", C.c_double), ("pool", C.c_int)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -73,7 +73,7 @@ class RunStats(C.Structure):
                 ("iterations", C.c_int64), ("device_ms", C.c_double), ("kernel_ms", C.c_double * 6),
                 ("kernel_launches", C.c_int64 * 6), ("units", C.c_int64 * 4), ("step_launches", C.c_int64),
                 ("step_units", C.c_int64), ("step_ms", C.c_double), ("ended_zero_energy", C.c_int64),
-                ("ended_step_limit", C.c_int64)]
+                ("ended_step_limit", C.c_int64), ("pool_restarts", C.c_int64)]
 
     KERNELS = ("flight", "elastic", "inelastic", "misc", "spawn", "tail")
 
@@ -87,6 +87,7 @@ class RunStats(C.Structure):
         d["step_ms"] = self.step_ms
         d["ended_zero_energy"] = self.ended_zero_energy
         d["ended_step_limit"] = self.ended_step_limit
+        d["pool_restarts"] = self.pool_restarts
         return d
 
 
@@ -144,6 +145,7 @@ def load(path=LIBPATH):
         "cm_run_device": [ctx, C.POINTER(RunDesc), C.c_void_p, C.c_void_p, C.POINTER(RunStats), C.c_void_p],
         "cm_run_noalloc": [ctx, C.POINTER(RunDesc), C.c_void_p, C.c_void_p, C.POINTER(RunStats), C.c_void_p],
         "cm_server_create": [C.c_int, C.c_int, C.c_double, C.POINTER(C.c_void_p)],
+        "cm_server_tune": [C.c_void_p, C.c_int, C.POINTER(Tuning)],
         "cm_server_destroy": [C.c_void_p],
         "cm_job_submit": [C.c_void_p, ctx, C.POINTER(RunDesc), i],
         "cm_job_poll": [C.c_void_p, C.c_int, C.POINTER(JobInfo)],
@@ -225,8 +227,8 @@ class Engine:
         self._check(self.L.cm_get_tuning(self.h, precision, C.byref(t)))
         return t
 
-    def set_tuning(self, precision=PREC_FP64, wave=0, tail_below=0, tail_steps=0, blocks_per_sm=0):
-        t = Tuning(wave, tail_below, tail_steps, blocks_per_sm, 0.0)
+    def set_tuning(self, precision=PREC_FP64, wave=0, tail_below=0, tail_steps=0, blocks_per_sm=0, pool=0):
+        t = Tuning(wave, tail_below, tail_steps, blocks_per_sm, 0.0, pool)
         self._check(self.L.cm_set_tuning(self.h, precision, C.byref(t)))
 
     def autotune(self, chamber, centers, energies, nprim, nbins, beam_width, seed, precision=PREC_FP64,
@@ -447,7 +449,7 @@ def _run_desc(chamber, centers, energies, nprim, nbins, beam_width, seed, precis
 
 
 class Server:
-    """cm_server: a job server with `slots` resident engine contexts on one GPU."""
+    """cm_server: a continuously batching job server on one GPU; up to `slots` jobs share a batch."""
 
     def __init__(self, device=0, slots=4, budget_gb=16.0):
         self.L = load()
@@ -482,6 +484,11 @@ class Server:
         self._check(self.L.cm_job_submit(self.h, engine.h, C.byref(desc), C.byref(job)))
         self.shape[job.value] = (npix, stride)
         return job.value
+
+    def tune(self, precision, wave=0, tail_below=0, tail_steps=0, blocks_per_sm=0, pool=0):
+        """Launch settings of the batches of one precision that start after the call (0 = default)."""
+        t = Tuning(wave, tail_below, tail_steps, blocks_per_sm, 0.0, pool)
+        self._check(self.L.cm_server_tune(self.h, precision, C.byref(t)))
 
     def poll(self, job):
         info = JobInfo()

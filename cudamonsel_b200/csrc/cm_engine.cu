@@ -1147,6 +1147,15 @@ static int ensure_buffers(cm_context* ctx, int W, int poolCap) {
   return 0;
 }
 
+// Secondary-pool records for a wave of W electrons and beams of up to emax_eV.  A wave full of primaries
+// creates about one tracked secondary per 20 eV of their energy before it drains (the refill takes new
+// primaries only into an empty pool), so the pool grows with the beam energy: 8 W at 1 keV and below, up
+// to 64 W (factor > 0: factor W).  What this does not cover, the overflow restart does (it doubles the pool).
+static int pool_records(int W, double emax_eV, int factor) {
+  const double f = factor > 0 ? (double)factor : std::min(64.0, std::max(8.0, 8.0 * emax_eV / 1000.0));
+  return (int)std::min<double>(f * (double)W, (double)(1 << 30));
+}
+
 // iterations of a loop body (an even number: the waves alternate)
 constexpr int kLoopBody = 16;
 
@@ -1285,15 +1294,18 @@ template <typename R> static void dump_live(const RunBuffers<R>& rb, const Count
 template <typename R>
 static int run_device_once(cm_context* ctx, const cm_run_desc* d, uint32_t* back, uint32_t* fwd, cm_run_stats* st,
                       cudaStream_t stream, const unsigned long long* prefix_dev, const double* e0ref_dev,
-                      const unsigned long long* pkey_dev, unsigned long long total) {
+                      const unsigned long long* pkey_dev, unsigned long long total, double emax_eV) {
   int rc;
   DevScene<R>& ds = scene_of<R>(ctx);
   if ((rc = build_scene<R>(ctx, ds))) return rc;
   const cm_tuning tu = resolved_tuning<R>(ctx);
   const int W = d->wave > 0 ? d->wave : tu.wave;
   RunBuffers<R>& rb0 = buffers_of<R>(ctx);
-  const int poolWant = rb0.cap == W && rb0.poolCap > 8 * W ? rb0.poolCap : 8 * W;
-  if ((rc = ensure_buffers<R>(ctx, W, poolWant))) return rc;
+  const int poolWant = std::max(pool_records(W, emax_eV, tu.pool), rb0.cap == W ? rb0.poolCap : 0);
+  if ((rc = ensure_buffers<R>(ctx, W, poolWant))) {
+    // a pool sized for the beam energy that the device cannot hold: the smallest one (restarts grow it)
+    if (rc != CM_ENOMEM || poolWant <= 8 * W || (rc = ensure_buffers<R>(ctx, W, 8 * W))) return rc;
+  }
   RunBuffers<R>& rb = buffers_of<R>(ctx);
   RunView<R> v;
 #ifdef CM_TRACE
@@ -1486,11 +1498,13 @@ static int clear_angles(const cm_run_desc* d, cudaStream_t s) {
 template <typename R>
 static int run_device(cm_context* ctx, const cm_run_desc* d, uint32_t* back, uint32_t* fwd, cm_run_stats* st,
                       cudaStream_t stream, const unsigned long long* prefix_dev, const double* e0ref_dev,
-                      const unsigned long long* pkey_dev, unsigned long long total) {
+                      const unsigned long long* pkey_dev, unsigned long long total, double emax_eV) {
   const size_t hbytes = (size_t)d->npix * d->hist_stride * sizeof(uint32_t);
   int rc_clear;
-  for (int attempt = 0; attempt < 4; ++attempt) {
-    const int rc = run_device_once<R>(ctx, d, back, fwd, st, stream, prefix_dev, e0ref_dev, pkey_dev, total);
+  for (int attempt = 0;; ++attempt) {
+    const int rc =
+        run_device_once<R>(ctx, d, back, fwd, st, stream, prefix_dev, e0ref_dev, pkey_dev, total, emax_eV);
+    if (st) st->pool_restarts = attempt;
     if (rc != CM_EOVERFLOW) return rc;
     RunBuffers<R>& rb = buffers_of<R>(ctx);
     const int W = rb.cap;
@@ -1502,7 +1516,6 @@ static int run_device(cm_context* ctx, const cm_run_desc* d, uint32_t* back, uin
     CM_CUDA(cudaMemsetAsync(fwd, 0, hbytes, stream));
     if ((rc_clear = clear_angles(d, stream))) return rc_clear;
   }
-  return fail(CM_EOVERFLOW, "secondary pool overflow");
 }
 
 // ------------------------------------------------------------------ per-function kernels
@@ -1765,6 +1778,7 @@ int cm_set_tuning(cm_context* ctx, int precision, const cm_tuning* t) {
   if (t->tail_below < 0) return fail(CM_EINVAL, "tail_below < 0");
   if (t->tail_steps < 0 || t->tail_steps > 4096) return fail(CM_EINVAL, "tail_steps out of range");
   if (t->blocks_per_sm < 0 || t->blocks_per_sm > 32) return fail(CM_EINVAL, "blocks_per_sm out of range");
+  if (t->pool < 0 || t->pool > 64) return fail(CM_EINVAL, "pool out of range");
   ctx->tune[precision] = *t;
   return 0;
 }
@@ -2319,9 +2333,10 @@ static int run_common(cm_context* ctx, const cm_run_desc* d, const double* cente
   dd.pixel_center = c_dev;
   dd.pixel_energy = e0_dev;
   dd.pixel_nbins = nbins_dev;
+  const double emax = p.e0.empty() ? 0.0 : *std::max_element(p.e0.begin(), p.e0.end());
   rc = d->precision == CM_PREC_FP64
-           ? run_device<double>(ctx, &dd, back_dev, fwd_dev, st, stream, prefix_dev, e0ref_dev, key_dev, p.total)
-           : run_device<float>(ctx, &dd, back_dev, fwd_dev, st, stream, prefix_dev, e0ref_dev, key_dev, p.total);
+           ? run_device<double>(ctx, &dd, back_dev, fwd_dev, st, stream, prefix_dev, e0ref_dev, key_dev, p.total, emax)
+           : run_device<float>(ctx, &dd, back_dev, fwd_dev, st, stream, prefix_dev, e0ref_dev, key_dev, p.total, emax);
   cudaStreamSynchronize(stream);
   for (void* a : allocs) cudaFree(a);
   return rc;

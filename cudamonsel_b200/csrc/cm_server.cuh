@@ -185,6 +185,9 @@ struct Batcher {
   unsigned long long total = 0;
   size_t tally_used = 0;
   bool counters_live = false;  // the device counters describe the current batch
+  int pool_want = 0;           // secondary-pool records to ask for (doubled after an overflow)
+  double emax_eV = 0;          // highest beam energy of the batch's jobs
+  int restarts = 0;            // restarts of the current batch after overflows
   std::vector<JobRecord*> active;
   // captured rounds of iterations for the current scene build and run buffers
   cudaGraphExec_t round_exec[2] = {nullptr, nullptr};
@@ -225,6 +228,7 @@ struct cm_server {
   std::deque<int> queue;  // admission order
   std::map<int, std::unique_ptr<cm::JobRecord>> jobs;
   std::map<std::pair<int, int>, std::unique_ptr<cm::Batcher>> batchers;  // by (precision, options)
+  cm_tuning tune[2] = {};                                                 // per precision, for new batches
   int next_id = 0;
   bool stop = false;
   std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
@@ -266,6 +270,7 @@ static int batch_add(Batcher& b, JobRecord& j) {
       (rc = b.job_steps.reserve(b.slots + 1)) || (rc = b.job_stop.reserve(b.slots + 1)))
     return rc;
   const int chamber = merge_scene(ctx, j);
+  for (double e : p.e0) b.emax_eV = std::max(b.emax_eV, e);
   j.slot = b.slots++;
   j.g0 = b.total;
   j.g1 = b.total + p.total;
@@ -314,8 +319,16 @@ static int batch_round(Batcher& b) {
   const cm_tuning tu = resolved_tuning<R>(ctx);
   const int W = tu.wave;
   RunBuffers<R>& rb0 = buffers_of<R>(ctx);
-  const int poolWant = rb0.cap == W && rb0.poolCap > 8 * W ? rb0.poolCap : 8 * W;
-  if ((rc = ensure_buffers<R>(ctx, W, poolWant))) return rc;
+  if (b.counters_live) {
+    // within a batch the buffers hold its electrons: they stay as they are (the launch settings and the
+    // pool are chosen when the batch starts; an overflow restarts the batch with a larger pool)
+    if (rb0.cap != W) return fail(CM_ESTATE, "job server: run buffers changed within a batch");
+  } else {
+    const int poolWant = std::max({pool_records(W, b.emax_eV, tu.pool), b.pool_want, rb0.cap == W ? rb0.poolCap : 0});
+    if ((rc = ensure_buffers<R>(ctx, W, poolWant))) {
+      if (rc != CM_ENOMEM || poolWant <= 8 * W || (rc = ensure_buffers<R>(ctx, W, 8 * W))) return rc;
+    }
+  }
   RunBuffers<R>& rb = buffers_of<R>(ctx);
   cudaStream_t s = ctx->stream;
   RunView<R> v;
@@ -363,6 +376,12 @@ static int batch_round(Batcher& b) {
     hc.total_primaries = b.total;
     hc.done = 0;
   }
+  // several whole steps per thread (the tail kernels) whenever fewer electrons are in the wave and pool than
+  // fill the GPU, even with primaries still to start; the refill then fills the wave only up to that many,
+  // so a light load runs at the latency of a job alone and a heavy one through the queue kernels
+  const long long left = (long long)hc.n[0] + hc.n[1] + std::min(hc.pool, v.poolCap);
+  const bool tail = !(ctx->options & CM_OPT_QUEUE_STEPS) && left < tu.tail_below;
+  hc.fill = tail ? std::min(W, tu.tail_below) : 0;
   CM_CUDA(cudaMemcpyAsync(ctx->counters, &hc, sizeof(Counters), cudaMemcpyHostToDevice, s));
   const int grid = ctx->nsm * tu.blocks_per_sm;
   v.s.nstaged = 0;
@@ -386,9 +405,6 @@ static int batch_round(Batcher& b) {
     b.round_buffers = (const void*)rb.w[0].px;
     b.round_pool = rb.poolCap;
   }
-  const long long left = (long long)hc.n[0] + hc.n[1] + std::min(hc.pool, v.poolCap);
-  const bool tail = !(ctx->options & CM_OPT_QUEUE_STEPS) && hc.next_primary == hc.total_primaries &&
-                    left < tu.tail_below;
   CM_CUDA(cudaGraphLaunch(b.round_exec[tail ? 1 : 0], s));
   CM_CUDA(cudaMemcpyAsync(&hc, ctx->counters, sizeof(Counters), cudaMemcpyDeviceToHost, s));
   CM_CUDA(cudaStreamSynchronize(s));
@@ -425,6 +441,27 @@ static int batch_collect(Batcher& b, std::vector<JobRecord*>& finished) {
   return 0;
 }
 
+static void batch_reset(Batcher& b);
+
+// The batch overflowed its secondary pool (a secondary was lost, so its tallies are void).  Every electron's
+// random stream is keyed by its lineage, so the batch's jobs are run again from their start with twice the
+// pool and give the tallies an unbounded pool would have given.
+static int batch_restart(Batcher& b) {
+  if (2LL * std::max(b.pool_want, b.round_pool) > (1LL << 30))
+    return fail(CM_EOVERFLOW, "job server: secondary pool overflow with a pool of 2^30 records");
+  b.pool_want = 2 * std::max(b.pool_want, b.round_pool);
+  const std::vector<JobRecord*> again = b.active;
+  batch_reset(b);
+  ++b.restarts;
+  b.active = again;  // a job that cannot be added again fails with the batch
+  for (JobRecord* j : again) {
+    j->stop_sent = false;
+    const int rc = batch_add(b, *j);
+    if (rc) return rc;
+  }
+  return 0;
+}
+
 // the batch ran empty: its scene and tables are dropped
 static void batch_reset(Batcher& b) {
   cm_context_reset(b.ctx);
@@ -433,6 +470,7 @@ static void batch_reset(Batcher& b) {
   b.slots = 0;
   b.total = 0;
   b.tally_used = 0;
+  b.emax_eV = 0;
   b.counters_live = false;
   b.drop_rounds();
 }
@@ -468,6 +506,10 @@ static void batcher_worker(cm_server* srv, Batcher* b) {
       }
     }
     int rc = 0;
+    if (b->slots == 0 && !admitted.empty()) {  // a new batch takes the server's current launch settings
+      std::lock_guard<std::mutex> lk(srv->mu);
+      b->ctx->tune[b->precision] = srv->tune[b->precision];
+    }
     std::vector<JobRecord*> added;
     for (JobRecord* j : admitted) {
       if (rc == 0) rc = batch_add(*b, *j);
@@ -480,12 +522,14 @@ static void batcher_worker(cm_server* srv, Batcher* b) {
     if (rc == 0 && !b->active.empty())
       rc = b->precision == CM_PREC_FP64 ? batch_round<double>(*b) : batch_round<float>(*b);
     if (rc == 0 && b->ctx->counters_host->error) rc = run_error(b->ctx->counters_host->error, *b->ctx->counters_host);
+    if (rc == CM_EOVERFLOW) rc = batch_restart(*b);
     if (rc == 0) rc = batch_collect(*b, finished);
     const std::string msg = rc ? cm_last_error() : "";
     {
       std::lock_guard<std::mutex> lk(srv->mu);
       const double t = srv->now();
       for (JobRecord* j : finished) {
+        j->stats.pool_restarts = b->restarts;
         srv->in_use -= j->footprint;
         j->t_end = t;
         j->state = j->cancel.load() ? CM_JOB_CANCELLED : CM_JOB_DONE;
@@ -509,7 +553,10 @@ static void batcher_worker(cm_server* srv, Batcher* b) {
       srv->cv_done.notify_all();
       srv->cv_work.notify_all();
     }
-    if (b->active.empty()) batch_reset(*b);
+    if (b->active.empty()) {
+      batch_reset(*b);
+      b->restarts = 0;
+    }
   }
 }
 
@@ -527,6 +574,19 @@ int cm_server_create(int device, int slots, double budget_gb, cm_server** out) {
   srv->max_active = slots;
   srv->budget = (size_t)(budget_gb * 1e9);
   *out = srv.release();
+  return 0;
+}
+
+int cm_server_tune(cm_server* srv, int precision, const cm_tuning* t) {
+  if (!srv || !t) return fail(CM_EINVAL, "null argument");
+  if (precision != CM_PREC_FP64 && precision != CM_PREC_FP32) return fail(CM_EINVAL, "bad precision");
+  if (t->wave < 0 || (t->wave > 0 && (t->wave < 1024 || t->wave > (1 << 24)))) return fail(CM_EINVAL, "wave out of range");
+  if (t->tail_below < 0) return fail(CM_EINVAL, "tail_below < 0");
+  if (t->tail_steps < 0 || t->tail_steps > 4096) return fail(CM_EINVAL, "tail_steps out of range");
+  if (t->blocks_per_sm < 0 || t->blocks_per_sm > 32) return fail(CM_EINVAL, "blocks_per_sm out of range");
+  if (t->pool < 0 || t->pool > 64) return fail(CM_EINVAL, "pool out of range");
+  std::lock_guard<std::mutex> lk(srv->mu);
+  srv->tune[precision] = *t;
   return 0;
 }
 

@@ -38,6 +38,7 @@ struct Counters {
   unsigned long long logged;      // escapes offered to the escape log
   unsigned long long slots, tail_slots;  // iteration slots the device-driven loop ran (all, tail)
   unsigned long long ended_zero, ended_limit;  // electrons ended by the zero-energy cut, by the step limit
+  int fill;  // the refill fills the wave up to this many electrons (0: W); set by the job server's tail rounds
 };
 
 template <typename R>
@@ -546,7 +547,8 @@ CM_D void steps_one(const RunView<R>& v, int cur, int i, int nsteps, Sink& sink,
 // cascades of one batch of primaries do not all peak together
 CM_D void refill_plan(const Counters* c, int nxt, int W, int poolCap, int& nn, int& take_se, int& take_p) {
   nn = survivors(c, nxt);
-  const int room = W - nn > 0 ? W - nn : 0;
+  const int cap = c->fill > 0 && c->fill < W ? c->fill : W;
+  const int room = cap - nn > 0 ? cap - nn : 0;
   const int pool = c->pool < poolCap ? c->pool : poolCap;  // an overflowed pool holds poolCap valid entries
   take_se = pool < room ? pool : room;
   const unsigned long long rem = c->total_primaries - c->next_primary;

@@ -90,10 +90,11 @@ def submit(server, holder, job, precision=capi.PREC_FP32):
 
 
 def serve(jobs, rate_per_s, slots=4, budget_gb=16.0, seed=1, precision=capi.PREC_FP32, device=0):
-    """Submit `jobs` at Poisson arrival times (mean rate_per_s) to a fresh server, wait for all of them;
-    returns per-job latencies (end - submit, s), makespan (s), primaries and electron-steps."""
+    """Submit `jobs` at Poisson arrival times (mean rate_per_s; None: all at once, which saturates the
+    server) to a fresh server, wait for all of them; returns per-job latencies (end - submit, s), makespan
+    (first submission to last end, s), primaries and electron-steps."""
     rng = np.random.default_rng(seed)
-    gaps = rng.exponential(1.0 / rate_per_s, len(jobs))
+    gaps = rng.exponential(1.0 / rate_per_s, len(jobs)) if rate_per_s else np.zeros(len(jobs))
     server = capi.Server(device, slots, budget_gb)
     holder = capi.Engine(device)
     ids = []
@@ -106,12 +107,18 @@ def serve(jobs, rate_per_s, slots=4, budget_gb=16.0, seed=1, precision=capi.PREC
             time.sleep(wait)
         ids.append(submit(server, holder, job, precision))
     infos = [server.wait(j) for j in ids]
-    bad = [i.state for i in infos if i.state != capi.JOB_DONE]
+    bad = [(j, i.state) for j, i in zip(ids, infos) if i.state != capi.JOB_DONE]
     results = [server.result(j) for j in ids] if not bad else []
+    why = ""
+    if bad:
+        try:
+            server.result(bad[0][0])
+        except capi.CMError as e:
+            why = str(e)
     server.close()
     holder.close()
     if bad:
-        raise capi.CMError("jobs did not complete: states %s" % bad)
+        raise capi.CMError("%d jobs did not complete (states %s): %s" % (len(bad), sorted({s for _, s in bad}), why))
     lat = np.array([i.end_s - i.submit_s for i in infos])
     first = min(i.submit_s for i in infos)
     makespan = max(i.end_s for i in infos) - first

@@ -150,3 +150,54 @@ def scan_z(a_batches, na, b_mean, nb):
     se = np.sqrt(v * (1.0 / B + na / float(nb)))
     t = (a.mean(0) - np.asarray(b_mean, dtype=np.float64)) / np.maximum(se, 1e-300)
     return t_to_z(t, B - 1)
+
+
+def repeats_z(a_runs, b_runs, nprim=None, groups=None, bins=32):
+    """Per-pixel z between two sets of independent repeats of the same scan: a_runs[Ra, npix] and
+    b_runs[Rb, npix] are per-pixel yields of runs on streams of their own (equal primaries per pixel
+    within a pixel).
+
+    Without nprim, each pixel's variance is pooled from its own repeats (Ra + Rb - 2 degrees of freedom)
+    and z is the normal equivalent of the pooled t statistic.  With few repeats of counts that take few
+    values this is fragile: repeats that happen to give the same count make the variance estimate zero.
+    With nprim[npix], a pixel's variance is instead v(y) / nprim, the per-primary variance v taken as the
+    mean of the pixels' own estimates (variance x nprim) over the pixels whose mean yield falls in the
+    same of `bins` quantile bins (within the same group, e.g. the same beam energy, when groups[npix] is
+    given): pixels of the same yield share a variance, estimated from thousands of degrees of freedom,
+    and z is normal."""
+    a = np.asarray(a_runs, dtype=np.float64)
+    b = np.asarray(b_runs, dtype=np.float64)
+    ra, rb = a.shape[0], b.shape[0]
+    ma, mb = a.mean(0), b.mean(0)
+    dof = ra + rb - 2
+    var = (((a - ma) ** 2).sum(0) + ((b - mb) ** 2).sum(0)) / dof
+    d = ma - mb
+    if nprim is None:
+        se = np.sqrt(var * (1.0 / ra + 1.0 / rb))
+        t = np.where(se > 0, d / np.where(se > 0, se, 1.0), np.where(d == 0, 0.0, np.sign(d) * 1e300))
+        return t_to_z(t, dof)
+    n = np.broadcast_to(np.asarray(nprim, dtype=np.float64), d.shape)
+    per_primary = var * n
+    m = (ma * ra + mb * rb) / (ra + rb)
+    g = np.zeros(d.shape, dtype=np.int64) if groups is None else np.unique(np.asarray(groups), return_inverse=True)[1]
+    model = np.empty_like(per_primary)
+    for k in np.unique(g):
+        sel = np.nonzero(g == k)[0]
+        edges = np.quantile(m[sel], np.linspace(0.0, 1.0, bins + 1))
+        idx = np.clip(np.searchsorted(edges, m[sel], side="right") - 1, 0, bins - 1)
+        cnt = np.bincount(idx, minlength=bins)
+        mean = np.bincount(idx, weights=per_primary[sel], minlength=bins) / np.maximum(cnt, 1)
+        model[sel] = mean[idx]
+    se = np.sqrt(model / n * (1.0 / ra + 1.0 / rb))
+    return np.where(se > 0, d / np.where(se > 0, se, 1.0), 0.0)
+
+
+def z_summary(z):
+    """What a per-pixel z map says: largest |z|, pixels beyond 3 and beyond the family-wise bound of
+    3 standard errors for this many pixels, and the chi-squared of the sum of z^2."""
+    z = np.asarray(z, dtype=np.float64).ravel()
+    bound = family_z_bound(len(z))
+    c, dof, p = chi2_of_z(z)
+    return {"pixels": int(len(z)), "max_abs_z": float(np.abs(z).max()), "over_3": int((np.abs(z) > 3).sum()),
+            "family_bound": bound, "over_family_bound": int((np.abs(z) > bound).sum()), "chi2": c, "dof": dof,
+            "chi2_p": p}

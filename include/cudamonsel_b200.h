@@ -72,6 +72,9 @@ typedef struct {
   int tail_steps;              /* whole steps per thread and launch in the tail (default 32) */
   int blocks_per_sm;           /* grid = SMs x blocks_per_sm blocks of 256 threads (default 8) */
   double ms;                   /* cm_autotune: device time of the transport loop under these settings */
+  int pool;                    /* secondary-pool records per wave electron (default by the highest beam
+                                  energy: 8 at 1 keV and below, 8 per keV above, up to 64; 1 .. 64); a run
+                                  that overflows the pool is run again with twice the pool */
 } cm_tuning;
 int cm_get_tuning(cm_context* ctx, int precision, cm_tuning* out);
 int cm_set_tuning(cm_context* ctx, int precision, const cm_tuning* tuning);
@@ -221,6 +224,9 @@ typedef struct {
                                   ended after 4096 steps (each one only bounces between barriers) */
   int64_t ended_step_limit;    /* electrons ended by the reference's 10^6-step limit
                                   (MONSEL_MaterialScatterModel.cu:86-90) */
+  int64_t pool_restarts;       /* times the run (a job: its batch) overflowed the secondary pool and was
+                                  run again from its start with twice the pool; the tallies are those of
+                                  a run with a large enough pool */
 } cm_run_stats;
 
 /* back/fwd: [npix * hist_stride] counts, index = histogram bin + 1 (0 = underflow,
@@ -261,15 +267,20 @@ int cm_run_noalloc(cm_context* ctx, const cm_run_desc* desc_device_arrays, uint3
 
 /* ---- job server: streams of scan jobs --------------------------------------
  * The reference runs one LinesOnLayers scan at a time on one thread
- * (JMONSELTests/LinesOnLayers.cu:327-398).  A server keeps `slots` engine
- * contexts resident on one GPU (own stream, scene, waves and pixel buffers) and
- * starts queued jobs first in, first out as soon as a slot is free and the
- * job's pixel and tally buffers fit in `budget_gb` beside the running jobs';
- * slots run concurrently, so jobs that arrive while others are on the GPU
- * overlap with them.  A job is a scene (copied from `scene` at submission, which
- * the caller may then reuse) and a run description with HOST arrays (copied).
- * Its tallies depend only on its scene, pixels and stream keys: the same alone
- * and in any mix. */
+ * (JMONSELTests/LinesOnLayers.cu:327-398).  A server batches jobs continuously
+ * on one GPU: the jobs of one precision and set of run options share one
+ * resident wave of electrons, one merged scene (each job's chamber and regions
+ * appended; tables, materials and scatter models shared when equal) and one set
+ * of pixel tables and tallies.  Queued jobs are admitted first in, first out
+ * while fewer than `slots` jobs are in their batch and the job's pixel and
+ * tally buffers fit in `budget_gb` beside the running jobs'; an admitted job's
+ * primaries join the wave as soon as those of the jobs before it have started,
+ * so jobs that arrive while others are on the GPU fill the room their ending
+ * cascades leave.  A job is done when its primaries have started and its
+ * electrons have all ended.  A job is a scene (copied from `scene` at
+ * submission, which the caller may then reuse) and a run description with HOST
+ * arrays (copied; energy histograms only).  Its tallies depend only on its
+ * scene, pixels and stream keys: the same alone, in any mix and through cm_run. */
 typedef struct cm_server cm_server;
 
 #define CM_JOB_QUEUED 0
@@ -286,13 +297,17 @@ typedef struct {
 } cm_job_info;
 
 int cm_server_create(int device, int slots, double budget_gb, cm_server** out);
-/* cancels running jobs at their next graph boundary, waits for the slots, frees everything */
+/* launch settings (as cm_set_tuning) of the server's batches of one precision, taken by the batches that
+ * start after the call */
+int cm_server_tune(cm_server* server, int precision, const cm_tuning* tuning);
+/* stops the batches after their current round of iterations and frees everything */
 int cm_server_destroy(cm_server* server);
 int cm_job_submit(cm_server* server, const cm_context* scene, const cm_run_desc* desc, int* out_job);
 int cm_job_poll(cm_server* server, int job, cm_job_info* info);
 /* waits until the job has ended or timeout_s passed (timeout_s < 0: no limit) */
 int cm_job_wait(cm_server* server, int job, double timeout_s, cm_job_info* info);
-/* a queued job is dropped; a running one stops at its next graph boundary */
+/* a queued job is dropped; a running one starts no more primaries after the current round of iterations
+ * and ends CANCELLED once its electrons in flight have ended */
 int cm_job_cancel(cm_server* server, int job);
 /* copies a finished job's tallies ([npix * hist_stride] each, may be NULL) and stats, then forgets the job;
  * a failed or cancelled job returns its error */

@@ -547,6 +547,34 @@ def test_oversized_wave_is_enomem_and_the_context_stays_usable(half):
 
 
 @pytest.mark.parametrize("prec", [FP64, FP32], ids=["fp64", "fp32"])
+def test_pool_overflow_restart_gives_the_same_tallies(prec):
+    """A secondary pool of one record per wave electron (cm_tuning.pool = 1, wave 1024) overflows on 5 keV
+    primaries; the run is repeated with twice the pool until it fits (pool_restarts > 0), and its tallies and
+    counts are those of a run with the default pool, because every electron's stream is keyed by its lineage.
+    The job server restarts a batch the same way."""
+    from cudamonsel_b200 import capi, scenes
+    c = np.tile([0.0, 0.0, -20e-9], (4, 1))
+    e = capi.Engine(0)
+    h = scenes.build_engine(scenes.halfspace(), e)
+    ref = e.run(h["chamber"], c, scenes.eV(5000.0), 100, 500, 0.0, 5, precision=prec)
+    assert ref[2].pool_restarts == 0
+    e.set_tuning(prec, wave=1024, pool=1)
+    small = e.run(h["chamber"], c, scenes.eV(5000.0), 100, 500, 0.0, 5, precision=prec)
+    assert small[2].pool_restarts > 0
+    assert (small[0] == ref[0]).all() and (small[1] == ref[1]).all()
+    assert small[2].steps == ref[2].steps and small[2].secondaries == ref[2].secondaries
+    srv = capi.Server(0, slots=4, budget_gb=4.0)
+    srv.tune(prec, wave=1024, pool=1)
+    job = srv.submit(e, h["chamber"], c, scenes.eV(5000.0), 100, 500, 0.0, 5, precision=prec)
+    assert srv.wait(job).state == capi.JOB_DONE
+    b, f, st = srv.result(job)
+    srv.close()
+    e.close()
+    assert st.pool_restarts > 0 and st.steps == ref[2].steps
+    assert (b == ref[0]).all() and (f == ref[1]).all()
+
+
+@pytest.mark.parametrize("prec", [FP64, FP32], ids=["fp64", "fp32"])
 def test_device_loop_limit_and_graph_reuse(half, prec):
     """The device-driven loop (one launch per run of a graph cached in the context): an iteration limit stops
     the run on the device with CM_ELIMIT; the following runs reuse the cached graph and give identical

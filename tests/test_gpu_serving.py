@@ -42,6 +42,36 @@ def test_job_same_alone_in_mix_and_through_cm_run(jobs):
     assert (back == b0).all() and (fwd == f0).all()
 
 
+def test_precisions_batch_apart_and_match_cm_run(jobs):
+    """FP32 and FP64 jobs submitted together run in two batches at once; each job's tallies are those of
+    cm_run at its precision, and FP32 is the same whether its neighbours in the batch came first or not."""
+    from cudamonsel_b200 import capi, scenes, serving
+    srv = capi.Server(0, slots=8, budget_gb=8.0)
+    holder = capi.Engine(0)
+    precs = [capi.PREC_FP32, capi.PREC_FP64, capi.PREC_FP32, capi.PREC_FP64]
+    ids = [serving.submit(srv, holder, j, p) for j, p in zip(jobs[2:6], precs)]
+    infos = [srv.wait(j) for j in ids]
+    assert all(i.state == capi.JOB_DONE for i in infos)
+    res = [srv.result(j) for j in ids]
+    e = capi.Engine(0)
+    for j, p, (b, f, st) in zip(jobs[2:6], precs, res):
+        e.reset()
+        h = scenes.replay(j["spec"], scenes.EngineBackend(e))
+        back, fwd, rs = e.run(h[j["chamber"].idx], j["centers"], j["energy"], j["nprim"], j["nbins"], 1e-9, 0,
+                              precision=p, pixel_keys=j["keys"])
+        assert (back == b).all() and (fwd == f).all()
+        assert st.primaries == rs.primaries and st.steps == rs.steps
+    e.close()
+    # the second FP32 job alone in a fresh server: the same as in the mix
+    j = jobs[4]
+    alone = serving.submit(srv, holder, j, capi.PREC_FP32)
+    assert srv.wait(alone).state == capi.JOB_DONE
+    b, f, _ = srv.result(alone)
+    assert (b == res[2][0]).all() and (f == res[2][1]).all()
+    srv.close()
+    holder.close()
+
+
 def test_cancel_queued_and_running(jobs):
     from cudamonsel_b200 import capi, serving
     srv = capi.Server(0, slots=1, budget_gb=8.0)
