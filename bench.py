@@ -184,7 +184,10 @@ def main():
     ap.add_argument("--serve-rate", type=float, default=None, help="mean arrival rate of the served stream (1/s)")
     ap.add_argument("--no-autotune", action="store_true", help="run with the default launch settings")
     ap.add_argument("--profile-run", action="store_true",
-                    help="run one FP32 step of the workload and exit (the case for ncu captures)")
+                    help="run one FP32 step of the workload (host-driven replays) and exit: the case for ncu")
+    ap.add_argument("--flight-units", type=int, nargs=2, metavar=("START", "END"),
+                    help="print the electron-steps the flight kernel took in iterations [START, END) of the "
+                         "--profile-run step (multiples of 16; two runs stopped by the iteration limit) and exit")
     a = ap.parse_args()
     a.warmup = max(a.warmup, 3) if a.impl == "ours" else a.warmup
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -228,8 +231,27 @@ def main():
         return eng.run_device(desc(prec, profile), t_back.data_ptr(), t_fwd.data_ptr(), stream.cuda_stream)
 
     prec = capi.PREC_FP32
+    if a.flight_units:
+        # the profiled replay stops at a multiple of 16 iterations when the limit is reached (CM_ELIMIT, stats
+        # still written): the difference of two such runs is what the flight launches of the window took
+        got = []
+        for lim in a.flight_units:
+            d = desc(prec, profile=1)
+            d.max_iterations = lim
+            st = capi.RunStats()
+            eng.L.cm_run_device(eng.h, C.byref(d), C.c_void_p(t_back.data_ptr()), C.c_void_p(t_fwd.data_ptr()),
+                                C.byref(st), C.c_void_p(stream.cuda_stream))
+            torch.cuda.synchronize()
+            got.append((int(st.iterations), int(st.units[0])))
+        n = got[1][0] - got[0][0]
+        print("flight electron-steps in iterations [%d, %d): %d (%.1f per launch)" % (
+            got[0][0], got[1][0], got[1][1] - got[0][1], (got[1][1] - got[0][1]) / max(1, n)))
+        eng.close()
+        return 0
     if a.profile_run:
-        st = step(prec)
+        # the host-driven replay of the same kernels (profile=1): ncu cannot profile the kernel nodes of
+        # the device-driven loop's graph, whose WHILE loops are conditional nodes
+        st = step(prec, profile=1)
         torch.cuda.synchronize()
         print("profile run: %d primaries, %d electron-steps, %d iterations" % (st.primaries, st.steps, st.iterations))
         eng.close()
@@ -337,10 +359,14 @@ def main():
     avg_ms = kms[dom] / max(1, nlaunch)
     achieved = units[dom] * BYTES_PER_STEP / (kms[dom] / 1000.0) / 1e9
     peak, peak_kind = peaks()
+    # DRAM traffic of the dominant kernel: bytes per electron-step from an ncu capture of three heavy launches
+    # of this workload (profiles/traffic.json), scaled to this run's mean electron-steps per launch
     traffic = None
     tf = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tf):
-        traffic = json.load(open(tf)).get(names[dom])
+        per = json.load(open(tf)).get(names[dom])
+        if isinstance(per, dict) and per.get("bytes_per_unit"):
+            traffic = float(per["bytes_per_unit"]) * per_launch_units
 
     # batched image: rough lines (3 x 128 segments), 256 x 256 pixels at 2 nm, Poisson(300) primaries per
     # pixel, energy per row from {300, 500, 1000} eV; FP32 batched form against the FP64 plain form

@@ -252,7 +252,7 @@ int cm_autotune(cm_context* ctx, const cm_run_desc* desc, cm_tuning* best);
  * library holds on every GPU that loads it until the process exits.  Same
  * arguments, same tallies as cm_run_device (stream 0 = the legacy default
  * stream; stats->kernel_ms stays zero).  Limits: npix <= 65536; the wave is
- * capped by the scratch (about 26 k electrons in FP32, 18 k in FP64), so a run
+ * capped by the scratch (about 17 k electrons in FP32, 12 k in FP64), so a run
  * whose secondaries overflow the fixed pool returns CM_EOVERFLOW instead of
  * growing it.  The scene must already be on the device for desc->precision
  * (uploading it allocates): after the last scene change, make one cm_run,
