@@ -37,6 +37,7 @@ WORKLOAD = ("linescan: 3 PMMA lines (h 100 nm, bottom w 40 nm, 3 deg, pitch 200 
 # served stream (latency line): jobs, mean arrival rate (1/s), server slots and budget, size scale
 SERVE_JOBS, SERVE_RATE, SERVE_SLOTS, SERVE_BUDGET_GB, SERVE_SCALE = 64, 8.0, 16, 16.0, 1 / 8
 IMAGE_REPEATS = 3  # runs per precision of the rough-line image
+IMAGE_BANDS = 16  # jobs the served image is split into (row bands)
 BYTES_PER_STEP = 128  # algorithmic bytes per electron-step: a 64 B SoA record read and written
 
 
@@ -390,6 +391,7 @@ def main():
         reps = {"fp32": [], "fp64": []}
         ys = {"fp32": [], "fp64": []}
         e_eV = ie / scenes.EV
+        first32 = None
         for r in range(IMAGE_REPEATS):
             for q, (name, pr) in enumerate((("fp32", capi.PREC_FP32), ("fp64", capi.PREC_FP64))):
                 kr = ikeys + np.uint64((2 * r + q + 1) * 1_000_000_007)
@@ -397,6 +399,30 @@ def main():
                 ib, _, ist = eimg.run(hi["chamber"], ic, ie, inp, inb, 1e-9, 0, precision=pr, pixel_keys=kr)
                 reps[name].append((ist.device_ms, time.perf_counter() - t0, int(ist.steps)))
                 ys[name].append(scenes.yields(ib.astype(np.int64), np.maximum(inp, 1), e_eV, inb))
+                if first32 is None and name == "fp32":
+                    first32 = (ib, kr)
+        # The same image served: IMAGE_BANDS row bands submitted at once to the job server (continuous
+        # batching, FP32, the batched form's tuned settings); primaries/s over the makespan against the FP64
+        # plain form's rate above, and each band's tallies against the batched FP32 run on the same streams
+        served = None
+        if not a.no_serving:
+            srv = capi.Server(local, IMAGE_BANDS, SERVE_BUDGET_GB)
+            if "fp32" in itune:
+                t = itune["fp32"]
+                srv.tune(capi.PREC_FP32, t["wave"], t["tail_below"], t["tail_steps"], t["blocks_per_sm"], t["pool"])
+            rows = np.array_split(np.arange(len(ic)), IMAGE_BANDS)
+            jobs = [srv.submit(eimg, hi["chamber"], ic[b], ie[b], inp[b], inb[b], 1e-9, 0, capi.PREC_FP32,
+                               pixel_keys=first32[1][b]) for b in rows]
+            infos = [srv.wait(j) for j in jobs]
+            outs = [srv.result(j) for j in jobs]
+            srv.close()
+            same = all(np.array_equal(o[0], first32[0][b][:, :o[0].shape[1]]) and
+                       not first32[0][b][:, o[0].shape[1]:].any() for o, b in zip(outs, rows))
+            mk = max(i.end_s for i in infos) - min(i.submit_s for i in infos)
+            lat = np.array([i.end_s - i.submit_s for i in infos])
+            served = {"bands": IMAGE_BANDS, "primaries_per_s": int(inp.sum()) / mk, "makespan_s": mk,
+                      "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
+                      "tallies_equal_batched": bool(same)}
         eimg.close()
         ntot = int(inp.sum())
         rate = {k: [ntot / (m / 1e3) for m, _, _ in v] for k, v in reps.items()}
@@ -425,6 +451,9 @@ def main():
                       "fp64_e2e_s": statistics.median(v[1] for v in reps["fp64"]),
                       "electron_steps_fp32": reps["fp32"][0][2],
                       "yield_error_vs_fp64": err}
+        if served:
+            served["fp32_served_over_fp64"] = served["primaries_per_s"] / statistics.median(rate["fp64"])
+            image_line["served_fp32"] = served
 
     # deep penetration: 16 x 16 seed-placed blocks and cylinders (PMMA or Si, 20-300 nm) on Si, 10 keV, a
     # --deep-side^2 scan over the 5.12 um layout, --deep-primaries per pixel, FP32 against FP64; the

@@ -10,8 +10,9 @@ Tolerances, written per check:
     mechanism/element selections identical;
   FP32 kernels: cross sections, rates, table values, sampled angles, energy
     losses and SE energies within 1e-6 relative; directions within 1e-6
-    (inelastic) and 5e-6 (elastic, 99.9 %) absolute; selections identical except where the reference's
-    value lies within float rounding of a decision boundary (counted, < 0.5 %).
+    (inelastic) and 5e-6 (elastic) absolute; every bound on the largest error, not a quantile;
+    selections identical (an element pick whose deviate lies within float rounding of a cumulative
+    cross section is counted and excluded, and none differs).
 The reference's 3-D theta interpolation extrapolates from the first four
 energy nodes (NULagrangeInterpolation.cu:236); its result amplifies rounding
 by up to (E/E3)^3, so directions after such events are compared only where
@@ -257,28 +258,28 @@ def test_tabulated_inelastic(lines_engine, oracle_lines, prec):
     if prec == FP64:
         r = (np.abs(dE1 - dE0) / np.maximum(np.abs(dE0), 1e-22))[ok]
         print("energy loss max rel %.3g" % r.max())
-        assert np.quantile(r, 0.999) < 1e-9
+        assert r.max() < 1e-9
     else:
         # in FP32 the loss is read off the float energy E' = E - dE, whose rounding is up to half a
         # float spacing of E: the bound is 1e-6 of the loss plus one spacing of E
         spacing = np.spacing(np.float32(inp[:, 0] * FROMSI)).astype(np.float64) / FROMSI
         q = (np.abs(dE1 - dE0) / (1e-6 * np.abs(dE0) + spacing))[ok]
         print("energy loss error / bound: max %.3g, 99.9%% %.3g" % (q.max(), np.quantile(q, 0.999)))
-        assert np.quantile(q, 0.999) < 1.0
+        assert q.max() < 1.0
     th = rel(out[first, 11], ref[first, 9])
     print("theta (first window) max rel %.3g" % th.max())
-    assert np.quantile(th, 0.999) < (1e-9 if prec == FP64 else 1e-6)
+    assert th.max() < (1e-9 if prec == FP64 else 1e-6)
     se = ok & first & (ref[:, 4] == 1)
     r = rel(out[se, 6], ref[se, 5])
     print("SE energy max rel %.3g over %d" % (r.max(), se.sum()))
-    assert np.quantile(r, 0.999) < (1e-9 if prec == FP64 else 1e-6)
+    assert r.max() < (1e-9 if prec == FP64 else 1e-6)
     tame = ok & first
     err = np.abs(out[:, 2:5] - unit(ref[:, 2], ref[:, 3])).max(axis=1)
     print("PE direction max abs err (first window) %.3g over %d" % (err[tame].max(), tame.sum()))
-    assert np.quantile(err[tame], 0.999) < (1e-7 if prec == FP64 else 1e-6)
+    assert err[tame].max() < (1e-7 if prec == FP64 else 1e-6)
     serr = np.abs(out[:, 7:10] - unit(ref[:, 6], ref[:, 7])).max(axis=1)
     print("SE direction max abs err %.3g over %d" % (serr[se].max(), se.sum()))
-    assert np.quantile(serr[se], 0.999) < (1e-7 if prec == FP64 else 1e-6)
+    assert serr[se].max() < (1e-7 if prec == FP64 else 1e-6)
 
 
 def scenes_eV(x):
@@ -323,7 +324,7 @@ def test_elastic(lines_engine, oracle_lines, mat, prec):
         assert sameZ[~edge].all()
     err = np.abs(out[:, 1:4] - unit(ref[:, 1], ref[:, 2])).max(axis=1)[sameZ]
     print("direction max abs err %.3g, 99.9%% %.3g" % (err.max(), np.quantile(err, 0.999)))
-    assert np.quantile(err, 0.999) < (1e-8 if prec == FP64 else 5e-6)
+    assert err.max() < (1e-8 if prec == FP64 else 5e-6)
     assert (out[:, 5] == ref[:, 4]).all()
 
 
@@ -492,7 +493,7 @@ def test_csd_fitted_polaron(lines_engine, oracle_lines, prec):
     for k, name in enumerate(("csd", "fitted", "polaron")):
         r = rel(out[:, k], ref[:, k])
         print("%s prec %d max rel %.3g, 99.9%% %.3g" % (name, prec, r.max(), np.quantile(r, 0.999)))
-        assert np.quantile(r, 0.999) < (1e-9 if prec == FP64 else 1e-6)
+        assert r.max() < (1e-9 if prec == FP64 else 1e-6)
 
 
 def test_shapes(engine):
@@ -527,7 +528,9 @@ def test_shapes(engine):
         r = rel(out[fin, 3], rows[fin, 10])
         print("shape %d u max rel %.3g" % (k, r.max() if fin.any() else 0))
         assert r.max() < 1e-12
-        assert (out[:, 4] == rows[:, 11]).mean() > 0.9999
+        inside = (out[:, 4] == rows[:, 11]).mean()
+        print("shape %d containment agreement %.6f" % (k, inside))
+        assert inside == 1.0
 
 
 @pytest.mark.parametrize("fixes", [0, 1])
@@ -536,7 +539,7 @@ def test_shapes2(fixes):
     own results (cases 0-4: cylinders as the reference builds them; 5-7: axis normalised, built
     here with CM_OPT_JMONSEL_FIXES).  The engine works in nm, the reference in m: u within 1e-9
     relative and normals within 1e-9 where both report a crossing, crossing/containment decisions
-    identical except within rounding of a tangency (< 0.1 %)."""
+    identical."""
     from conftest import shapes2_scene
     from cudamonsel_b200 import capi, scenes
     s, shapes = shapes2_scene(fixes)
@@ -555,11 +558,12 @@ def test_shapes2(fixes):
         nerr = np.abs(out[both, 0:3] - rows[both, 7:10]).max(axis=1) if both.any() else np.zeros(1)
         print("case %d crossings %d agree %.5f u max rel %.3g normal max err %.3g" % (
             k, fin.sum(), agree, r.max() if both.any() else 0, nerr.max()))
-        assert agree > 0.999
+        inside = ((out[:, 4] == rows[:, 11]).mean(), (out[:, 5] == rows[:, 12]).mean())
+        print("case %d containment agreement %.6f %.6f" % (k, inside[0], inside[1]))
+        assert agree == 1.0
         if both.any():
-            assert np.quantile(r, 0.999) < 1e-9 and np.quantile(nerr, 0.999) < 1e-9
-        assert (out[:, 4] == rows[:, 11]).mean() > 0.999
-        assert (out[:, 5] == rows[:, 12]).mean() > 0.999
+            assert r.max() < 1e-9 and nerr.max() < 1e-9
+        assert inside == (1.0, 1.0)
     e.close()
 
 
@@ -567,8 +571,7 @@ def test_rotate_shapes():
     """ITransform::rotate (cm_shape_rotate) against the reference's own rotated shapes: blocks rotated with
     both forms of the Euler matrix, a tilted half-space, a cylinder rotated once (which normalises the
     reference's cylinder axis) and twice.  The engine works in nm, the reference in m: u within 1e-9
-    relative and normals within 1e-9 where both report a crossing, crossing/containment decisions identical
-    except within rounding of a tangency (< 0.1 %)."""
+    relative and normals within 1e-9 where both report a crossing, crossing/containment decisions identical."""
     from conftest import rotate_scene
     from cudamonsel_b200 import capi, scenes
     s, shapes = rotate_scene()
@@ -585,10 +588,11 @@ def test_rotate_shapes():
         nerr = np.abs(out[both, 0:3] - rows[both, 7:10]).max(axis=1)
         print("rotated shape %d crossings %d agree %.5f u max rel %.3g normal max err %.3g" % (
             k, fin.sum(), agree, r.max(), nerr.max()))
-        assert fin.sum() > 40 and agree > 0.999
-        assert np.quantile(r, 0.999) < 1e-9 and np.quantile(nerr, 0.999) < 1e-9
-        assert (out[:, 4] == rows[:, 11]).mean() > 0.999
-        assert (out[:, 5] == rows[:, 12]).mean() > 0.999
+        inside = ((out[:, 4] == rows[:, 11]).mean(), (out[:, 5] == rows[:, 12]).mean())
+        print("rotated shape %d containment agreement %.6f %.6f" % (k, inside[0], inside[1]))
+        assert fin.sum() > 40 and agree == 1.0
+        assert r.max() < 1e-9 and nerr.max() < 1e-9
+        assert inside == (1.0, 1.0)
     e.close()
 
 
@@ -612,7 +616,7 @@ def test_barrier(engine, prec):
         reg = np.where(out[:, 7] == h["si_region"], 1, 0)
         agree = reg == r[:, 13]
         print("dir %d prec %d region agreement %.5f" % (d, prec, agree.mean()))
-        assert agree.all() if prec == FP64 else agree.mean() > 0.995
+        assert agree.all()
         er = np.abs(out[agree, 0] - r[agree, 7]) / np.maximum(np.abs(r[agree, 7]), 0.1 * EV)
         print("energy max rel %.3g" % er.max())
         assert er.max() < (1e-12 if prec == FP64 else 2e-6)
