@@ -859,17 +859,37 @@ __device__ __forceinline__ void flush_counts(Counters* c, StepCounts& sc) {
   }
 }
 
+// Where each class segment of wave `cur` starts in the order the threads take its electrons, in the block's
+// shared memory (a per-thread array indexed by segment would live in local memory).  Every thread of the
+// block calls it.
+__device__ __forceinline__ void segment_starts(const Counters* c, int cur, int* first) {
+  if (threadIdx.x == 0) {
+    int a = 0;
+    for (int k = 0; k < kSegments; ++k) {
+      first[k] = a;
+      a += c->nc[cur][k];
+    }
+    first[kSegments] = a;
+  }
+  __syncthreads();
+}
+
+__device__ __forceinline__ int segment_of(const int* first, int i) {
+  int k = 0;
+  while (k < kSegments - 1 && i >= first[k + 1]) ++k;
+  return k;
+}
+
 template <typename R, int D> __device__ __forceinline__ void flight_loop(const RunView<R>& v, int cur) {
   DeviceSink sink;
   StepCounts sc;
   const int n = v.c->n[cur];
   if ((int)(blockIdx.x * blockDim.x) >= n || !stage_tables(v)) return;  // blocks without work stage nothing
-  int cnt[kSegments];
-  for (int k = 0; k < kSegments; ++k) cnt[k] = v.c->nc[cur][k];
+  __shared__ int first[kSegments + 1];
+  segment_starts(v.c, cur, first);
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    int k = 0, j = i;  // i-th electron over the class segments in order
-    while (k < kSegments - 1 && j >= cnt[k]) j -= cnt[k++];
-    flight_one<R, D>(v, cur, k * v.W + j, sink, sc);
+    const int k = segment_of(first, i);  // the i-th electron over the class segments in order
+    flight_one<R, D>(v, cur, k * v.W + (i - first[k]), sink, sc);
   }
   flush_counts(v.c, sc);
 }
@@ -981,12 +1001,11 @@ template <typename R, int D> __global__ void CM_LB_STEPS k_steps(RunView<R> v, i
   StepCounts sc;
   const int n = v.c->n[cur];
   if ((int)(blockIdx.x * blockDim.x) >= n || !stage_tables(v)) return;
-  int cnt[kSegments];
-  for (int k = 0; k < kSegments; ++k) cnt[k] = v.c->nc[cur][k];
+  __shared__ int first[kSegments + 1];
+  segment_starts(v.c, cur, first);
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    int k = 0, j = i;
-    while (k < kSegments - 1 && j >= cnt[k]) j -= cnt[k++];
-    steps_one<R, D>(v, cur, k * v.W + j, nsteps, sink, sc);
+    const int k = segment_of(first, i);
+    steps_one<R, D>(v, cur, k * v.W + (i - first[k]), nsteps, sink, sc);
   }
   flush_counts(v.c, sc);
 }
@@ -2466,11 +2485,8 @@ int cm_autotune(cm_context* ctx, const cm_run_desc* d, cm_tuning* best) {
     slot = saved;
     return rc;
   }
-  const int w = cur.wave;
-  const int waves[] = {w / 2, w * 2};
   const int belows[] = {65536, 131072, 524288};
   const int steps[] = {16, 64};
-  const int blocks[] = {4, 16};
   auto sweep = [&](int cm_tuning::*field, const int* vals, int n) -> int {
     for (int k = 0; k < n; ++k) {
       if (vals[k] == cur.*field) continue;
@@ -2486,10 +2502,20 @@ int cm_autotune(cm_context* ctx, const cm_run_desc* d, cm_tuning* best) {
     }
     return 0;
   };
-  if ((rc = sweep(&cm_tuning::wave, waves, 2)) || (rc = sweep(&cm_tuning::tail_below, belows, 3)) ||
-      (rc = sweep(&cm_tuning::tail_steps, steps, 2)) || (rc = sweep(&cm_tuning::blocks_per_sm, blocks, 2))) {
-    slot = saved;
-    return rc;
+  // passes of coordinate descent until one changes nothing (at most 3): the wave and the blocks per SM are
+  // tried at half and twice their current values, so a later pass can go on in the direction that paid
+  for (int pass = 0; pass < 3; ++pass) {
+    const cm_tuning before = cur;
+    const int waves[] = {std::max(1024, cur.wave / 2), std::min(1 << 24, cur.wave * 2)};
+    const int blocks[] = {std::max(2, cur.blocks_per_sm / 2), std::min(32, cur.blocks_per_sm * 2)};
+    if ((rc = sweep(&cm_tuning::wave, waves, 2)) || (rc = sweep(&cm_tuning::tail_below, belows, 3)) ||
+        (rc = sweep(&cm_tuning::tail_steps, steps, 2)) || (rc = sweep(&cm_tuning::blocks_per_sm, blocks, 2))) {
+      slot = saved;
+      return rc;
+    }
+    if (cur.wave == before.wave && cur.tail_below == before.tail_below && cur.tail_steps == before.tail_steps &&
+        cur.blocks_per_sm == before.blocks_per_sm)
+      break;
   }
   cur.ms = cur_ms;
   slot = cur;

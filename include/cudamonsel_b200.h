@@ -239,7 +239,8 @@ int cm_run_device(cm_context* ctx, const cm_run_desc* desc_device_arrays, uint32
 
 /* Autotuner: times the transport loop of desc (host arrays as for cm_run; its tallies are discarded)
  * under candidate settings, one setting at a time from the defaults (coordinate descent; a change is
- * kept when it is at least 1 % faster), and keeps the fastest for this context's later runs.  desc
+ * kept when it is at least 1 % faster; passes repeat, at most 3, until one changes nothing), and keeps
+ * the fastest for this context's later runs.  desc
  * should hold at least a wave's worth of primaries so that the trial sees the full and the tail phases
  * of a run.  The settings are kept for desc->precision; *best (may be NULL) receives them. */
 int cm_autotune(cm_context* ctx, const cm_run_desc* desc, cm_tuning* best);
