@@ -200,6 +200,9 @@ struct cm_context {
   int* cancel_host = nullptr;      // mapped host flag the device loop reads (the server sets it on cancel)
   const int* cancel_dev = nullptr; // its device address
   cm_tuning tune[2] = {{0, 0, 0, 0, 0.0}, {0, 0, 0, 0, 0.0}};  // launch settings per precision (0: default)
+  // boxes of plane sets by their planes (normals then points): a job server's batch scene holds many
+  // copies of the same shapes and is rebuilt as jobs join, and each box is a vertex enumeration
+  std::map<std::vector<double>, std::array<double, 6>> box_memo;
   void dirty() {
     d64.release();
     d32.release();
@@ -360,12 +363,27 @@ static Box planes_box(const HShape& s) {
   return b;  // empty (lo > hi) when the plane set holds nothing inside the world box
 }
 
+// planes_box, remembered by the context for plane sets it has boxed before
+static Box planes_box_memo(cm_context* ctx, const HShape& s) {
+  std::vector<double> key(s.n);
+  key.insert(key.end(), s.p.begin(), s.p.end());
+  auto it = ctx->box_memo.find(key);
+  if (it != ctx->box_memo.end()) {
+    const auto& v = it->second;
+    return Box{{v[0], v[1], v[2]}, {v[3], v[4], v[5]}};
+  }
+  const Box b = planes_box(s);
+  if (ctx->box_memo.size() > 200000) ctx->box_memo.clear();  // bounded over a long-lived server
+  ctx->box_memo.emplace(std::move(key), std::array<double, 6>{b.lo[0], b.lo[1], b.lo[2], b.hi[0], b.hi[1], b.hi[2]});
+  return b;
+}
+
 static Box shape_box(cm_context* ctx, int id) {
   const HShape& s = ctx->shapes[id];
   Box b;
   switch (s.kind) {
     case SHAPE_PLANES:
-      return planes_box(s);
+      return planes_box_memo(ctx, s);
     case SHAPE_SPHERE:
       for (int a = 0; a < 3; ++a) {
         b.lo[a] = s.c[a] - s.r;
@@ -400,7 +418,7 @@ static Box shape_box(cm_context* ctx, int id) {
             planar = false;
           }
         }
-        if (planar) return planes_box(all);
+        if (planar) return planes_box_memo(ctx, all);
       }
       const Box x = shape_box(ctx, s.a), y = shape_box(ctx, s.b);
       for (int a = 0; a < 3; ++a) {

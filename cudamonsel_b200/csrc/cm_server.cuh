@@ -8,7 +8,7 @@
 // join the wave as soon as those of the jobs admitted before it have all started, so new jobs fill the
 // room the ending cascades of earlier ones leave; the wave does not drain between jobs.  Jobs are admitted
 // first in, first out while fewer than `slots` are in the batch and their pixel and tally buffers fit
-// `budget_gb`.  Per job the device counts the electrons alive and their steps; a job is done when its
+// `budget_gb`; a new batch first gathers the submissions of a burst, so that its scene is built once.  Per job the device counts the electrons alive and their steps; a job is done when its
 // primaries have all started and none of its electrons is left, and its tallies are copied out.  A
 // job's tallies depend only on its scene, pixels and stream keys: the same alone, in any mix and
 // through cm_run.  Cancelling a running job stops its unstarted primaries; the ones in flight end
@@ -475,6 +475,10 @@ static void batch_reset(Batcher& b) {
   b.drop_rounds();
 }
 
+// submissions closer together than this (ms) are gathered into a new batch, for at most kGatherMaxMs
+constexpr int kGatherMs = 5;
+constexpr int kGatherMaxMs = 50;
+
 template <typename R>
 static void batcher_worker(cm_server* srv, Batcher* b) {
   cudaSetDevice(srv->device);
@@ -492,7 +496,20 @@ static void batcher_worker(cm_server* srv, Batcher* b) {
         }
         return false;
       };
-      if (b->active.empty()) srv->cv_work.wait(lk, [&] { return srv->stop || head_fits(); });
+      if (b->active.empty()) {
+        srv->cv_work.wait(lk, [&] { return srv->stop || head_fits(); });
+        // A new batch: jobs submitted together (a scan split into bands, a burst of requests) join it at
+        // once, so that its scene is merged, uploaded and its rounds captured once rather than once per
+        // job as they come in: admission waits while submissions keep arriving less than kGatherMs
+        // apart, at most kGatherMaxMs.
+        const auto t0 = std::chrono::steady_clock::now();
+        while (!srv->stop && std::chrono::steady_clock::now() - t0 < std::chrono::milliseconds(kGatherMaxMs)) {
+          const size_t q = srv->queue.size();
+          if (!srv->cv_work.wait_for(lk, std::chrono::milliseconds(kGatherMs),
+                                     [&] { return srv->stop || srv->queue.size() != q; }))
+            break;
+        }
+      }
       if (srv->stop) return;
       while (head_fits()) {
         auto it = srv->queue.begin();
