@@ -13,8 +13,10 @@ settings of each precision on this workload (--no-autotune: defaults); they
 are printed in config.tuning.  Under torchrun each rank runs the full linescan
 with its own random streams (weak scaling, no collective on the data path);
 the time is the max over ranks.  Further lines: the rough-line image (both
-precisions autotuned on its first eighth of rows), the 10 keV deep layout and
-the served stream.
+precisions autotuned on its first eighth of rows; FP32 batched against the plain
+FP64 form at default settings and against FP64 tuned; the image also served as
+16 jobs), the 10 keV deep layout (--deep-side 512 --deep-primaries 500 for its
+full size) and the served stream (Poisson arrivals and saturated, FP32 and FP64).
 """
 import argparse
 import json
