@@ -123,6 +123,40 @@ def test_nistmott_methods_2_3(lines_engine, oracle_lines, method, prec):
         assert r.max() < tol and d.max() < tol
 
 
+@pytest.mark.parametrize("prec", [FP64, FP32], ids=["fp64", "fp32"])
+def test_browning_with_fixes(prec):
+    """Browning's cross section and screened angle below the NIST Mott range as JMONSEL computes them
+    (BrowningEmpiricalCrossSection.cu:24-45 with the element's Z; CM_OPT_JMONSEL_FIXES), where the compiled
+    reference reads Z through a dangling reference and always takes the isotropic branch: engine vs the
+    oracle in its fixes mode on 2-49 eV and uniform deviates, FP32 on float-rounded inputs."""
+    import pyoracle
+    from cudamonsel_b200 import capi, scenes
+    sc = scenes.lines()
+    sc.spec.options = 1
+    e = capi.Engine(0)
+    scenes.build_engine(sc, e)
+    b, _ = pyoracle.build_oracle(sc)
+    rng = np.random.default_rng(17)
+    n = 4000
+    E = np.exp(rng.uniform(np.log(2.0), np.log(49.0), n)) / FROMSI
+    u = rng.random((n, 2))
+    if prec == FP32:
+        E, u = f32_energy(E), f32(u)
+    u = np.ascontiguousarray(u)
+    for Z in (1, 6, 8, 14):
+        sig, th = e.eval_nistmott(Z, np.ascontiguousarray(E), u, prec)
+        rs, rt = oracle_nistmott(b, Z, E, u)
+        r = rel(sig, rs)
+        d = np.abs(th - rt) if prec == FP64 else np.abs(th - rt) / np.maximum(rt, 1e-6)
+        iso = np.abs(np.cos(rt) - (1 - 2 * u[:, 1])) < 1e-12
+        print("Z=%d prec %d sigma max rel %.3g theta max %.3g (screened branch in %d of %d)" % (
+            Z, prec, r.max(), d.max(), (~iso).sum(), n))
+        assert (~iso).sum() > n // 10  # the screened branch is taken, not only the isotropic one
+        assert r.max() < (1e-9 if prec == FP64 else 1e-6)
+        assert d.max() < (1e-9 if prec == FP64 else 1e-6)
+    e.close()
+
+
 def test_nistmott_sweep(lines_engine, oracle_lines):
     """Sampled Mott angle over a fine grid of deviates and energies (FP64 vs the oracle)."""
     e, h = lines_engine
