@@ -188,6 +188,7 @@ struct Batcher {
   int pool_want = 0;           // secondary-pool records to ask for (doubled after an overflow)
   double emax_eV = 0;          // highest beam energy of the batch's jobs
   int restarts = 0;            // restarts of the current batch after overflows
+  bool waiting = false;        // jobs of this batcher wait in the queue (set before each round)
   std::vector<JobRecord*> active;
   // captured rounds of iterations for the current scene build and run buffers
   cudaGraphExec_t round_exec[2] = {nullptr, nullptr};
@@ -308,6 +309,9 @@ static int batch_add(Batcher& b, JobRecord& j) {
   return 0;
 }
 
+// rounds a batch runs between two reads of its counters while its wave is full and no job waits
+constexpr int kRoundRepeats = 4;
+
 // one round of the batch: kLoopBody iterations of the queue kernels, or of the tail kernels once every
 // primary has started and fewer electrons are left than the tail threshold
 template <typename R>
@@ -405,7 +409,11 @@ static int batch_round(Batcher& b) {
     b.round_buffers = (const void*)rb.w[0].px;
     b.round_pool = rb.poolCap;
   }
-  CM_CUDA(cudaGraphLaunch(b.round_exec[tail ? 1 : 0], s));
+  // While the wave is full and no job waits for admission, kRoundRepeats rounds run back to back before
+  // the counters are read: the host's turn between rounds (counter copies, job bookkeeping) leaves the GPU
+  // idle.  In the tail, where jobs end, and while jobs wait, one round per turn keeps latency short.
+  const int reps = (!tail && !b.waiting) ? kRoundRepeats : 1;
+  for (int r = 0; r < reps; ++r) CM_CUDA(cudaGraphLaunch(b.round_exec[tail ? 1 : 0], s));
   CM_CUDA(cudaMemcpyAsync(&hc, ctx->counters, sizeof(Counters), cudaMemcpyDeviceToHost, s));
   CM_CUDA(cudaStreamSynchronize(s));
   return 0;
@@ -536,6 +544,15 @@ static void batcher_worker(cm_server* srv, Batcher* b) {
       }
     }
     std::vector<JobRecord*> finished;
+    {
+      std::lock_guard<std::mutex> lk(srv->mu);
+      b->waiting = false;
+      for (int id : srv->queue)
+        if (srv->jobs[id]->desc.precision == b->precision && srv->jobs[id]->options == b->options) {
+          b->waiting = true;
+          break;
+        }
+    }
     if (rc == 0 && !b->active.empty())
       rc = b->precision == CM_PREC_FP64 ? batch_round<double>(*b) : batch_round<float>(*b);
     if (rc == 0 && b->ctx->counters_host->error) rc = run_error(b->ctx->counters_host->error, *b->ctx->counters_host);
