@@ -45,7 +45,8 @@ class RunDesc(C.Structure):
                 ("hist_stride", C.c_int), ("wave", C.c_int), ("max_iterations", C.c_int),
                 ("pixel_key", C.POINTER(C.c_uint64)), ("profile", C.c_int),
                 ("elevation", C.POINTER(C.c_uint32)), ("azimuth", C.POINTER(C.c_uint32)),
-                ("escape_log", C.c_void_p), ("escape_log_cap", C.c_int64)]
+                ("escape_log", C.c_void_p), ("escape_log_cap", C.c_int64),
+                ("pixel_first", C.POINTER(C.c_int64))]
 
 
 ELEVATION_COUNTS, AZIMUTH_COUNTS = 182, 362
@@ -321,9 +322,10 @@ class Engine:
 
     # ---- runs
     def run(self, chamber, centers, energies, nprim, nbins, beam_width, seed, precision=PREC_FP64, wave=0,
-            max_iterations=0, pixel_keys=None, profile=0, angles=False, escape_log_cap=0):
+            max_iterations=0, pixel_keys=None, profile=0, angles=False, escape_log_cap=0, first_primary=None):
         """cm_run: (back, fwd, stats); with angles or an escape log also a dict of BackscatterStats'
-        elevation [npix, 182] and azimuthal [npix, 362] histograms and the escape records."""
+        elevation [npix, 182] and azimuthal [npix, 362] histograms and the escape records.  first_primary
+        (per pixel, or None: 0) is the index of each pixel's first primary, for a scan run in parts."""
         centers = np.ascontiguousarray(centers, dtype=np.float64).reshape(-1, 3)
         npix = len(centers)
         e, pe = _d(np.broadcast_to(np.asarray(energies, dtype=np.float64), (npix,)).copy())
@@ -336,6 +338,10 @@ class Engine:
             keys = np.ascontiguousarray(pixel_keys, dtype=np.uint64)
         desc = RunDesc(chamber, precision, npix, beam_width, pc, pe, pn, pb, seed, stride, wave, max_iterations,
                        keys.ctypes.data_as(C.POINTER(C.c_uint64)) if keys is not None else None, profile)
+        first = None
+        if first_primary is not None:
+            first = np.ascontiguousarray(np.broadcast_to(np.asarray(first_primary), (npix,)), dtype=np.int64)
+            desc.pixel_first = first.ctypes.data_as(C.POINTER(C.c_int64))
         extra = None
         if angles or escape_log_cap:
             extra = {}

@@ -21,6 +21,7 @@
 #include <cooperative_groups/reduce.h>
 #include <cuda_runtime.h>
 #include <dlfcn.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <algorithm>
 #include <array>
@@ -211,6 +212,16 @@ struct cm_context {
 
 // ------------------------------------------------------------------ scene upload
 namespace cm {
+
+// An NVTX range over the scope: the phases of a run (scene upload, run buffers, launch graph, transport,
+// tally copies), autotuner trials and job-server rounds appear by name on a timeline (Nsight Systems,
+// ncu's NVTX filters); without a tool attached a range costs a call that returns at once.
+struct NvtxRange {
+  explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+  NvtxRange(const NvtxRange&) = delete;
+  NvtxRange& operator=(const NvtxRange&) = delete;
+};
 
 template <typename T>
 static int dev_copy(std::vector<void*>& allocs, const std::vector<T>& v, const T** out, bool host = false) {
@@ -434,6 +445,7 @@ static Box shape_box(cm_context* ctx, int id) {
 template <typename R>
 static int build_scene(cm_context* ctx, DevScene<R>& ds) {
   if (ds.valid) return 0;
+  NvtxRange range("cm scene upload");
   ds.release();
   std::vector<R> blob;
   std::vector<double> dbl;  // SceneView::dbl
@@ -1149,6 +1161,7 @@ template <typename R>
 static int ensure_buffers(cm_context* ctx, int W, int poolCap) {
   RunBuffers<R>& rb = buffers_of<R>(ctx);
   if (rb.cap == W && rb.poolCap >= poolCap) return 0;
+  NvtxRange range("cm run buffers");
   rb.release();
   // two waves of kSegments segments, the pool, three queues: refused before any allocation when the
   // device has not that much free memory (less a reserve for the run's other buffers)
@@ -1238,6 +1251,7 @@ static void launch_tail_iteration(const RunView<R>& v, const RunView<R>& vs, int
 template <typename R>
 static int build_loop_graph(cm_context* ctx, RunBuffers<R>& rb, const RunView<R>& v, const RunView<R>& vs, int grid,
                             size_t smem, int tail_steps) {
+  NvtxRange range("cm launch graph");
   rb.drop_graph();
   cudaGraph_t g = nullptr;
   CM_CUDA(cudaGraphCreate(&g, 0));
@@ -1371,6 +1385,7 @@ static int run_device_once(cm_context* ctx, const cm_run_desc* d, uint32_t* back
   io.npix = d->npix;
   io.width = d->beam_width * 1e9;  // m -> nm
   io.pkey = pkey_dev;
+  io.pfirst = (const unsigned long long*)d->pixel_first;
   io.back = back;
   io.fwd = fwd;
   io.stride = d->hist_stride;
@@ -2306,7 +2321,7 @@ static int check_desc(cm_context* ctx, const cm_run_desc* d) {
 
 struct PixelPrep {
   std::vector<double> center_nm, e0, e0ref;
-  std::vector<unsigned long long> prefix, key;
+  std::vector<unsigned long long> prefix, key, first;  // first: empty when the run starts every pixel at 0
   unsigned long long total = 0;
 };
 
@@ -2334,6 +2349,13 @@ static int prep_pixels(const cm_run_desc* d, const double* center, const double*
     p.key[i] = d->pixel_key ? (unsigned long long)d->pixel_key[i]
                             : mix64(mix64(d->seed ^ 0x243F6A8885A308D3ULL) + (unsigned long long)i);
   p.total = p.prefix[d->npix];
+  if (d->pixel_first) {
+    p.first.resize(d->npix);
+    for (int i = 0; i < d->npix; ++i) {
+      if (d->pixel_first[i] < 0) return fail(CM_EINVAL, "negative pixel_first");
+      p.first[i] = (unsigned long long)d->pixel_first[i];
+    }
+  }
   return 0;
 }
 
@@ -2351,17 +2373,19 @@ template <typename T> static int up(std::vector<void*>& allocs, const std::vecto
 static int run_common(cm_context* ctx, const cm_run_desc* d, const double* center_h, const double* energy_h,
                       const int* nprim_h, const int* nbins_h, int* nbins_dev_in, uint32_t* back_dev, uint32_t* fwd_dev,
                       cm_run_stats* st, cudaStream_t stream) {
+  NvtxRange range("cm run");
   PixelPrep p;
   int rc = prep_pixels(d, center_h, energy_h, nprim_h, nbins_h, d->hist_stride, p);
   if (rc) return rc;
   std::vector<void*> allocs;
   double *c_dev, *e0_dev, *e0ref_dev;
-  unsigned long long *prefix_dev, *key_dev;
+  unsigned long long *prefix_dev, *key_dev, *first_dev = nullptr;
   int* nbins_dev = nbins_dev_in;
   std::vector<int> nb(nbins_h, nbins_h + d->npix);
   if ((rc = up(allocs, p.center_nm, &c_dev, stream)) || (rc = up(allocs, p.e0, &e0_dev, stream)) ||
       (rc = up(allocs, p.e0ref, &e0ref_dev, stream)) || (rc = up(allocs, p.prefix, &prefix_dev, stream)) ||
       (rc = up(allocs, p.key, &key_dev, stream)) ||
+      (!p.first.empty() && (rc = up(allocs, p.first, &first_dev, stream))) ||
       (!nbins_dev && (rc = up(allocs, nb, &nbins_dev, stream)))) {
     for (void* a : allocs) cudaFree(a);
     return rc;
@@ -2370,7 +2394,9 @@ static int run_common(cm_context* ctx, const cm_run_desc* d, const double* cente
   dd.pixel_center = c_dev;
   dd.pixel_energy = e0_dev;
   dd.pixel_nbins = nbins_dev;
+  dd.pixel_first = (const int64_t*)first_dev;  // device copy (null: every pixel from 0)
   const double emax = p.e0.empty() ? 0.0 : *std::max_element(p.e0.begin(), p.e0.end());
+  NvtxRange transport("cm transport");
   rc = d->precision == CM_PREC_FP64
            ? run_device<double>(ctx, &dd, back_dev, fwd_dev, st, stream, prefix_dev, e0ref_dev, key_dev, p.total, emax)
            : run_device<float>(ctx, &dd, back_dev, fwd_dev, st, stream, prefix_dev, e0ref_dev, key_dev, p.total, emax);
@@ -2455,11 +2481,17 @@ int cm_run_device(cm_context* ctx, const cm_run_desc* d, uint32_t* back, uint32_
   CM_CUDA(cudaMemcpyAsync(np.data(), d->pixel_nprim, np.size() * 4, cudaMemcpyDeviceToHost, s));
   CM_CUDA(cudaMemcpyAsync(nb.data(), d->pixel_nbins, nb.size() * 4, cudaMemcpyDeviceToHost, s));
   std::vector<uint64_t> keys;
+  std::vector<int64_t> firsts;
   cm_run_desc dh = *d;
   if (d->pixel_key) {
     keys.resize(d->npix);
     CM_CUDA(cudaMemcpyAsync(keys.data(), d->pixel_key, keys.size() * 8, cudaMemcpyDeviceToHost, s));
     dh.pixel_key = keys.data();
+  }
+  if (d->pixel_first) {
+    firsts.resize(d->npix);
+    CM_CUDA(cudaMemcpyAsync(firsts.data(), d->pixel_first, firsts.size() * 8, cudaMemcpyDeviceToHost, s));
+    dh.pixel_first = firsts.data();
   }
   CM_CUDA(cudaStreamSynchronize(s));
   d = &dh;
@@ -2490,6 +2522,7 @@ int cm_autotune(cm_context* ctx, const cm_run_desc* d, cm_tuning* best) {
   cm_tuning& slot = ctx->tune[d->precision];
   const cm_tuning saved = slot;
   auto trial = [&](const cm_tuning& t, double& ms) -> int {
+    NvtxRange range("cm autotune trial");
     slot = t;
     cm_run_stats st;
     memset(&st, 0, sizeof(st));
@@ -2960,6 +2993,7 @@ extern "C" int cm_run_noalloc(cm_context* ctx, const cm_run_desc* d, uint32_t* b
   int rc = check_desc(ctx, d);
   if (!rc && (d->elevation || d->azimuth || d->escape_log))
     rc = fail(CM_EINVAL, "cm_run_noalloc tallies the energy histograms only (no angle histograms or escape log)");
+  if (!rc && d->pixel_first) rc = fail(CM_EINVAL, "cm_run_noalloc starts every pixel at its primary 0 (no pixel_first)");
   if (rc) return rc;
   if (!d->pixel_center || !d->pixel_energy || !d->pixel_nprim || !d->pixel_nbins || !back || !fwd)
     return fail(CM_EINVAL, "null array");

@@ -255,6 +255,7 @@ static void fill_info(const JobRecord& j, cm_job_info* info) {
 
 // append one job to the batch: scene, pixel tables, tally rows, counters (between rounds, device idle)
 static int batch_add(Batcher& b, JobRecord& j) {
+  NvtxRange range("cm job admit");
   cm_context* ctx = b.ctx;
   const cm_run_desc& d = j.desc;
   PixelPrep p;
@@ -316,6 +317,7 @@ constexpr int kRoundRepeats = 4;
 // primary has started and fewer electrons are left than the tail threshold
 template <typename R>
 static int batch_round(Batcher& b) {
+  NvtxRange range("cm server round");
   cm_context* ctx = b.ctx;
   DevScene<R>& ds = scene_of<R>(ctx);
   int rc;
@@ -422,6 +424,7 @@ static int batch_round(Batcher& b) {
 // the jobs whose primaries have all started and whose electrons have all ended: tallies copied out;
 // the jobs cancelled since the last round: their unstarted primaries stopped
 static int batch_collect(Batcher& b, std::vector<JobRecord*>& finished) {
+  NvtxRange range("cm job results");
   if (b.slots == 0 || !b.counters_live) return 0;
   const Counters& hc = *b.ctx->counters_host;
   std::vector<unsigned long long> alive(b.slots), steps(b.slots);
@@ -654,6 +657,7 @@ int cm_job_submit(cm_server* srv, const cm_context* scene, const cm_run_desc* d,
   if (!(d->beam_width >= 0)) return fail(CM_EINVAL, "negative beam width");
   if (d->elevation || d->azimuth || d->escape_log)
     return fail(CM_EINVAL, "jobs tally the energy histograms only (no angle histograms or escape log)");
+  if (d->pixel_first) return fail(CM_EINVAL, "jobs start every pixel at its primary 0 (no pixel_first)");
   std::unique_ptr<JobRecord> j(new JobRecord());
   j->options = scene->options;
   j->mott = scene->mott;

@@ -118,6 +118,7 @@ struct RunIO {
   const int* pnbins;
   const unsigned long long* prefix;
   const unsigned long long* pkey;  // per-pixel stream key
+  const unsigned long long* pfirst;  // per-pixel index of its first primary (a scan resumed), or null: 0
   int npix;
   double width;          // nm
   uint32_t *back, *fwd;
@@ -580,7 +581,7 @@ CM_D void spawn_one(const RunView<R>& v, int nxt, int j, int take_se, int poolTo
   }
   const int px = lo;
   if (io.job_stop && io.job_stop[io.pjob[px]]) return;  // a stopped job starts no more primaries
-  const unsigned long long k = gi - io.prefix[px];
+  const unsigned long long k = gi - io.prefix[px] + (io.pfirst ? io.pfirst[px] : 0ull);
   El<R> e;
   e.key = mix64(io.pkey[px] + mix64(k + 1));
   Rng<R> g(e.key, 0xFFFFFFFFu, 0);

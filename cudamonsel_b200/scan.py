@@ -67,3 +67,44 @@ def read_pgm(path):
     parts = data.split(b"\n", 3)
     w, h = (int(v) for v in parts[1].split())
     return np.frombuffer(parts[3], dtype=np.uint8).reshape(h, w)
+
+
+def run_checkpointed(engine, chamber, centers, energies, nprim, nbins, beam_width, precision, pixel_keys, part=None,
+                     checkpoint=None, max_parts=None):
+    """A scan run in parts of at most `part` primaries per pixel, resumable.
+
+    After each part the primaries done per pixel and the tallies so far are written to `checkpoint` (an .npz,
+    replaced atomically); a call that finds the file carries on from it (its pixel keys and primary counts
+    must be this scan's).  Primary k of a pixel draws from a stream keyed by (pixel key, k) -- the run's
+    pixel_first is the primaries already done -- so the result equals that of one cm_run over the whole scan,
+    count for count.  max_parts stops after that many parts (the checkpoint holds the rest).  Returns
+    (back, fwd, done): uint64 tallies [npix, max(nbins) + 2] and the primaries done per pixel."""
+    import os
+    centers = np.asarray(centers, dtype=np.float64).reshape(-1, 3)
+    npix = len(centers)
+    keys = np.ascontiguousarray(pixel_keys, dtype=np.uint64)
+    nprim = np.ascontiguousarray(np.broadcast_to(np.asarray(nprim), (npix,)), dtype=np.int64)
+    stride = int(np.max(nbins)) + 2
+    done = np.zeros(npix, dtype=np.int64)
+    back = np.zeros((npix, stride), dtype=np.uint64)
+    fwd = np.zeros((npix, stride), dtype=np.uint64)
+    if checkpoint and os.path.exists(checkpoint):
+        z = np.load(checkpoint)
+        if not (np.array_equal(z["keys"], keys) and np.array_equal(z["nprim"], nprim) and z["back"].shape == back.shape):
+            raise ValueError("checkpoint %s belongs to another scan" % checkpoint)
+        done, back, fwd = z["done"].astype(np.int64), z["back"].astype(np.uint64), z["fwd"].astype(np.uint64)
+    part = int(part or max(1, int(nprim.max())))
+    parts = 0
+    while (done < nprim).any() and (max_parts is None or parts < max_parts):
+        todo = np.minimum(part, nprim - done)
+        b, f, _ = engine.run(chamber, centers, energies, todo.astype(np.int32), nbins, beam_width, 0,
+                             precision=precision, pixel_keys=keys, first_primary=done)
+        back += b.astype(np.uint64)
+        fwd += f.astype(np.uint64)
+        done = done + todo
+        parts += 1
+        if checkpoint:
+            tmp = checkpoint + ".tmp.npz"
+            np.savez(tmp, keys=keys, nprim=nprim, done=done, back=back, fwd=fwd)
+            os.replace(tmp, checkpoint)
+    return back, fwd, done

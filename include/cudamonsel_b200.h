@@ -184,6 +184,12 @@ typedef struct {
    * many there were.  Host array for cm_run, device array for cm_run_device. */
   struct cm_escape_record* escape_log;
   int64_t escape_log_cap;
+  /* [npix] index of each pixel's first primary, or NULL: 0.  Primary k of a pixel draws from a stream keyed
+   * by (pixel key, k), so a scan can run in parts -- pixel_first = primaries done so far, pixel_nprim = the
+   * next part -- and the parts' tallies add up to exactly those of one run: checkpoint/resume of a scan from
+   * (pixel_first, tallies).  Host array for cm_run, device array for cm_run_device; not taken by
+   * cm_run_noalloc or the job server (CM_EINVAL). */
+  const int64_t* pixel_first;
 } cm_run_desc;
 
 #define CM_ELEVATION_COUNTS 182 /* 180 bins + underflow + overflow */
