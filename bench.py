@@ -365,11 +365,17 @@ def main():
     # DRAM traffic of the dominant kernel: bytes per electron-step from an ncu capture of three heavy launches
     # of this workload (profiles/traffic.json), scaled to this run's mean electron-steps per launch
     traffic = None
+    issue = None
     tf = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tf):
         per = json.load(open(tf)).get(names[dom])
         if isinstance(per, dict) and per.get("bytes_per_unit"):
             traffic = float(per["bytes_per_unit"]) * per_launch_units
+        if isinstance(per, dict) and per.get("warp_instructions_per_unit"):
+            # the kernel is issue- and latency-bound: its instruction rate against the SMs' issue peak (4 warp
+            # schedulers per SM, one instruction per cycle each, at the SM clock sampled during the timed steps)
+            issue = {"warp_instructions_per_unit": per["warp_instructions_per_unit"], "sm_count": 148,
+                     "schedulers_per_sm": 4}
 
     # batched image: rough lines (3 x 128 segments), 256 x 256 pixels at 2 nm, Poisson(300) primaries per
     # pixel, energy per row from {300, 500, 1000} eV; FP32 batched form against the FP64 plain form
@@ -563,6 +569,11 @@ def main():
         cpu = {"value": n / secs, "unit": "primaries/s", "cores": nproc, "kind": kind,
                "sample": "%d processes x 4 linescan pixels x 500 primaries" % nproc}
 
+    if issue and clk and clk.get("sm_mhz"):
+        rate = units[dom] / (kms[dom] / 1000.0) * issue["warp_instructions_per_unit"]
+        peak_issue = issue["sm_count"] * issue["schedulers_per_sm"] * clk["sm_mhz"] * 1e6
+        issue.update({"achieved_warp_instructions_per_s": rate, "peak_warp_instructions_per_s": peak_issue,
+                      "frac": rate / peak_issue})
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": "primaries/s", "n_gpus": world, "steps": a.steps,
                 "warmup": a.warmup, "ms_per_step": ms / a.steps, "higher_is_better": True, "scaling": "weak",
@@ -578,6 +589,7 @@ def main():
                              "unit": "GB/s", "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
                              "bytes_per_unit": BYTES_PER_STEP, "units_per_launch": per_launch_units,
                              "avg_launch_ms": avg_ms},
+                "issue_roofline": issue,
                 "kernel_ms_share": dict({n: float(v / (kms.sum() + step_ms)) for n, v in zip(names, kms)},
                                         steps=float(step_ms / (kms.sum() + step_ms))),
                 "clocks": clk, "gpu_launches": launches,
