@@ -2,14 +2,16 @@
 //
 // Continuous batching: the jobs of one precision and set of run options share one wave of electrons on the
 // GPU.  A batcher (one host thread, one engine context) merges the scene of every job it admits into one
-// scene -- its own chamber and regions appended, scattering tables, materials and scatter models shared
-// with earlier jobs when their contents are equal -- and appends the job's pixels to the batch's pixel
-// tables (with the job's chamber, beam width, tally row and job number per pixel).  A job's primaries
-// join the wave as soon as those of the jobs admitted before it have all started, so new jobs fill the
-// room the ending cascades of earlier ones leave; the wave does not drain between jobs.  Jobs are admitted
-// first in, first out while fewer than `slots` are in the batch and their pixel and tally buffers fit
-// `budget_gb`; a new batch first gathers the submissions of a burst, so that its scene is built once.  Per job the device counts the electrons alive and their steps; a job is done when its
-// primaries have all started and none of its electrons is left, and its tallies are copied out.  A
+// scene -- its chamber and regions appended unless an earlier job of the batch has the same geometry (then
+// it shares that chamber), scattering tables, materials and scatter models shared with earlier jobs when
+// their contents are equal -- and appends the job's pixels to the batch's pixel tables (with the job's
+// chamber, beam width, tally row and job number per pixel).  A job's primaries join the wave as soon as
+// those of the jobs admitted before it have all started, so new jobs fill the room the ending cascades of
+// earlier ones leave; the wave does not drain between jobs.  Jobs are admitted first in, first out while
+// fewer than `slots` are in the batch and their pixel and tally buffers fit `budget_gb`; a new batch first
+// gathers the submissions of a burst, so that its scene is built once.  Per job the device counts the
+// electrons alive and their steps; a job is done when its primaries have all started and none of its
+// electrons is left, and its tallies are copied out.  A
 // job's tallies depend only on its scene, pixels and stream keys: the same alone, in any mix and
 // through cm_run.  Cancelling a running job stops its unstarted primaries; the ones in flight end
 // on their own.
@@ -111,9 +113,50 @@ static bool same_msm(const HMsm& a, const HMsm& b) {
   return true;
 }
 
-// the job's scene into the batch's scene: shared parts found by content, its shapes and regions appended;
-// returns the job's chamber in the batch's scene
-static int merge_scene(cm_context* ctx, const JobRecord& j) {
+// shape k of a job (its child indices moved by shape0) equals shape a of the batch's scene
+static bool same_shape(const HShape& a, const HShape& k, int shape0) {
+  if (a.kind != k.kind) return false;
+  switch (k.kind) {
+    case SHAPE_SPHERE:
+      return std::equal(a.c, a.c + 3, k.c) && a.r == k.r;
+    case SHAPE_PLANES:
+      return a.n == k.n && a.p == k.p;
+    case SHAPE_INTERSECTION:
+    case SHAPE_UNION:
+      return a.a == k.a + shape0 && a.b == k.b + shape0;
+    case SHAPE_CYLINDER:
+      return std::equal(a.e0, a.e0 + 3, k.e0) && std::equal(a.ax, a.ax + 3, k.ax) &&
+             std::equal(a.nax, a.nax + 3, k.nax) && a.radius == k.radius && a.len2 == k.len2;
+  }
+  return false;
+}
+
+// Where a job's geometry sits in the batch's scene (merge_scene): jobs with the same geometry (a scan split
+// into bands, repeated scans of one sample) share its chamber and regions.
+struct MergedGeometry {
+  int shape0, nshapes, region0, nregions;
+};
+
+static bool same_geometry(const cm_context* ctx, const MergedGeometry& g, const JobRecord& j,
+                          const std::vector<int>& smap) {
+  if (g.nshapes != (int)j.shapes.size() || g.nregions != (int)j.regions.size()) return false;
+  for (int k = 0; k < g.nshapes; ++k)
+    if (!same_shape(ctx->shapes[g.shape0 + k], j.shapes[k], g.shape0)) return false;
+  for (int k = 0; k < g.nregions; ++k) {
+    const HRegion& a = ctx->regions[g.region0 + k];
+    const HRegion& r = j.regions[k];
+    if (a.parent != (r.parent >= 0 ? r.parent + g.region0 : -1) || a.msm != smap[r.msm] ||
+        a.shape != r.shape + g.shape0 || a.children.size() != r.children.size())
+      return false;
+    for (size_t c = 0; c < r.children.size(); ++c)
+      if (a.children[c] != r.children[c] + g.region0) return false;
+  }
+  return true;
+}
+
+// the job's scene into the batch's scene: shared parts found by content, its shapes and regions appended
+// unless a job before it in the batch had the same geometry; returns the job's chamber in the batch's scene
+static int merge_scene(cm_context* ctx, std::vector<MergedGeometry>& merged, const JobRecord& j) {
   for (const auto& kv : j.mott)
     if (!ctx->mott.count(kv.first)) ctx->mott[kv.first] = kv.second;
   std::vector<int> tmap(j.tables.size()), mmap(j.mats.size()), smap(j.msms.size());
@@ -152,7 +195,10 @@ static int merge_scene(cm_context* ctx, const JobRecord& j) {
     }
     smap[s] = hit;
   }
+  for (const MergedGeometry& g : merged)
+    if (same_geometry(ctx, g, j, smap)) return g.region0 + j.desc.chamber;  // the scene is unchanged
   const int shape0 = (int)ctx->shapes.size(), region0 = (int)ctx->regions.size();
+  merged.push_back(MergedGeometry{shape0, (int)j.shapes.size(), region0, (int)j.regions.size()});
   for (HShape s : j.shapes) {
     if (s.kind == SHAPE_INTERSECTION || s.kind == SHAPE_UNION) {
       s.a += shape0;
@@ -188,6 +234,7 @@ struct Batcher {
   int pool_want = 0;           // secondary-pool records to ask for (doubled after an overflow)
   double emax_eV = 0;          // highest beam energy of the batch's jobs
   int restarts = 0;            // restarts of the current batch after overflows
+  std::vector<MergedGeometry> merged;  // the geometries merged into the batch's scene
   bool waiting = false;        // jobs of this batcher wait in the queue (set before each round)
   std::vector<JobRecord*> active;
   // captured rounds of iterations for the current scene build and run buffers
@@ -271,7 +318,7 @@ static int batch_add(Batcher& b, JobRecord& j) {
       (rc = b.fwd.reserve(b.tally_used + rows)) || (rc = b.job_alive.reserve(b.slots + 1)) ||
       (rc = b.job_steps.reserve(b.slots + 1)) || (rc = b.job_stop.reserve(b.slots + 1)))
     return rc;
-  const int chamber = merge_scene(ctx, j);
+  const int chamber = merge_scene(ctx, b.merged, j);
   for (double e : p.e0) b.emax_eV = std::max(b.emax_eV, e);
   j.slot = b.slots++;
   j.g0 = b.total;
@@ -476,6 +523,7 @@ static int batch_restart(Batcher& b) {
 // the batch ran empty: its scene and tables are dropped
 static void batch_reset(Batcher& b) {
   cm_context_reset(b.ctx);
+  b.merged.clear();
   b.ctx->options = b.options;
   b.npix = 0;
   b.slots = 0;

@@ -277,7 +277,8 @@ int cm_run_noalloc(cm_context* ctx, const cm_run_desc* desc_device_arrays, uint3
  * (JMONSELTests/LinesOnLayers.cu:327-398).  A server batches jobs continuously
  * on one GPU: the jobs of one precision and set of run options share one
  * resident wave of electrons, one merged scene (each job's chamber and regions
- * appended; tables, materials and scatter models shared when equal) and one set
+ * appended, or shared with an earlier job of the same geometry; tables,
+ * materials and scatter models shared when equal) and one set
  * of pixel tables and tallies.  Queued jobs are admitted first in, first out
  * while fewer than `slots` jobs are in their batch and the job's pixel and
  * tally buffers fit in `budget_gb` beside the running jobs'; an admitted job's

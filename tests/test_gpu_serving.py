@@ -116,3 +116,38 @@ def test_poisson_stream_latencies():
     assert len(lat) == 12 and (lat > 0).all()
     print("p50 %.3f s p99 %.3f s makespan %.2f s %d primaries" % (np.percentile(lat, 50), np.percentile(lat, 99),
                                                                  out["makespan"], out["primaries"]))
+
+
+def test_jobs_on_one_sample_share_its_geometry_and_match_cm_run():
+    """Jobs with the same geometry (a linescan split into bands with keys of their own, and a job on another
+    sample between them) share one chamber in the batch's scene; each job's tallies are those of cm_run on
+    its own."""
+    from cudamonsel_b200 import capi, scenes
+    sc = scenes.lines()
+    holder = capi.Engine(0)
+    h = scenes.build_engine(sc, holder)
+    other = capi.Engine(0)
+    ho = scenes.build_engine(scenes.halfspace(), other)
+    centers = scenes.linescan_pixels(48, 2e-9, 0.0, -120e-9)
+    bands = [slice(0, 16), slice(16, 32), slice(32, 48)]
+    keys = np.arange(48, dtype=np.uint64) * np.uint64(104729) + np.uint64(11)
+    srv = capi.Server(0, slots=8, budget_gb=8.0)
+    ids = [srv.submit(holder, h["chamber"], centers[b], scenes.eV(500.0), 300, 50, 1e-9, 0, capi.PREC_FP32,
+                      pixel_keys=keys[b]) for b in bands[:2]]
+    ids.append(srv.submit(other, ho["chamber"], centers[:4], scenes.eV(800.0), 300, 80, 1e-9, 0, capi.PREC_FP32,
+                          pixel_keys=keys[:4]))
+    ids.append(srv.submit(holder, h["chamber"], centers[bands[2]], scenes.eV(500.0), 300, 50, 1e-9, 0,
+                          capi.PREC_FP32, pixel_keys=keys[bands[2]]))
+    infos = [srv.wait(j) for j in ids]
+    assert all(i.state == capi.JOB_DONE for i in infos)
+    res = [srv.result(j) for j in ids]
+    srv.close()
+    back, fwd, _ = holder.run(h["chamber"], centers, scenes.eV(500.0), 300, 50, 1e-9, 0, precision=capi.PREC_FP32,
+                              pixel_keys=keys)
+    for (b, f, _), band in zip([res[0], res[1], res[3]], bands):
+        assert (b == back[band]).all() and (f == fwd[band]).all()
+    bo, fo, _ = other.run(ho["chamber"], centers[:4], scenes.eV(800.0), 300, 80, 1e-9, 0, precision=capi.PREC_FP32,
+                          pixel_keys=keys[:4])
+    assert (res[2][0] == bo).all() and (res[2][1] == fo).all()
+    holder.close()
+    other.close()
